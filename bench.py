@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""NUFFT forward + adjoint benchmark on B200 (one JSON line on rank 0).
+
+Default workload (the 3D golden-means radial configuration):
+  image 200^3 complex64, 32 coils (smooth Gaussian sensitivities times a
+  smooth random phantom of 20 seeded ellipsoids), 20,000 spokes x 400 readout
+  points = 8,000,000 samples per coil, k in [-100, 100), oversampling 1.25,
+  Kaiser-Bessel width 4.  Seeded synthetic data (no dataset is named).
+A step is one forward NUFFT followed by one adjoint NUFFT over all coils.
+``value`` = non-uniform samples per second of a forward+adjoint pair
+(coils x samples per coil / step time), inputs resident in HBM; ``e2e`` =
+the same through the public API with the image in pinned host memory and the
+results returned to the host every step.
+
+Usage:  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Under torchrun every rank runs its own 32-coil workload (weak scaling, no
+collective on the data path); the time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "NUFFT fwd+adj non-uniform samples/s (3D golden-means radial, 32 coils)"
+
+
+# --------------------------------------------------------------------------------------
+# synthetic workload
+# --------------------------------------------------------------------------------------
+def golden_means_radial_3d(nspokes, nread, N):
+    """Full-diameter spokes with directions from the 2D golden means (0.4656, 0.6823)."""
+    n = np.arange(nspokes, dtype=np.float64)
+    z = np.mod(n * 0.4656, 1.0)
+    az = 2 * np.pi * np.mod(n * 0.6823, 1.0)
+    s = np.sqrt(1 - z ** 2)
+    d = np.stack([s * np.cos(az), s * np.sin(az), z], -1)  # (x, y, z)
+    kr = (np.arange(nread) - nread // 2) / nread * N
+    return (d[:, None, :] * kr[None, :, None]).astype(np.float32)  # (nspokes, nread, 3)
+
+
+def phantom_3d(torch, N, nell, device, seed=0):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    ax = (torch.arange(N, dtype=torch.float32, device=device) - N // 2) / N
+    zz, yy, xx = torch.meshgrid(ax, ax, ax, indexing="ij")
+    img = torch.zeros((N, N, N), dtype=torch.complex64, device=device)
+    for _ in range(nell):
+        c = (torch.rand(3, generator=g) - 0.5) * 0.6
+        r = 0.05 + 0.25 * torch.rand(3, generator=g)
+        amp = torch.complex(torch.randn(1, generator=g), torch.randn(1, generator=g)).to(device)
+        inside = ((xx - c[0]) / r[0]) ** 2 + ((yy - c[1]) / r[1]) ** 2 + ((zz - c[2]) / r[2]) ** 2 <= 1
+        img += amp * inside
+    # smooth: Gaussian low-pass in k-space
+    k = torch.fft.fftfreq(N, device=device)
+    kz, ky, kx = torch.meshgrid(k, k, k, indexing="ij")
+    lp = torch.exp(-(kx ** 2 + ky ** 2 + kz ** 2) / (2 * 0.08 ** 2))
+    return torch.fft.ifftn(torch.fft.fftn(img) * lp).to(torch.complex64)
+
+
+def coil_maps_3d(torch, N, ncoils, device):
+    i = torch.arange(ncoils, dtype=torch.float64)
+    zc = 1 - 2 * (i + 0.5) / ncoils
+    phi = i * math.pi * (3 - math.sqrt(5))
+    rc = torch.sqrt(1 - zc ** 2)
+    cen = 0.6 * torch.stack([rc * torch.cos(phi), rc * torch.sin(phi), zc], -1).to(torch.float32).to(device)
+    ax = (torch.arange(N, dtype=torch.float32, device=device) - N // 2) / N
+    zz, yy, xx = torch.meshgrid(ax, ax, ax, indexing="ij")
+    maps = []
+    for c in range(ncoils):
+        d2 = (xx - cen[c, 0]) ** 2 + (yy - cen[c, 1]) ** 2 + (zz - cen[c, 2]) ** 2
+        ph = torch.exp(1j * 2 * math.pi * (c / ncoils))
+        maps.append((torch.exp(-d2 / (2 * 0.4 ** 2)) * ph).to(torch.complex64))
+    m = torch.stack(maps)
+    rss = torch.sqrt(torch.sum(torch.abs(m) ** 2, 0, keepdim=True))
+    return (m / rss).to(torch.complex64)
+
+
+WORKLOADS = {
+    "cfg2": dict(desc="3D golden-means radial NUFFT fwd+adj", N=200, nspokes=20000, nread=400, coils=32,
+                 width=4, oversamp=1.25, nell=20),
+    # reduced variant for quick checks (same construction)
+    "cfg2-small": dict(desc="3D golden-means radial NUFFT fwd+adj (reduced)", N=64, nspokes=2000, nread=128,
+                       coils=8, width=4, oversamp=1.25, nell=20),
+}
+
+
+# --------------------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="pfb_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# --------------------------------------------------------------------------------------
+# CPU baseline (the oracle: C restatement of the reference's Numba kernels + NumPy glue)
+# --------------------------------------------------------------------------------------
+def cpu_baseline(wl, coord, coils_sample, steps=1):
+    from oracle import nufft_oracle as orc
+
+    rng = np.random.default_rng(1)
+    N = wl["N"]
+    x = (rng.standard_normal((coils_sample, N, N, N)) + 1j * rng.standard_normal((coils_sample, N, N, N))
+         ).astype(np.complex64)
+    plan = orc.plan_nufft(coord, (N, N, N), width=wl["width"], oversamp=wl["oversamp"])
+    y = orc.nufft_fwd(x, plan)  # warm-up (first-touch, thread pools)
+    times = []
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        y = orc.nufft_fwd(x, plan)
+        orc.nufft_adj(y, plan)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    M = coord.shape[0] * coord.shape[1]
+    return {"value": coils_sample * M / t, "seconds": t, "threads": orc.lib().orc_num_threads()}
+
+
+# --------------------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------------------
+def stage_times(torch, pf, plan, x, iters):
+    """Per-kernel CUDA-event timings of one forward + adjoint, via the C ABI stages."""
+    import ctypes
+
+    from pyfourier_b200 import _lib
+    from pyfourier_b200._nufft import _Ctx
+
+    L = _lib.load()
+    ctx = _Ctx(plan, None, None, _lib.PFB_NORM_NONE)
+    B = x.shape[0]
+    o = ctx.opts(B, (0, 1))
+    h = plan.interpolator.handle
+    nplanes = B * ctx.C
+    ws = ctx.workspace(nplanes)
+    gbytes = nplanes * int(np.prod(plan.os_shape)) * 8
+    goff = (gbytes + 255) // 256 * 256
+    grid = ws[:gbytes]
+    work = ws[goff:]
+    y = torch.empty((B, plan.interpolator.total_samples), dtype=torch.complex64, device=x.device)
+    xa = torch.empty_like(x)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    fac_f = ctx.fac_fwd
+    fac_a = ctx.fac_adj
+    stages = {
+        "deapod_pad": lambda: L.pfb_deapod_pad(h, ctypes.byref(o), P(x), P(grid), ctypes.c_float(fac_f), st),
+        "fft_fwd": lambda: L.pfb_grid_fft(h, P(grid), nplanes, -1, P(work), work.numel(), st),
+        "interp": lambda: L.pfb_interp(h, ctypes.byref(o), P(grid), P(y), 1, st),
+        "spread": lambda: L.pfb_spread(h, ctypes.byref(o), P(y), P(grid), 1, st),
+        "fft_adj": lambda: L.pfb_grid_fft(h, P(grid), nplanes, 1, P(work), work.numel(), st),
+        "crop_deapod": lambda: L.pfb_crop_deapod(h, ctypes.byref(o), P(grid), P(xa), ctypes.c_float(fac_a), st),
+    }
+    out = {}
+    for name, fn in stages.items():
+        _lib.check(fn())
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(iters)]
+        for a, b in ev:
+            a.record()
+            _lib.check(fn())
+            b.record()
+        torch.cuda.synchronize()
+        out[name] = sum(a.elapsed_time(b) for a, b in ev) / iters
+    return out
+
+
+def algorithmic_bytes(wl, plan, B):
+    M = plan.interpolator.total_samples
+    G = int(np.prod(plan.os_shape))
+    Nv = int(np.prod(plan.shape))
+    nd = plan.ndim
+    coords = M * (4 * nd + 4 + 4)  # sorted coords, permutation, frame index
+    return {
+        "interp": B * G * 8 + B * M * 8 + coords,       # grid read once, samples written
+        "spread": B * M * 8 + B * G * 8 + coords,       # samples read, grid written once
+        "deapod_pad": B * Nv * 8 + B * G * 8,            # image read, padded grid written
+        "crop_deapod": B * Nv * 8 + B * Nv * 8,          # image region of the grid read, image written
+    }
+
+
+def gpu_arm(args, wl, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import pyfourier_b200 as pf
+
+    dev = torch.device(f"cuda:{local_rank}")
+    torch.cuda.set_device(dev)
+    N, B = wl["N"], wl["coils"]
+    coord = golden_means_radial_3d(wl["nspokes"], wl["nread"], N)
+    coord_t = torch.as_tensor(coord, device=dev)
+    plan = pf.plan_nufft(coord_t, (N, N, N), width=wl["width"], oversamp=wl["oversamp"], device=dev)
+    ph = phantom_3d(torch, N, wl["nell"], dev, seed=rank)
+    maps = coil_maps_3d(torch, N, B, dev)
+    x = (maps * ph[None]).contiguous()
+    del maps
+    M = plan.interpolator.total_samples
+    samples_per_step = B * M
+
+    def step(inp):
+        y = pf.nufft(inp, nufft_plan=plan, device=dev)
+        return pf.nufft_adj(y, nufft_plan=plan, device=dev)
+
+    for _ in range(args.warmup):
+        step(x)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        out = step(x)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * samples_per_step / (ms / 1e3)
+
+    # end to end through the public API with host buffers (pinned)
+    x_host = x.cpu().pin_memory()
+    for _ in range(1):
+        pf.nufft_adj(pf.nufft(x_host, nufft_plan=plan, device=dev), nufft_plan=plan, device=dev)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        yk = pf.nufft(x_host, nufft_plan=plan, device=dev)       # H2D image, D2H k-space
+        xa = pf.nufft_adj(yk, nufft_plan=plan, device=dev)       # H2D k-space, D2H image
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = x_host.numel() * 8 + yk.numel() * 8
+    d2h = yk.numel() * 8 + xa.numel() * 8
+    del x_host, yk, xa
+
+    stages = stage_times(torch, pf, plan, x, max(3, args.steps))
+    alg = algorithmic_bytes(wl, plan, B)
+    mine = {k: v for k, v in stages.items() if k in alg}
+    dom = max(mine, key=mine.get)
+    peak, peak_kind = measured_hbm_peak()
+    achieved = alg[dom] / (mine[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": NCU_TRAFFIC.get((args.workload, dom)),
+                "algorithmic_bytes": alg[dom]}
+    return dict(ms=ms, value=value, e2e=world * samples_per_step / e2e_s, h2d=h2d, d2h=d2h, stages=stages,
+                roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=4)
+
+
+# DRAM bytes (read + write) per launch from one ncu capture of the named
+# workload; the capture and its command are summarised under profiles/.
+NCU_TRAFFIC = {}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-coils", type=int, default=2, help="coils in the bounded CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    config = {"workload": wl["desc"], "image": [wl["N"]] * 3, "coils": wl["coils"],
+              "spokes": wl["nspokes"], "readout": wl["nread"], "samples_per_coil": wl["nspokes"] * wl["nread"],
+              "oversamp": wl["oversamp"], "width": wl["width"],
+              "step": "one forward + one adjoint NUFFT over all coils",
+              "l2": "inputs larger than L2 (grid 32 x 250^3 complex64 = 4 GB)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        coord = golden_means_radial_3d(wl["nspokes"], wl["nread"], wl["N"])
+        res = cpu_baseline(wl, coord, args.cpu_coils, steps=max(1, args.steps))
+        sample = (f"{args.cpu_coils} of {wl['coils']} coils, full trajectory "
+                  f"({wl['nspokes'] * wl['nread']} samples/coil), median of {max(1, args.steps)} fwd+adj")
+        line = {"metric": METRIC, "value": res["value"], "unit": "samples/s", "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": res["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "complex64", "data": "synthetic (seeded)", "config": config,
+                "cpu_baseline": {"value": res["value"], "unit": "samples/s", "cores": res["threads"],
+                                 "kind": "port", "sample": sample},
+                "e2e": {"value": res["value"], "unit": "samples/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    r = gpu_arm(args, wl, rank, world, local_rank)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = cpu_baseline(wl, r["coord"], args.cpu_coils, steps=1)
+        cpu = {"value": res["value"], "unit": "samples/s", "cores": res["threads"], "kind": "port",
+               "sample": f"{args.cpu_coils} of {wl['coils']} coils, full trajectory, one fwd+adj "
+                         "(oracle: C restatement of the reference's Numba kernels + NumPy/pocketfft glue)"}
+    if rank == 0:
+        config["stages_ms"] = {k: round(v, 4) for k, v in r["stages"].items()}
+        line = {"metric": METRIC, "value": r["value"], "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "complex64", "data": "synthetic (seeded)", "config": config,
+                "e2e": {"value": r["e2e"], "unit": "samples/s", "h2d_bytes_per_step": r["h2d"],
+                        "d2h_bytes_per_step": r["d2h"]},
+                "gpu_launches": r["launches_per_step"] * args.steps,
+                "roofline": r["roofline"], "cpu_baseline": cpu, "clocks": r["clocks"]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,21 @@
+"""pyfourier_b200: the NUFFT hot path of pyfourier, B200-native (sm_100a CUDA + cuFFT).
+
+Drop-in entry points (same names, arguments and shape conventions as
+pyfourier): ``nufft``, ``nufft_adj``, ``plan_nufft`` / ``NUFFTPlan``,
+``plan_spgram`` / ``sparse_gram`` / ``GramMatrix``.  Everything computes in
+``libpfb200.so`` through its C ABI (include/pfb200.h); there is no CPU
+fallback and importing an operator without the library raises.
+"""
+
+from . import _lib
+from ._b0 import mri_exp_approx
+from ._gram import GramMatrix, plan_spgram, sparse_gram
+from ._nufft import nufft, nufft_adj
+from ._plan import Interpolator, NUFFTPlan, plan_nufft
+
+__version__ = "0.1.0"
+
+__all__ = [
+    "nufft", "nufft_adj", "plan_nufft", "NUFFTPlan", "Interpolator",
+    "plan_spgram", "sparse_gram", "GramMatrix", "mri_exp_approx",
+]

@@ -1,0 +1,409 @@
+// Plan construction: coordinate scaling, tile binning and the stable sort of
+// samples by (tile, frame).  Plan-time only; allocations and host syncs here
+// are intended.
+//
+// Reference behaviour restated (paths inside the pyfourier project):
+//   coordinate scaling   src/pyfourier/_subroutines/_traj.py:57-65 (float32 ops)
+//   first tap x0         src/pyfourier/_subroutines/_grid/_plan.py:201 (float64 ceil)
+//   tap index            src/pyfourier/_subroutines/_grid/_plan.py:210 ((x0+i) mod n_os)
+//   kernel scaling       src/pyfourier/_subroutines/_grid/_plan.py:118-141
+//   deapodisation        src/pyfourier/_subroutines/_apod.py:24-44 (here in float64)
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+
+#include "pfb_common.cuh"
+
+namespace pfb {
+
+namespace {
+
+struct ScaleParams {
+    int ndim;
+    int nframes;
+    int64_t mtot;
+    float s[kMaxDim];
+    float shift[kMaxDim];
+    int nos[kMaxDim];
+    int w[kMaxDim];
+    int cart[kMaxDim];
+    int tile[kMaxDim];
+    int nbins[kMaxDim];
+};
+
+__global__ void scale_and_key_kernel(ScaleParams P, const float *__restrict__ coord,
+                                     const int64_t *__restrict__ frame_off, float *__restrict__ cos_out,
+                                     int *__restrict__ keys, int *__restrict__ vals, int *__restrict__ bad) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= P.mtot) return;
+    // frame of sample g: largest f with frame_off[f] <= g
+    int lo = 0, hi = P.nframes;  // invariant frame_off[lo] <= g < frame_off[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (frame_off[mid] <= g) lo = mid; else hi = mid;
+    }
+    int bin = 0;
+    int stride = 1;
+    for (int a = 0; a < P.ndim; ++a) {
+        float c = coord[g * P.ndim + a];
+        // float32 multiply then add, each rounded (no contraction into an FMA)
+        float cos_ = __fadd_rn(__fmul_rn(c, P.s[a]), P.shift[a]);
+        cos_out[(int64_t)a * P.mtot + g] = cos_;
+        if (!isfinite(cos_) || fabsf(cos_) > 1.0e9f) {
+            atomicExch(bad, 1);
+            cos_ = 0.0f;
+        }
+        long long x0 = start_index(cos_, P.w[a], P.cart[a]);
+        int x0m = pmod(x0, P.nos[a]);
+        bin += (x0m / P.tile[a]) * stride;
+        stride *= P.nbins[a];
+    }
+    keys[g] = bin * P.nframes + lo;
+    vals[g] = (int)g;
+}
+
+__global__ void gather_sorted_kernel(int ndim, int64_t mtot, int nframes, const float *__restrict__ cos_in,
+                                     const int *__restrict__ perm, const int *__restrict__ keys_sorted,
+                                     float *__restrict__ c0, float *__restrict__ c1, float *__restrict__ c2,
+                                     int *__restrict__ sframe) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= mtot) return;
+    int g = perm[j];
+    c0[j] = cos_in[g];
+    if (ndim > 1) c1[j] = cos_in[mtot + g];
+    if (ndim > 2) c2[j] = cos_in[2 * mtot + g];
+    sframe[j] = keys_sorted[j] % nframes;
+}
+
+// bin_start[k] = first sorted position whose key >= k (lower bound), k in [0, nkeys].
+__global__ void bin_start_kernel(const int *__restrict__ keys_sorted, int64_t mtot, int nkeys,
+                                 int *__restrict__ bin_start) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > nkeys) return;
+    int64_t lo = 0, hi = mtot;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (keys_sorted[mid] < k) lo = mid + 1; else hi = mid;
+    }
+    bin_start[k] = (int)lo;
+}
+
+// Interpolator tables in the reference's layout (original sample order).
+__global__ void tables_kernel(Geom g, int axis, int64_t mtot, const float *__restrict__ cos_sorted,
+                              const int *__restrict__ perm, int32_t *__restrict__ index,
+                              float *__restrict__ value) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= mtot) return;
+    int gi = perm[j];
+    float wv[kMaxWidth];
+    long long x0 = axis_weights(cos_sorted[j], g.w[axis], g.cart[axis], g.beta[axis], wv);
+    int w = g.w[axis];
+    for (int i = 0; i < w; ++i) {
+        index[(int64_t)gi * w + i] = pmod(x0 + i, g.nos[axis]);
+        value[(int64_t)gi * w + i] = wv[i];
+    }
+}
+
+double kb_host(double x, double beta) {
+    if (std::fabs(x) > 1.0) return 0.0;
+    double a = beta * std::sqrt(1.0 - x * x);
+    double t = a / 3.75;
+    if (a < 3.75) {
+        double t2 = t * t;
+        return 1.0 + t2 * (3.5156229 + t2 * (3.0899424 + t2 * (1.2067492 +
+               t2 * (0.2659732 + t2 * (0.0360768 + t2 * 0.0045813)))));
+    }
+    double ti = 1.0 / t;
+    return std::pow(a, -0.5) * std::exp(a) *
+           (0.39894228 + ti * (0.01328592 + ti * (0.00225319 + ti * (-0.00157565 +
+            ti * (0.00916281 + ti * (-0.02057706 + ti * (0.02635537 +
+            ti * (-0.01647633 + ti * 0.00392377))))))));
+}
+
+int default_tile(int ndim, int nos) {
+    int t = ndim == 1 ? 1024 : (ndim == 2 ? 32 : 8);
+    return std::max(1, std::min(t, nos));
+}
+
+template <typename T>
+int dev_alloc(T **p, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(e == cudaErrorMemoryAllocation ? PFB_ERR_NOMEM : PFB_ERR_CUDA,
+                    std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return PFB_OK;
+}
+
+void free_plan_buffers(pfb_plan *p) {
+    for (int a = 0; a < kMaxDim; ++a) {
+        cudaFree(p->d_cos[a]);
+        cudaFree(p->d_apod[a]);
+        p->d_cos[a] = p->d_apod[a] = nullptr;
+    }
+    cudaFree(p->d_perm);
+    cudaFree(p->d_sframe);
+    cudaFree(p->d_bin_start);
+    cudaFree(p->d_items_frame);
+    cudaFree(p->d_items_all);
+    cudaFree(p->d_frame_off);
+    p->d_perm = p->d_sframe = p->d_bin_start = nullptr;
+    p->d_items_frame = p->d_items_all = nullptr;
+    p->d_frame_off = nullptr;
+}
+
+void build_items(const std::vector<int> &bs, int nbins, int nframes, int chunk, bool per_frame,
+                 std::vector<SpreadItem> &items) {
+    items.clear();
+    for (int b = 0; b < nbins; ++b) {
+        if (per_frame) {
+            for (int f = 0; f < nframes; ++f) {
+                int s0 = bs[b * nframes + f], s1 = bs[b * nframes + f + 1];
+                for (int s = s0; s < s1; s += chunk)
+                    items.push_back({s, std::min(s1, s + chunk), b, f});
+            }
+        } else {
+            int s0 = bs[b * nframes], s1 = bs[(b + 1) * nframes];
+            for (int s = s0; s < s1; s += chunk)
+                items.push_back({s, std::min(s1, s + chunk), b, -1});
+        }
+    }
+}
+
+}  // namespace
+
+int rebuild_items(pfb_plan *p, int chunk) {
+    std::vector<SpreadItem> a, b;
+    build_items(p->bin_start, p->nbins_total, p->nframes, chunk, true, a);
+    build_items(p->bin_start, p->nbins_total, p->nframes, chunk, false, b);
+    cudaFree(p->d_items_frame);
+    cudaFree(p->d_items_all);
+    p->d_items_frame = p->d_items_all = nullptr;
+    int st;
+    if ((st = dev_alloc(&p->d_items_frame, a.size()))) return st;
+    if ((st = dev_alloc(&p->d_items_all, b.size()))) return st;
+    if (!a.empty())
+        PFB_CUDA_TRY(cudaMemcpy(p->d_items_frame, a.data(), a.size() * sizeof(SpreadItem), cudaMemcpyHostToDevice));
+    if (!b.empty())
+        PFB_CUDA_TRY(cudaMemcpy(p->d_items_all, b.data(), b.size() * sizeof(SpreadItem), cudaMemcpyHostToDevice));
+    p->n_items_frame = (int)a.size();
+    p->n_items_all = (int)b.size();
+    p->chunk = chunk;
+    return PFB_OK;
+}
+
+int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_offsets,
+                int readout_len, const int *shape, const int *os_shape, const int *width,
+                const float *beta, const int *is_cart, const int *tile, int device,
+                cudaStream_t stream, pfb_plan **out) {
+    if (!out) return fail(PFB_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (ndim < 1 || ndim > 3) return fail(PFB_ERR_INVALID, "ndim must be 1, 2 or 3");
+    if (nframes < 1 || !frame_offsets) return fail(PFB_ERR_INVALID, "nframes < 1 or no frame offsets");
+    if (!shape || !os_shape || !width || !beta) return fail(PFB_ERR_INVALID, "missing per-axis parameters");
+    if (frame_offsets[0] != 0) return fail(PFB_ERR_INVALID, "frame_offsets[0] must be 0");
+    for (int f = 0; f < nframes; ++f)
+        if (frame_offsets[f + 1] < frame_offsets[f]) return fail(PFB_ERR_INVALID, "frame_offsets not ascending");
+    int64_t mtot = frame_offsets[nframes];
+    if (mtot >= (int64_t)1 << 31) return fail(PFB_ERR_INVALID, "more than 2^31-1 samples per plan");
+    if (mtot > 0 && !coord) return fail(PFB_ERR_INVALID, "coord is NULL");
+    if (readout_len < 1) return fail(PFB_ERR_INVALID, "readout_len < 1");
+
+    pfb_plan *p = new pfb_plan();
+    p->device = device;
+    p->nframes = nframes;
+    p->mtot = mtot;
+    p->readout = readout_len;
+    p->frame_off.assign(frame_offsets, frame_offsets + nframes + 1);
+    Geom &g = p->g;
+    g.ndim = ndim;
+    g.gvol = 1;
+    g.nvol = 1;
+    int64_t nbins_total = 1;
+    for (int a = 0; a < kMaxDim; ++a) {
+        if (a < ndim) {
+            int z = ndim - 1 - a;  // (z, y, x) input index of x-first axis a
+            g.n[a] = shape[z];
+            g.nos[a] = os_shape[z];
+            // width 1 means integer positions with unit weight, whatever is_cart says
+            // (_grid/_plan.py:69-72)
+            g.cart[a] = (is_cart && is_cart[z] != 0) || width[z] == 1;
+            g.w[a] = g.cart[a] ? 1 : width[z];
+            g.beta[a] = beta[z];
+            g.tile[a] = tile && tile[z] > 0 ? std::min(tile[z], g.nos[a]) : default_tile(ndim, g.nos[a]);
+        } else {
+            g.n[a] = g.nos[a] = g.w[a] = g.tile[a] = 1;
+            g.cart[a] = 1;
+            g.beta[a] = 0.f;
+        }
+        if (g.n[a] < 1 || g.nos[a] < g.n[a]) {
+            delete p;
+            return fail(PFB_ERR_INVALID, "need 1 <= shape <= os_shape on every axis");
+        }
+        if (g.w[a] < 1 || g.w[a] > kMaxWidth) {
+            delete p;
+            return fail(PFB_ERR_INVALID, "kernel width must be in [1, 8]");
+        }
+        if (g.w[a] > g.nos[a]) {
+            delete p;
+            return fail(PFB_ERR_INVALID, "kernel width larger than the oversampled grid");
+        }
+        g.nbins[a] = (g.nos[a] + g.tile[a] - 1) / g.tile[a];
+        g.sh[a] = g.nos[a] / 2;
+        g.gvol *= g.nos[a];
+        g.nvol *= g.n[a];
+        nbins_total *= g.nbins[a];
+    }
+    if (nbins_total * nframes >= (int64_t)1 << 30) {
+        delete p;
+        return fail(PFB_ERR_INVALID, "too many (tile, frame) bins; use a larger tile");
+    }
+    p->nbins_total = (int)nbins_total;
+
+    // kernel scaling: product over axes of the node-centred sums (_grid/_plan.py:118-141)
+    double scale = 1.0;
+    for (int a = 0; a < ndim; ++a) {
+        if (g.w[a] == 1) continue;
+        double start = std::ceil(-g.w[a] / 2.0), s = 0.0;
+        for (int e = 0; e < g.w[a]; ++e) s += kb_host((start + e) / (g.w[a] / 2.0), (double)g.beta[a]);
+        scale *= s;
+    }
+    p->scale = scale;
+
+    int st = PFB_OK;
+    float *d_cos_tmp = nullptr;
+    int *d_keys = nullptr, *d_vals = nullptr, *d_keys_sorted = nullptr, *d_bad = nullptr;
+    void *d_temp = nullptr;
+    size_t temp_bytes = 0;
+    int nkeys = (int)(nbins_total * nframes);
+    const int T = 256;
+
+    auto cleanup = [&](int code) {
+        cudaFree(d_cos_tmp);
+        cudaFree(d_keys);
+        cudaFree(d_vals);
+        cudaFree(d_keys_sorted);
+        cudaFree(d_bad);
+        cudaFree(d_temp);
+        if (code != PFB_OK) {
+            free_plan_buffers(p);
+            delete p;
+        }
+        return code;
+    };
+
+#define PFB_TRY_ST(expr) do { st = (expr); if (st != PFB_OK) return cleanup(st); } while (0)
+#define PFB_TRY_CU(expr) do { cudaError_t _e = (expr); if (_e != cudaSuccess) \
+        return cleanup(fail(PFB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e))); } while (0)
+
+    PFB_TRY_ST(dev_alloc(&p->d_frame_off, nframes + 1));
+    PFB_TRY_CU(cudaMemcpyAsync(p->d_frame_off, frame_offsets, (nframes + 1) * sizeof(int64_t),
+                               cudaMemcpyHostToDevice, stream));
+    for (int a = 0; a < ndim; ++a) PFB_TRY_ST(dev_alloc(&p->d_cos[a], mtot));
+    PFB_TRY_ST(dev_alloc(&p->d_perm, mtot));
+    PFB_TRY_ST(dev_alloc(&p->d_sframe, mtot));
+    PFB_TRY_ST(dev_alloc(&p->d_bin_start, nkeys + 1));
+    PFB_TRY_ST(dev_alloc(&d_cos_tmp, (size_t)ndim * mtot));
+    PFB_TRY_ST(dev_alloc(&d_keys, mtot));
+    PFB_TRY_ST(dev_alloc(&d_vals, mtot));
+    PFB_TRY_ST(dev_alloc(&d_keys_sorted, mtot));
+    PFB_TRY_ST(dev_alloc(&d_bad, 1));
+    PFB_TRY_CU(cudaMemsetAsync(d_bad, 0, sizeof(int), stream));
+
+    ScaleParams sp{};
+    sp.ndim = ndim;
+    sp.nframes = nframes;
+    sp.mtot = mtot;
+    for (int a = 0; a < ndim; ++a) {
+        // _traj.py:62-65: scale = ceil(osf*N)/N and shift = ceil(osf*N)//2, float32
+        sp.s[a] = (float)g.nos[a] / (float)g.n[a];
+        sp.shift[a] = (float)(g.nos[a] / 2);
+        sp.nos[a] = g.nos[a];
+        sp.w[a] = g.w[a];
+        sp.cart[a] = g.cart[a];
+        sp.tile[a] = g.tile[a];
+        sp.nbins[a] = g.nbins[a];
+    }
+    if (mtot > 0) {
+        unsigned blocks = (unsigned)((mtot + T - 1) / T);
+        scale_and_key_kernel<<<blocks, T, 0, stream>>>(sp, coord, p->d_frame_off, d_cos_tmp, d_keys, d_vals, d_bad);
+        PFB_TRY_CU(cudaGetLastError());
+        int end_bit = 1;
+        while ((1LL << end_bit) < (long long)nkeys) ++end_bit;
+        PFB_TRY_CU(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, d_keys, d_keys_sorted, d_vals,
+                                                   p->d_perm, (int)mtot, 0, end_bit, stream));
+        PFB_TRY_CU(cudaMalloc(&d_temp, std::max<size_t>(temp_bytes, 1)));
+        PFB_TRY_CU(cub::DeviceRadixSort::SortPairs(d_temp, temp_bytes, d_keys, d_keys_sorted, d_vals,
+                                                   p->d_perm, (int)mtot, 0, end_bit, stream));
+        gather_sorted_kernel<<<blocks, T, 0, stream>>>(ndim, mtot, nframes, d_cos_tmp, p->d_perm, d_keys_sorted,
+                                                       p->d_cos[0], p->d_cos[1], p->d_cos[2], p->d_sframe);
+        PFB_TRY_CU(cudaGetLastError());
+    }
+    bin_start_kernel<<<(nkeys + 1 + T - 1) / T, T, 0, stream>>>(d_keys_sorted, mtot, nkeys, p->d_bin_start);
+    PFB_TRY_CU(cudaGetLastError());
+    p->bin_start.resize(nkeys + 1);
+    int bad = 0;
+    PFB_TRY_CU(cudaMemcpyAsync(p->bin_start.data(), p->d_bin_start, (nkeys + 1) * sizeof(int),
+                               cudaMemcpyDeviceToHost, stream));
+    PFB_TRY_CU(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PFB_TRY_CU(cudaStreamSynchronize(stream));
+    if (bad) return cleanup(fail(PFB_ERR_INVALID, "non-finite or out-of-range coordinates"));
+
+    // deapodisation vectors (float64 math, _apod.py:27-41)
+    for (int a = 0; a < ndim; ++a) {
+        if (g.w[a] == 1) continue;
+        int n = g.n[a];
+        std::vector<double> v(n);
+        for (int i = 0; i < n; ++i) {
+            double q = M_PI * g.w[a] * (double)(i - n / 2) / (double)g.nos[a];
+            double arg = (double)g.beta[a] * (double)g.beta[a] - q * q;
+            double r = std::sqrt(arg);
+            v[i] = r / std::sinh(r);
+        }
+        double dc = v[n / 2];
+        std::vector<float> vf(n);
+        for (int i = 0; i < n; ++i) {
+            double r = v[i] / dc;
+            vf[i] = std::isnan(r) ? 1.0f : (float)r;
+        }
+        PFB_TRY_ST(dev_alloc(&p->d_apod[a], n));
+        PFB_TRY_CU(cudaMemcpy(p->d_apod[a], vf.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    }
+
+    int maxbin = 0;
+    for (int k = 0; k < nkeys; ++k) maxbin = std::max(maxbin, p->bin_start[k + 1] - p->bin_start[k]);
+    p->max_bin = maxbin;
+    int chunk = ndim == 3 ? 256 : 512;
+    PFB_TRY_ST(rebuild_items(p, chunk));
+#undef PFB_TRY_ST
+#undef PFB_TRY_CU
+    cleanup(PFB_OK);
+    *out = p;
+    return PFB_OK;
+}
+
+int plan_tables(const pfb_plan *p, int axis_zyx, int32_t *index, float *value, cudaStream_t s) {
+    if (axis_zyx < 0 || axis_zyx >= p->g.ndim) return fail(PFB_ERR_INVALID, "axis out of range");
+    int a = p->g.ndim - 1 - axis_zyx;
+    if (p->mtot == 0) return PFB_OK;
+    const int T = 256;
+    tables_kernel<<<(unsigned)((p->mtot + T - 1) / T), T, 0, s>>>(p->g, a, p->mtot, p->d_cos[a], p->d_perm,
+                                                                  index, value);
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
+void plan_free(pfb_plan *p) {
+    {
+        std::lock_guard<std::mutex> lk(p->fft_mu);
+        for (auto &kv : p->fft_plans) cufftDestroy(kv.second);
+        p->fft_plans.clear();
+    }
+    free_plan_buffers(p);
+    delete p;
+}
+
+}  // namespace pfb

@@ -1,0 +1,94 @@
+"""CPU checks of the C ABI boundary and of host-side logic (no GPU calls)."""
+
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "pfb200.h")
+
+
+def _declared():
+    hdr = open(HEADER).read()
+    return set(re.findall(r"^(?:int|const char \*)\s*(pfb_\w+)\(", hdr, re.M))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    from pyfourier_b200 import _lib
+
+    L = _lib.load()
+    declared = _declared()
+    assert declared == set(_lib.EXPORTS)
+    for name in declared:
+        assert hasattr(L, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (pfb_\w+)", out))
+    assert declared <= exported
+    assert L.pfb_version().startswith(b"pyfourier_b200")
+
+
+def test_status_mapping_without_gpu():
+    """Argument validation happens before any CUDA call and maps to ValueError."""
+    from pyfourier_b200 import _lib
+
+    L = _lib.load()
+    out = ctypes.c_void_p()
+    st = L.pfb_plan_create(None, 4, 1, None, 1, None, None, None, None, None, None, 0, None,
+                           ctypes.byref(out))
+    assert st == _lib.PFB_ERR_INVALID
+    assert b"ndim" in L.pfb_last_error()
+    with pytest.raises(ValueError):
+        _lib.check(st)
+    st = L.pfb_gram_create(2, None, None, 4, 1, None, 0, None, ctypes.byref(out))
+    assert st == _lib.PFB_ERR_INVALID
+    # NULL handles are rejected, destroy(NULL) is a no-op
+    assert L.pfb_plan_destroy(None) == 0
+    assert L.pfb_gram_destroy(None) == 0
+    info = _lib.PlanInfoT()
+    assert L.pfb_plan_info(None, ctypes.byref(info)) == _lib.PFB_ERR_INVALID
+
+
+def test_apply_struct_layout_matches_header():
+    from pyfourier_b200 import _lib
+
+    # int64 + 2*int32 + 4 pointers + 2*int32 = 8 + 8 + 32 + 8 = 56 bytes on LP64
+    assert ctypes.sizeof(_lib.ApplyT) == 56
+    assert ctypes.sizeof(_lib.PlanInfoT) == 4 + 4 + 8 + 4 * 12 + 8 + 4 + 4
+
+
+def test_host_parameter_math_matches_oracle():
+    from oracle import nufft_oracle as orc
+    from pyfourier_b200 import _plan
+
+    for w, o in [((4, 4), (2.0, 2.0)), ((4, 4, 4), (1.25,) * 3), ((6, 3), (1.25, 1.5))]:
+        np.testing.assert_array_equal(_plan.beta_f32(w, o), orc.beta_f32(w, o))
+    for n, o in [((128, 128), (2.0, 2.0)), ((200, 200, 200), (1.25,) * 3), ((192, 220), (1.25, 1.1))]:
+        assert _plan.oversamp_shape(n, o) == orc.oversamp_shape(n, o)
+
+
+def test_frames_from_coord_shapes():
+    from pyfourier_b200._plan import _frames_from_coord
+
+    flat, offs, ro, ds = _frames_from_coord(np.zeros((3, 5, 7, 2), np.float32))
+    assert flat.shape == (105, 2) and list(offs) == [0, 35, 70, 105] and ro == 7 and ds == (5, 7)
+    flat, offs, ro, ds = _frames_from_coord(np.zeros((7, 3), np.float32))
+    assert flat.shape == (7, 3) and list(offs) == [0, 7] and ds == (7,)
+    flat, offs, ro, ds = _frames_from_coord([np.zeros((2, 8, 2), np.float32), np.zeros((5, 8, 2), np.float32)])
+    assert flat.shape == (56, 2) and list(offs) == [0, 16, 56] and ro == 8 and ds is None
+
+
+def test_b0_basis_fp64_matches_oracle():
+    from oracle import nufft_oracle as orc
+    from pyfourier_b200._b0 import mri_exp_approx
+
+    rng = np.random.default_rng(0)
+    zmap = 100 * rng.standard_normal((16, 16))
+    t = 5e-3 * np.arange(64) / 64
+    b1, c1 = mri_exp_approx(zmap, t, 6, 40)
+    b2, c2 = orc.mri_exp_approx(zmap, t, 6, 40)
+    np.testing.assert_allclose(b1, b2, rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(c1, c2, rtol=1e-12)

@@ -1,0 +1,124 @@
+"""GPU parity of the libpfb200 stages against the reference's own Numba kernels
+(golden vectors in tests/golden/kernels.npz), called through the C ABI."""
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+from oracle import nufft_oracle as orc  # noqa: E402
+
+
+def _lib():
+    from pyfourier_b200 import _lib
+
+    return _lib
+
+
+def _plan(coord, N, osf, w):
+    import pyfourier_b200 as pf
+
+    return pf.plan_nufft(torch.as_tensor(coord), tuple(int(n) for n in N), width=tuple(int(x) for x in w),
+                         oversamp=tuple(float(o) for o in osf), device="cuda:0")
+
+
+def _opts(batch, ncoeff, basis=None):
+    L = _lib()
+    o = L.ApplyT()
+    o.batch, o.ncoeff, o.nseg, o.norm, o.flags = batch, ncoeff, 1, 0, 0
+    o.basis = basis.data_ptr() if basis is not None else None
+    return o
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def rel(a, b):
+    return orc.rel_l2(np.asarray(a), np.asarray(b))
+
+
+@pytest.mark.parametrize("w", [2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("osf", [1.25, 2.0])
+def test_tables_edge_coords(golden, w, osf):
+    c = golden["tab_coord"]
+    N = int(golden["tab_N"])
+    plan = _plan(c[None, None, :, None], (N,), (osf,), (w,))
+    idx, val = plan.interpolator.tables(0)
+    tag = f"tab_w{w}_os{osf}"
+    np.testing.assert_array_equal(idx.cpu().numpy()[0], golden[tag + "_index"])
+    np.testing.assert_allclose(val.cpu().numpy()[0], golden[tag + "_value"], rtol=3e-6, atol=1e-7)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_tables_and_scale(golden, d):
+    p = f"k{d}d_"
+    coord = golden[p + "coord"]
+    F = coord.shape[0]
+    plan = _plan(coord[:, None], golden[p + "N"], golden[p + "osf"], golden[p + "width"])
+    ip = plan.interpolator
+    for a in range(d):
+        idx, val = ip.tables(a)
+        np.testing.assert_array_equal(idx.cpu().numpy().reshape(F, -1, idx.shape[-1]), golden[p + f"index{a}"])
+        np.testing.assert_allclose(val.cpu().numpy().reshape(F, -1, val.shape[-1]), golden[p + f"value{a}"],
+                                   rtol=3e-6, atol=1e-7)
+    ref_scale = orc.kernel_scaling([float(b) for b in golden[p + "beta"]], golden[p + "width"])
+    assert ip.scale == pytest.approx(ref_scale, rel=1e-12)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+@pytest.mark.parametrize("subspace", [False, True])
+def test_spread_interp_vs_reference(golden, d, subspace):
+    L = _lib()
+    lib = L.load()
+    p = f"k{d}d_"
+    coord = golden[p + "coord"]
+    F, M = coord.shape[:2]
+    plan = _plan(coord[:, None], golden[p + "N"], golden[p + "osf"], golden[p + "width"])
+    h = plan.interpolator.handle
+    os_ = tuple(int(v) for v in golden[p + "os"])
+    nc = golden[p + "noncart"]  # (F, B, M)
+    B = nc.shape[1]
+    y = torch.as_tensor(np.ascontiguousarray(nc.transpose(1, 0, 2).reshape(B, F * M))).cuda()
+    basis = torch.as_tensor(golden[p + "basis"]).cuda() if subspace else None
+    C = basis.shape[1] if subspace else F
+    grid = torch.empty((B, C, *os_), dtype=torch.complex64, device="cuda")
+    o = _opts(B, C, basis)
+    L.check(lib.pfb_spread(h, ctypes.byref(o), ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(grid.data_ptr()),
+                           0, _stream()))
+    ref = golden[p + ("spread_sub" if subspace else "spread")]  # (C, B, *os)
+    assert rel(grid.cpu().numpy().swapaxes(0, 1), ref) < 1e-5
+
+    gin = golden[p + ("grid_in_sub" if subspace else "grid_in")]  # (C, B, *os)
+    g = torch.as_tensor(np.ascontiguousarray(gin.swapaxes(0, 1))).cuda()
+    out = torch.empty((B, F * M), dtype=torch.complex64, device="cuda")
+    L.check(lib.pfb_interp(h, ctypes.byref(o), ctypes.c_void_p(g.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                           0, _stream()))
+    ref = golden[p + ("interp_sub" if subspace else "interp")]  # (F, B, M)
+    got = out.cpu().numpy().reshape(B, F, M).transpose(1, 0, 2)
+    assert rel(got, ref) < 1e-5
+
+
+def test_spread_is_deterministic_in_layout_and_fft_shift(golden):
+    """fft_layout=1 is the centred grid rolled by -(n_os // 2) on every axis."""
+    L = _lib()
+    lib = L.load()
+    p = "k2d_"
+    coord = golden[p + "coord"]
+    F, M = coord.shape[:2]
+    plan = _plan(coord[:, None], golden[p + "N"], golden[p + "osf"], golden[p + "width"])
+    h = plan.interpolator.handle
+    os_ = tuple(int(v) for v in golden[p + "os"])
+    nc = golden[p + "noncart"]
+    B = nc.shape[1]
+    y = torch.as_tensor(np.ascontiguousarray(nc.transpose(1, 0, 2).reshape(B, F * M))).cuda()
+    g0 = torch.empty((B, F, *os_), dtype=torch.complex64, device="cuda")
+    g1 = torch.empty_like(g0)
+    o = _opts(B, F)
+    L.check(lib.pfb_spread(h, ctypes.byref(o), ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(g0.data_ptr()), 0, _stream()))
+    L.check(lib.pfb_spread(h, ctypes.byref(o), ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(g1.data_ptr()), 1, _stream()))
+    rolled = torch.fft.ifftshift(g0, dim=(-2, -1))
+    assert rel(g1.cpu(), rolled.cpu()) < 1e-6

@@ -1,0 +1,257 @@
+"""GPU parity of the public operators (nufft, nufft_adj, B0, subspace, weights)
+against the CPU oracle on identical seeded inputs; edge cases; error paths."""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+from oracle import nufft_oracle as orc  # noqa: E402
+
+TOL = 1e-5  # rel-L2 vs the oracle (float32 atomics: order differs, so a tolerance)
+
+
+def pf():
+    import pyfourier_b200
+
+    return pyfourier_b200
+
+
+def crandn(rng, *shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+def radial(nspokes, nread, N, seed=0, rot=0.0):
+    ga = np.pi / ((1 + 5 ** 0.5) / 2)
+    ang = np.arange(nspokes) * ga + rot
+    kr = (np.arange(nread) - nread // 2) / nread * N
+    return np.stack([np.cos(ang)[:, None] * kr, np.sin(ang)[:, None] * kr], -1).astype(np.float32)
+
+
+def rel(a, b):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    return orc.rel_l2(a, b)
+
+
+def check_pair(coord, N, x, y, width=4, oversamp=2.0, norm=None, basis=None, weight=None, **plan_kw):
+    """nufft and nufft_adj on GPU vs the oracle (same plan parameters)."""
+    P = pf()
+    oplan = orc.plan_nufft(coord, N, width=width, oversamp=oversamp, **plan_kw)
+    gplan = P.plan_nufft(torch.as_tensor(coord), N, width=width, oversamp=oversamp, device="cuda:0", **plan_kw)
+    xr = orc.nufft_fwd(x, oplan, basis=basis, weight=weight, norm=norm)
+    xg = P.nufft(torch.as_tensor(x).cuda(), nufft_plan=gplan, basis=basis, weight=weight, norm=norm,
+                 device="cuda:0")
+    assert xg.shape == xr.shape
+    e1 = rel(xg, xr)
+    yr = orc.nufft_adj(y, oplan, basis=basis, weight=weight, norm=norm)
+    yg = P.nufft_adj(torch.as_tensor(y).cuda(), nufft_plan=gplan, basis=basis, weight=weight, norm=norm,
+                     device="cuda:0")
+    assert yg.shape == yr.shape
+    e2 = rel(yg, yr)
+    assert e1 < TOL and e2 < TOL, (e1, e2)
+    return gplan
+
+
+def test_cfg1_radial_2d_full_size():
+    rng = np.random.default_rng(0)
+    N = 128
+    coord = radial(201, 256, N)
+    x = crandn(rng, 8, N, N)
+    y = crandn(rng, 8, 201, 256)
+    check_pair(coord, (N, N), x, y, width=4, oversamp=2.0)
+
+
+@pytest.mark.parametrize("norm", [None, "ortho"])
+def test_2d_small_norms(norm):
+    rng = np.random.default_rng(1)
+    N = 48
+    coord = radial(37, 96, N)
+    check_pair(coord, (N, N), crandn(rng, 3, N, N), crandn(rng, 3, 37, 96), norm=norm, oversamp=1.25)
+
+
+@pytest.mark.parametrize("w", [2, 3, 5, 6, 7, 8])
+def test_widths(w):
+    rng = np.random.default_rng(2)
+    N = 40
+    coord = radial(21, 80, N)
+    check_pair(coord, (N, N), crandn(rng, 2, N, N), crandn(rng, 2, 21, 80), width=w, oversamp=2.0)
+
+
+def test_odd_sizes_and_anisotropic():
+    rng = np.random.default_rng(3)
+    N = (45, 37)
+    coord = ((rng.random((30, 50, 2)) - 0.5) * np.array(N[::-1])).astype(np.float32)
+    check_pair(coord, N, crandn(rng, 2, *N), crandn(rng, 2, 30, 50), width=(5, 3), oversamp=(1.5, 2.0))
+
+
+def test_edges_and_out_of_range_wrap():
+    """Samples at exactly -N/2 and +N/2 - eps, and beyond +-N/2 (reference wraps mod n_os)."""
+    rng = np.random.default_rng(4)
+    N = 32
+    c = np.array([[-16, -16], [15.999, 15.999], [-16, 15.5], [16, 0], [20.25, -19.5], [0, 0], [0.5, -0.5],
+                  [7.0, 7.0]], np.float32)
+    coord = np.concatenate([c, ((rng.random((56, 2)) - 0.5) * N).astype(np.float32)])[None]
+    check_pair(coord, (N, N), crandn(rng, 2, N, N), crandn(rng, 2, 1, 64), width=4, oversamp=1.25)
+
+
+def test_all_samples_in_one_tile_and_chunking():
+    """A crowded bin (k-space centre hot spot) split into several work items."""
+    rng = np.random.default_rng(5)
+    N = 64
+    coord = ((rng.random((1, 4000, 2)) - 0.5) * 3.0).astype(np.float32)
+    gplan = check_pair(coord, (N, N), crandn(rng, 3, N, N), crandn(rng, 3, 1, 4000), oversamp=2.0)
+    assert gplan.interpolator.max_bin >= 3000
+
+
+def test_multiframe_and_weights():
+    rng = np.random.default_rng(6)
+    N, F = 40, 3
+    coord = np.stack([radial(10, 64, N, rot=0.3 * f) for f in range(F)])
+    x = crandn(rng, 2, F, N, N)
+    y = crandn(rng, 2, F, 10, 64)
+    wps = rng.random((F, 10, 64)).astype(np.float32)
+    check_pair(coord, (N, N), x, y, weight=wps)
+    wfull = rng.random((2, F, 10, 64)).astype(np.float32)  # varies over the batch: torch multiply
+    check_pair(coord, (N, N), x, y, weight=wfull)
+
+
+def test_subspace_basis():
+    rng = np.random.default_rng(7)
+    N, F, K = 32, 6, 3
+    coord = np.stack([radial(8, 48, N, rot=0.2 * f) for f in range(F)])
+    basis = np.linalg.qr(crandn(rng, F, K))[0].astype(np.complex64)
+    check_pair(coord, (N, N), crandn(rng, 2, K, N, N), crandn(rng, 2, F, 8, 48), basis=basis)
+
+
+def test_3d():
+    rng = np.random.default_rng(8)
+    N = (20, 24, 22)
+    coord = ((rng.random((40, 60, 3)) - 0.5) * np.array(N[::-1])).astype(np.float32)
+    check_pair(coord, N, crandn(rng, 2, *N), crandn(rng, 2, 40, 60), width=4, oversamp=1.25)
+
+
+def test_1d():
+    rng = np.random.default_rng(9)
+    N = 100
+    coord = ((rng.random((5, 70, 1)) - 0.5) * N).astype(np.float32)
+    check_pair(coord, (N,), crandn(rng, 3, N), crandn(rng, 3, 5, 70), width=4, oversamp=2.0)
+
+
+def test_stack_of_stars_cartesian_axis():
+    """z Cartesian (integer positions, width 1, osf 1) as in _nufft/_plan.py:139-146."""
+    rng = np.random.default_rng(10)
+    N = (8, 32, 32)
+    r = radial(12, 40, 32)
+    kz = np.arange(-4, 4, dtype=np.float32)
+    coord = np.concatenate([np.broadcast_to(r[None], (8, 12, 40, 2)),
+                            np.broadcast_to(kz[:, None, None, None], (8, 12, 40, 1))], -1)
+    coord = np.ascontiguousarray(coord.reshape(96, 40, 3))
+    gplan = check_pair(coord, N, crandn(rng, 2, *N), crandn(rng, 2, 96, 40), width=4, oversamp=2.0)
+    assert gplan.width[0] == 1 and gplan.os_shape[0] == 8
+
+
+def test_b0_segments_and_chunks():
+    rng = np.random.default_rng(11)
+    N, nv, ns = 32, 10, 64
+    coord = radial(nv, ns, N)
+    yy, xx = np.mgrid[:N, :N] / N - 0.5
+    b0 = 150 * np.exp(-((xx - 0.1) ** 2 + yy ** 2) / 0.05) - 80
+    dt = 5e-3 / ns
+    for Lb in (None, 4):
+        check_pair(coord, (N, N), crandn(rng, 3, N, N), crandn(rng, 3, nv, ns), zmap=b0, L=6, nbins=40,
+                   dt=dt, L_batch_size=Lb)
+
+
+def test_adjointness_ortho_gpu():
+    P = pf()
+    rng = np.random.default_rng(12)
+    N = 64
+    coord = radial(50, 128, N)
+    plan = P.plan_nufft(torch.as_tensor(coord), (N, N), width=4, oversamp=2.0, device="cuda:0")
+    x = torch.as_tensor(crandn(rng, 4, N, N)).cuda()
+    y = torch.as_tensor(crandn(rng, 4, 50, 128)).cuda()
+    lhs = torch.vdot(y.flatten(), P.nufft(x, nufft_plan=plan, norm="ortho").flatten())
+    rhs = torch.vdot(P.nufft_adj(y, nufft_plan=plan, norm="ortho").flatten(), x.flatten())
+    assert abs((lhs - rhs) / lhs).item() < 1e-5
+
+
+def test_ragged_frames_match_per_frame_calls():
+    """A plan over frames of uneven length equals separate per-frame plans."""
+    P = pf()
+    rng = np.random.default_rng(13)
+    N = 32
+    frames = [radial(n, 64, N, rot=0.1 * i) for i, n in enumerate([5, 1, 17, 9])]
+    frames.append(np.zeros((0, 64, 2), np.float32))  # an empty frame
+    plan = P.plan_nufft([torch.as_tensor(f) for f in frames], (N, N), width=4, oversamp=2.0, device="cuda:0")
+    F = len(frames)
+    x = torch.as_tensor(crandn(rng, 2, F, N, N)).cuda()
+    y = P.nufft(x, nufft_plan=plan)
+    offs = plan.interpolator.frame_offsets
+    tot = offs[-1]
+    assert y.shape == (2, tot)
+    yk = torch.as_tensor(crandn(rng, 2, tot)).cuda()
+    xa = P.nufft_adj(yk, nufft_plan=plan)
+    for f, c in enumerate(frames):
+        if c.shape[0] == 0:
+            assert torch.count_nonzero(xa[:, f]) == 0
+            continue
+        pl = P.plan_nufft(torch.as_tensor(c), (N, N), width=4, oversamp=2.0, device="cuda:0")
+        yf = P.nufft(x[:, f], nufft_plan=pl)
+        assert rel(y[:, offs[f]:offs[f + 1]], yf.reshape(2, -1).cpu().numpy()) < 1e-6
+        xf = P.nufft_adj(yk[:, offs[f]:offs[f + 1]].reshape(2, *c.shape[:-1]), nufft_plan=pl)
+        assert rel(xa[:, f], xf.cpu().numpy()) < 1e-6
+
+
+def test_single_sample_and_real_input_dtype():
+    P = pf()
+    N = 16
+    coord = np.array([[[1.25, -3.5]]], np.float32)
+    x = np.random.default_rng(14).standard_normal((N, N)).astype(np.float32)
+    plan = orc.plan_nufft(coord, (N, N), width=4, oversamp=2.0)
+    ref = orc.nufft_fwd(x.astype(np.complex64), plan).real
+    got = P.nufft(torch.as_tensor(x), torch.as_tensor(coord), (N, N), width=4, oversamp=2.0)
+    assert got.dtype == torch.float32 and got.device.type == "cpu"
+    assert rel(got, ref) < 1e-5
+    got_np = P.nufft(x, coord, (N, N), width=4, oversamp=2.0)
+    assert isinstance(got_np, np.ndarray)
+
+
+def test_errors_raise_value_error():
+    P = pf()
+    coord = radial(4, 16, 16)
+    plan = P.plan_nufft(torch.as_tensor(coord), (16, 16), device="cuda:0")
+    with pytest.raises(ValueError):
+        P.nufft(torch.zeros(2, 15, 16, dtype=torch.complex64), nufft_plan=plan)
+    with pytest.raises(ValueError):
+        P.nufft_adj(torch.zeros(2, 4, 15, dtype=torch.complex64), nufft_plan=plan)
+    with pytest.raises(ValueError):
+        P.plan_nufft(torch.full((1, 4, 2), float("nan")), (16, 16), device="cuda:0")
+    with pytest.raises(ValueError):
+        P.nufft(torch.zeros(16, 16, dtype=torch.complex64), nufft_plan=plan, norm="bogus")
+    with pytest.raises(ValueError):
+        P.plan_nufft(torch.as_tensor(coord), (16, 16), width=9, device="cuda:0")
+
+
+def test_cuda_graph_capture():
+    """An apply contains no host sync or allocation inside the library: capturable."""
+    P = pf()
+    rng = np.random.default_rng(15)
+    N = 64
+    coord = radial(40, 128, N)
+    plan = P.plan_nufft(torch.as_tensor(coord), (N, N), width=4, oversamp=2.0, device="cuda:0")
+    x = torch.as_tensor(crandn(rng, 4, N, N)).cuda()
+    ref = P.nufft_adj(P.nufft(x, nufft_plan=plan), nufft_plan=plan)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            P.nufft_adj(P.nufft(x, nufft_plan=plan), nufft_plan=plan)
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        out = P.nufft_adj(P.nufft(x, nufft_plan=plan), nufft_plan=plan)
+    g.replay()
+    torch.cuda.synchronize()
+    assert rel(out, ref.cpu().numpy()) < 1e-6

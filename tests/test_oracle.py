@@ -1,0 +1,157 @@
+"""CPU tests of the oracle: pinned against the reference's golden vectors, then
+checked against an FP64 direct NUDFT and for adjointness.  No GPU needed."""
+
+import numpy as np
+import pytest
+
+from oracle import nufft_oracle as orc
+
+
+def test_kaiser_bessel_matches_reference(golden):
+    xs, betas, ref = golden["kb_x"], golden["kb_beta"], golden["kb_val"]
+    got = np.array([[orc.kaiser_bessel(x, b) for x in xs] for b in betas])
+    np.testing.assert_allclose(got, ref, rtol=1e-13, atol=0)
+
+
+def test_kernel_scaling_matches_reference(golden):
+    for w, b, v in zip(golden["scal_width"], golden["scal_beta"], golden["scal_value"]):
+        nd = int((w > 0).sum())
+        got = orc.kernel_scaling(b[:nd], w[:nd])
+        assert got == pytest.approx(v, rel=1e-13)
+
+
+@pytest.mark.parametrize("w", [2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("osf", [1.25, 2.0])
+def test_tables_match_reference(golden, w, osf):
+    c = golden["tab_coord"]
+    N = int(golden["tab_N"])
+    beta = orc.beta_f32((w,), (osf,))
+    c_os = orc.scale_coord(c[None, :, None], (N,), (osf,))
+    n_os = orc.oversamp_shape((N,), (osf,))
+    idx, val = orc.prepare_tables(c_os, n_os, (w,), beta)
+    tag = f"tab_w{w}_os{osf}"
+    np.testing.assert_array_equal(idx[0], golden[tag + "_index"])
+    np.testing.assert_allclose(val[0], golden[tag + "_value"], rtol=2e-7, atol=0)
+
+
+@pytest.mark.parametrize("d", [1, 2, 3])
+def test_spread_interp_match_reference(golden, d):
+    p = f"k{d}d_"
+    N, osf, w, beta, os_ = (golden[p + k] for k in ("N", "osf", "width", "beta", "os"))
+    coord = golden[p + "coord"]
+    c_os = orc.scale_coord(coord, N[::-1], osf[::-1])
+    idx, val = orc.prepare_tables(c_os, os_, w, beta)
+    for a in range(d):
+        np.testing.assert_array_equal(idx[a], golden[p + f"index{a}"])
+        np.testing.assert_allclose(val[a], golden[p + f"value{a}"], rtol=2e-7)
+    F = coord.shape[0]
+    sp = orc.spread(golden[p + "noncart"], idx, val, tuple(os_))
+    assert orc.rel_l2(sp, golden[p + "spread"]) < 1e-6
+    it = orc.interp(golden[p + "grid_in"], idx, val, tuple(os_), F)
+    assert orc.rel_l2(it, golden[p + "interp"]) < 1e-6
+    basis = golden[p + "basis"]
+    sps = orc.spread(golden[p + "noncart"], idx, val, tuple(os_), np.ascontiguousarray(basis.conj().T))
+    assert orc.rel_l2(sps, golden[p + "spread_sub"]) < 1e-6
+    its = orc.interp(golden[p + "grid_in_sub"], idx, val, tuple(os_), F, basis)
+    assert orc.rel_l2(its, golden[p + "interp_sub"]) < 1e-6
+
+
+def _radial(nspokes, nread, N, seed=0):
+    ga = np.pi / ((1 + 5 ** 0.5) / 2)
+    ang = np.arange(nspokes) * ga
+    kr = (np.arange(nread) - nread // 2) / nread * N
+    c = np.stack([np.cos(ang)[:, None] * kr, np.sin(ang)[:, None] * kr], -1)
+    return c.astype(np.float32)
+
+
+@pytest.mark.parametrize("osf,w,tol", [(2.0, 4, 2e-3), (1.25, 4, 2e-2), (2.0, 6, 1e-4)])
+def test_oracle_nufft_vs_nudft(osf, w, tol):
+    rng = np.random.default_rng(1)
+    N = 32
+    coord = _radial(24, 48, N)
+    x = (rng.standard_normal((2, N, N)) + 1j * rng.standard_normal((2, N, N))).astype(np.complex64)
+    plan = orc.plan_nufft(coord, (N, N), width=w, oversamp=osf)
+    y = orc.nufft_fwd(x, plan)
+    y_ref = orc.nudft_fwd(x, coord.reshape(-1, 2), (N, N)).reshape(y.shape)
+    assert orc.rel_l2(y, y_ref) < tol
+    G = float(np.prod(plan.os_shape))
+    xa = orc.nufft_adj(y_ref.astype(np.complex64), plan) * G
+    xa_ref = orc.nudft_adj(y_ref.reshape(2, -1), coord.reshape(-1, 2), (N, N))
+    assert orc.rel_l2(xa, xa_ref) < tol
+
+
+def test_oracle_adjointness_ortho():
+    rng = np.random.default_rng(2)
+    N = 24
+    coord = _radial(16, 40, N)
+    plan = orc.plan_nufft(coord, (N, N), width=4, oversamp=2.0)
+    x = (rng.standard_normal((3, N, N)) + 1j * rng.standard_normal((3, N, N))).astype(np.complex64)
+    y = (rng.standard_normal((3, 16, 40)) + 1j * rng.standard_normal((3, 16, 40))).astype(np.complex64)
+    lhs = np.vdot(y, orc.nufft_fwd(x, plan, norm="ortho"))
+    rhs = np.vdot(orc.nufft_adj(y, plan, norm="ortho"), x)
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+
+
+def test_oracle_3d_vs_nudft():
+    rng = np.random.default_rng(3)
+    N = (10, 12, 14)
+    M = 300
+    coord = ((rng.random((M, 3)) - 0.5) * np.array(N[::-1])).astype(np.float32)
+    x = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    plan = orc.plan_nufft(coord, N, width=6, oversamp=2.0)
+    y = orc.nufft_fwd(x, plan)
+    y_ref = orc.nudft_fwd(x, coord, N)
+    assert orc.rel_l2(y, y_ref) < 1e-4
+
+
+def test_oracle_gram_exact_matches_ahwa():
+    rng = np.random.default_rng(4)
+    N = 20
+    coord = _radial(12, 40, N)
+    wgt = rng.random(coord.shape[:-1]).astype(np.float32)
+    gm = orc.plan_spgram(coord, (N, N), weight=wgt, normalize=None)
+    x = (rng.standard_normal((2, N, N)) + 1j * rng.standard_normal((2, N, N))).astype(np.complex64)
+    g = orc.sparse_gram(x, gm)
+    ref = orc.nudft_adj(wgt.ravel() * orc.nudft_fwd(x, coord.reshape(-1, 2), (N, N)),
+                        coord.reshape(-1, 2), (N, N))
+    assert orc.rel_l2(g, ref) < 1e-3
+
+
+def test_oracle_gram_subspace_exact():
+    rng = np.random.default_rng(5)
+    N, F, K = 16, 6, 3
+    coord = np.stack([_radial(6, 32, N) @ np.array([[np.cos(a), -np.sin(a)], [np.sin(a), np.cos(a)]],
+                                                   np.float32) for a in np.linspace(0, 1, F)])
+    basis = np.linalg.qr(rng.standard_normal((F, K)) + 1j * rng.standard_normal((F, K)))[0].astype(np.complex64)
+    gm = orc.plan_spgram(coord, (N, N), basis=basis, normalize=None)
+    x = (rng.standard_normal((2, K, N, N)) + 1j * rng.standard_normal((2, K, N, N))).astype(np.complex64)
+    g = orc.sparse_gram(x, gm)
+    # A: x_k -> y_f = sum_k basis[f,k] NUDFT_f(x_k); A^H: y -> sum_f conj(basis[f,k]) NUDFT_f^H y_f
+    ref = np.zeros_like(g, dtype=np.complex128)
+    for f in range(F):
+        cf = coord[f].reshape(-1, 2)
+        yf = sum(basis[f, k] * orc.nudft_fwd(x[:, k], cf, (N, N)) for k in range(K))
+        af = orc.nudft_adj(yf, cf, (N, N))
+        for k in range(K):
+            ref[:, k] += np.conj(basis[f, k]) * af
+    assert orc.rel_l2(g, ref) < 1e-3
+
+
+def test_oracle_b0_segmentation_vs_exact():
+    rng = np.random.default_rng(6)
+    N, nv, ns = 24, 12, 64
+    coord = _radial(nv, ns, N)
+    yy, xx = np.mgrid[:N, :N] / N - 0.5
+    b0 = (120 * np.exp(-((xx - 0.1) ** 2 + yy ** 2) / 0.05) - 60 * np.exp(-((xx + 0.2) ** 2 + (yy - 0.2) ** 2) / 0.02))
+    dt = 5e-3 / ns
+    t = dt * np.arange(ns)
+    plan = orc.plan_nufft(coord, (N, N), width=6, oversamp=2.0, zmap=b0, L=8, nbins=40, dt=dt)
+    x = (rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))).astype(np.complex64)
+    y = orc.nufft_fwd(x, plan)
+    # exact: y(m) = sum_r x(r) exp(-2 pi i b0(r) t(m)) exp(-2 pi i k.r / N)
+    r = orc.pixel_grid((N, N))
+    cm = coord.reshape(-1, 2).astype(np.float64)
+    tm = np.tile(t, nv)
+    E = np.exp(-2j * np.pi * (cm / N) @ r.T) * np.exp(-2j * np.pi * tm[:, None] * b0.ravel()[None, :])
+    y_ref = (E @ x.ravel().astype(np.complex128)).reshape(nv, ns)
+    assert orc.rel_l2(y, y_ref) < 2e-3
