@@ -82,7 +82,7 @@ def coil_maps_3d(torch, N, ncoils, device):
     maps = []
     for c in range(ncoils):
         d2 = (xx - cen[c, 0]) ** 2 + (yy - cen[c, 1]) ** 2 + (zz - cen[c, 2]) ** 2
-        ph = torch.exp(1j * 2 * math.pi * (c / ncoils))
+        ph = complex(math.cos(2 * math.pi * c / ncoils), math.sin(2 * math.pi * c / ncoils))
         maps.append((torch.exp(-d2 / (2 * 0.4 ** 2)) * ph).to(torch.complex64))
     m = torch.stack(maps)
     rss = torch.sqrt(torch.sum(torch.abs(m) ** 2, 0, keepdim=True))

@@ -28,20 +28,28 @@ def build(force=False, verbose=False, extra_flags=()):
     if nvcc is None:
         raise RuntimeError("nvcc not found; set CUDA_HOME")
     cuda_home = os.path.dirname(os.path.dirname(nvcc))
-    cmd = [
-        nvcc, "-O3", "-std=c++17", "-lineinfo",
-        "-gencode", "arch=compute_100a,code=sm_100a",
-        "-Xcompiler", "-fPIC", "-shared", "-cudart", "static",
-        "--expt-relaxed-constexpr",
-        "-I", os.path.join(ROOT, "include"),
-        *extra_flags,
-        "-o", LIB + ".tmp", *srcs,
-        "-L", os.path.join(cuda_home, "lib64"), "-lcufft",
-        "-Xlinker", "-rpath," + os.path.join(cuda_home, "lib64"),
-    ]
+    flags = ["-O3", "-std=c++17", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
+             "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include"),
+             *extra_flags]
+    objdir = os.path.join(HERE, "_objs")
+    os.makedirs(objdir, exist_ok=True)
+    procs, objs = [], []
+    for src in srcs:
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        cmd = [nvcc, *flags, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        procs.append((src, subprocess.Popen(cmd)))
+    failed = [src for src, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed for {failed}")
+    link = [nvcc, "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a",
+            "-o", LIB + ".tmp", *objs, "-L", os.path.join(cuda_home, "lib64"), "-lcufft",
+            "-Xlinker", "-rpath," + os.path.join(cuda_home, "lib64")]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -70,8 +70,9 @@ class Interpolator:
 
     def __init__(self, coord, frame_offsets, readout_len, dshape, shape, os_shape, width, beta,
                  is_cart, device, tile=None):
+        self._handle = None
         self.ndim = int(coord.shape[-1])
-        self.dshape = tuple(dshape)
+        self.dshape = tuple(dshape) if dshape is not None else None
         self.ishape = tuple(int(s) for s in os_shape)
         self.shape = tuple(int(s) for s in shape)
         self.width = tuple(int(w) for w in width)
@@ -84,7 +85,6 @@ class Interpolator:
         self.device = torch.device(device)
         self._coord = coord  # float32 (total, ndim) on device, kept for rebuilds
         self._tile = tile
-        self._handle = None
         self._build()
 
     def _build(self):

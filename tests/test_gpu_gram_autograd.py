@@ -218,7 +218,7 @@ def test_traj_and_image_grad_vs_fp64_nudft_autograd():
     c64 = torch.as_tensor(coord.reshape(-1, 2), dtype=torch.float64).requires_grad_(True)
     x64 = torch.as_tensor(x, dtype=torch.complex128).requires_grad_(True)
     r = torch.as_tensor(orc.pixel_grid((N, N)))
-    E = torch.exp(-2j * math.pi * (c64 / N) @ r.T) / math.sqrt(G)
+    E = torch.exp(-2j * math.pi * ((c64 / N) @ r.T)) / math.sqrt(G)
     y64 = E @ x64.flatten()
     z64 = (E.conj().T @ y64).reshape(N, N)
     loss64 = torch.sum(torch.abs(z64 - x64) ** 2)

@@ -49,8 +49,8 @@ def test_tables_edge_coords(golden, w, osf):
     plan = _plan(c[None, None, :, None], (N,), (osf,), (w,))
     idx, val = plan.interpolator.tables(0)
     tag = f"tab_w{w}_os{osf}"
-    np.testing.assert_array_equal(idx.cpu().numpy()[0], golden[tag + "_index"])
-    np.testing.assert_allclose(val.cpu().numpy()[0], golden[tag + "_value"], rtol=3e-6, atol=1e-7)
+    np.testing.assert_array_equal(idx.cpu().numpy(), golden[tag + "_index"])
+    np.testing.assert_allclose(val.cpu().numpy(), golden[tag + "_value"], rtol=3e-6, atol=1e-7)
 
 
 @pytest.mark.parametrize("d", [1, 2, 3])

@@ -100,7 +100,8 @@ def test_all_samples_in_one_tile_and_chunking():
     """A crowded bin (k-space centre hot spot) split into several work items."""
     rng = np.random.default_rng(5)
     N = 64
-    coord = ((rng.random((1, 4000, 2)) - 0.5) * 3.0).astype(np.float32)
+    # every first tap x0 = ceil(2c + 62) in [56, 63]: one 32-wide tile on both axes
+    coord = ((rng.random((1, 4000, 2)) - 1.0) * 3.0 + 0.49).astype(np.float32)
     gplan = check_pair(coord, (N, N), crandn(rng, 3, N, N), crandn(rng, 3, 1, 4000), oversamp=2.0)
     assert gplan.interpolator.max_bin >= 3000
 
