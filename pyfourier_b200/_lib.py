@@ -29,7 +29,7 @@ EXPORTS = (
     "pfb_plan_set_tuning", "pfb_plan_set_chunk", "pfb_plan_tables", "pfb_workspace_size",
     "pfb_nufft_fwd", "pfb_nufft_adj", "pfb_spread", "pfb_interp", "pfb_deapod_pad",
     "pfb_crop_deapod", "pfb_grid_fft", "pfb_traj_grad", "pfb_gram_create", "pfb_gram_destroy",
-    "pfb_gram_workspace_size", "pfb_gram_apply",
+    "pfb_gram_workspace_size", "pfb_gram_apply", "pfb_nufft_adj_noalloc",
 )
 
 
@@ -109,6 +109,7 @@ def load(path=LIB_PATH):
         "pfb_gram_destroy": (i32, [vp]),
         "pfb_gram_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),
         "pfb_gram_apply": (i32, [vp, vp, vp, i64, vp, ctypes.c_size_t, vp]),
+        "pfb_nufft_adj_noalloc": (i32, [vp, P(ApplyT), vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
