@@ -92,6 +92,9 @@ def coil_maps_3d(torch, N, ncoils, device):
 WORKLOADS = {
     "cfg2": dict(desc="3D golden-means radial NUFFT fwd+adj", N=200, nspokes=20000, nread=400, coils=32,
                  width=4, oversamp=1.25, nell=20),
+    # mid-size variant for profiler captures (grid 8 x 160^3 complex64 = 262 MB > L2)
+    "cfg2-mid": dict(desc="3D golden-means radial NUFFT fwd+adj (mid)", N=128, nspokes=8000, nread=256,
+                     coils=8, width=4, oversamp=1.25, nell=20),
     # reduced variant for quick checks (same construction)
     "cfg2-small": dict(desc="3D golden-means radial NUFFT fwd+adj (reduced)", N=64, nspokes=2000, nread=128,
                        coils=8, width=4, oversamp=1.25, nell=20),
@@ -184,7 +187,8 @@ def cpu_baseline(wl, coord, coils_sample, steps=1):
 # GPU arm
 # --------------------------------------------------------------------------------------
 def stage_times(torch, pf, plan, x, iters):
-    """Per-kernel CUDA-event timings of one forward + adjoint, via the C ABI stages."""
+    """Per-kernel CUDA-event timings of one forward + adjoint, stage by stage
+    through the C ABI (pfb_nufft_stage), on the launching stream."""
     import ctypes
 
     from pyfourier_b200 import _lib
@@ -195,28 +199,19 @@ def stage_times(torch, pf, plan, x, iters):
     B = x.shape[0]
     o = ctx.opts(B, (0, 1))
     h = plan.interpolator.handle
-    nplanes = B * ctx.C
-    ws = ctx.workspace(nplanes)
-    gbytes = nplanes * int(np.prod(plan.os_shape)) * 8
-    goff = (gbytes + 255) // 256 * 256
-    grid = ws[:gbytes]
-    work = ws[goff:]
+    ws = ctx.workspace(o)
     y = torch.empty((B, plan.interpolator.total_samples), dtype=torch.complex64, device=x.device)
     xa = torch.empty_like(x)
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-    P = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
-    fac_f = ctx.fac_fwd
-    fac_a = ctx.fac_adj
-    stages = {
-        "deapod_pad": lambda: L.pfb_deapod_pad(h, ctypes.byref(o), P(x), P(grid), ctypes.c_float(fac_f), st),
-        "fft_fwd": lambda: L.pfb_grid_fft(h, P(grid), nplanes, -1, P(work), work.numel(), st),
-        "interp": lambda: L.pfb_interp(h, ctypes.byref(o), P(grid), P(y), 1, st),
-        "spread": lambda: L.pfb_spread(h, ctypes.byref(o), P(y), P(grid), 1, st),
-        "fft_adj": lambda: L.pfb_grid_fft(h, P(grid), nplanes, 1, P(work), work.numel(), st),
-        "crop_deapod": lambda: L.pfb_crop_deapod(h, ctypes.byref(o), P(grid), P(xa), ctypes.c_float(fac_a), st),
-    }
+    P = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
+    order = [("pad", x, None, ctx.fac_fwd), ("fft", None, None, 1.0), ("transpose", None, None, 1.0),
+             ("interp", None, None, 1.0),
+             ("out", None, y, 1.0), ("vals", y, None, 1.0), ("spread", None, None, 1.0),
+             ("ifft", None, None, 1.0), ("crop", None, xa, ctx.fac_adj)]
     out = {}
-    for name, fn in stages.items():
+    for name, src, dst, fac in order:
+        fn = lambda: L.pfb_nufft_stage(h, ctypes.byref(o), _lib.STAGES[name], P(src), P(dst),  # noqa: E731
+                                       ctypes.c_float(fac), P(ws), ws.numel(), st)
         _lib.check(fn())
         torch.cuda.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(iters)]
@@ -230,16 +225,20 @@ def stage_times(torch, pf, plan, x, iters):
 
 
 def algorithmic_bytes(wl, plan, B):
+    """Bytes each kernel must move at minimum (inputs read once, outputs written once)."""
     M = plan.interpolator.total_samples
     G = int(np.prod(plan.os_shape))
     Nv = int(np.prod(plan.shape))
     nd = plan.ndim
     coords = M * (4 * nd + 4 + 4)  # sorted coords, permutation, frame index
     return {
-        "interp": B * G * 8 + B * M * 8 + coords,       # grid read once, samples written
-        "spread": B * M * 8 + B * G * 8 + coords,       # samples read, grid written once
-        "deapod_pad": B * Nv * 8 + B * G * 8,            # image read, padded grid written
-        "crop_deapod": B * Nv * 8 + B * Nv * 8,          # image region of the grid read, image written
+        "interp": B * G * 8 + B * M * 8 + coords,   # grid read once, per-channel results written
+        "out": 2 * B * M * 8,                        # results read, k-space written
+        "vals": 2 * B * M * 8,                       # k-space read, per-channel values written
+        "spread": B * M * 8 + B * G * 8 + coords,   # values read, grid written once
+        "pad": B * Nv * 8 + B * G * 8,               # image read, padded grid written
+        "transpose": 2 * B * G * 8,                  # planar grid read, interleaved grid written
+        "crop": B * Nv * 8 + B * Nv * 8,             # image region of the grid read, image written
     }
 
 
@@ -324,7 +323,226 @@ def gpu_arm(args, wl, rank, world, local_rank):
                 "traffic": NCU_TRAFFIC.get((args.workload, dom)),
                 "algorithmic_bytes": alg[dom]}
     return dict(ms=ms, value=value, e2e=world * samples_per_step / e2e_s, h2d=h2d, d2h=d2h, stages=stages,
-                roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=4)
+                roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=8)
+
+
+# --------------------------------------------------------------------------------------
+# further configurations (each prints its own JSON line with the same keys)
+# --------------------------------------------------------------------------------------
+def radial_2d(nspokes, nread, N, start=0):
+    """Golden-angle radial spokes (angle step pi / golden ratio), k in [-N/2, N/2)."""
+    ga = np.pi / ((1 + 5 ** 0.5) / 2)
+    ang = (start + np.arange(nspokes)) * ga
+    kr = (np.arange(nread) - nread // 2) / nread * N
+    return np.stack([np.cos(ang)[:, None] * kr, np.sin(ang)[:, None] * kr], -1).astype(np.float32)
+
+
+def vd_spiral(ninter, nsamp, N, turns=12, rot=0.0):
+    """Variable-density spiral: r = (N/2 - 1) tau^1.5, theta = 2 pi turns tau + 2 pi i / ninter + rot."""
+    tau = np.linspace(0, 1, nsamp)
+    r = (N / 2 - 1) * tau ** 1.5
+    out = []
+    for i in range(ninter):
+        th = 2 * np.pi * turns * tau + 2 * np.pi * i / ninter + rot
+        out.append(np.stack([r * np.cos(th), r * np.sin(th)], -1))
+    return np.stack(out).astype(np.float32)
+
+
+def maps_2d(torch, N, ncoils, dev):
+    ax = (torch.arange(N, dtype=torch.float32, device=dev) - N // 2) / N
+    yy, xx = torch.meshgrid(ax, ax, indexing="ij")
+    maps = []
+    for c in range(ncoils):
+        a = 2 * math.pi * c / ncoils
+        d2 = (xx - 0.4 * math.cos(a)) ** 2 + (yy - 0.4 * math.sin(a)) ** 2
+        maps.append(torch.exp(-d2 / (2 * 0.4 ** 2)).to(torch.complex64) * complex(math.cos(a), math.sin(a)))
+    m = torch.stack(maps)
+    return (m / torch.sqrt(torch.sum(torch.abs(m) ** 2, 0, keepdim=True))).to(torch.complex64)
+
+
+def phantom_2d(torch, N, dev, seed=0, nell=10):
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    ax = (torch.arange(N, dtype=torch.float32, device=dev) - N // 2) / N
+    yy, xx = torch.meshgrid(ax, ax, indexing="ij")
+    img = torch.zeros((N, N), dtype=torch.complex64, device=dev)
+    for _ in range(nell):
+        c = (torch.rand(2, generator=g) - 0.5) * 0.6
+        r = 0.05 + 0.25 * torch.rand(2, generator=g)
+        amp = complex(float(torch.randn(1, generator=g)), float(torch.randn(1, generator=g)))
+        img += amp * ((((xx - c[0]) / r[0]) ** 2 + ((yy - c[1]) / r[1]) ** 2) <= 1)
+    return img
+
+
+def smooth_field(N, seed=0, max_hz=200.0):
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[:N, :N] / N - 0.5
+    f = np.zeros((N, N))
+    for _ in range(6):
+        c = rng.uniform(-0.3, 0.3, 2)
+        s = rng.uniform(0.1, 0.3)
+        f += rng.uniform(-1, 1) * np.exp(-((xx - c[0]) ** 2 + (yy - c[1]) ** 2) / (2 * s ** 2))
+    return (f / np.abs(f).max() * max_hz).astype(np.float32)
+
+
+def exp_recovery_basis(K, nt=48, ncurves=500, seed=0):
+    rng = np.random.default_rng(seed)
+    t = np.linspace(10.0, 3000.0, nt)                 # ms
+    T1 = rng.uniform(200.0, 2000.0, ncurves)          # ms
+    curves = 1 - 2 * np.exp(-t[None, :] / T1[:, None])
+    _, _, vh = np.linalg.svd(curves, full_matrices=False)
+    return vh[:K].T.astype(np.complex64)              # (nt, K), orthonormal columns
+
+
+def time_device(torch, fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def extra_workload(args):
+    """2D radial (cfg1), Toeplitz Gram (cfg3), B0 plain vs batched (cfg4), autograd (cfg5)."""
+    import torch
+
+    import pyfourier_b200 as pf
+    from oracle import nufft_oracle as orc
+
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    line = {"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex64", "data": "synthetic (seeded)"}
+    clocks = ClockSampler(0)
+    if args.workload == "cfg1":
+        N, B = 128, 8
+        coord = radial_2d(201, 256, N)
+        plan = pf.plan_nufft(torch.as_tensor(coord, device=dev), (N, N), width=4, oversamp=2.0, device=dev)
+        x = (maps_2d(torch, N, B, dev) * phantom_2d(torch, N, dev)[None]).contiguous()
+        step = lambda: pf.nufft_adj(pf.nufft(x, nufft_plan=plan), nufft_plan=plan)  # noqa: E731
+        clocks.start()
+        ms = time_device(torch, step, args.steps, args.warmup)
+        clk = clocks.stop()
+        M = 201 * 256
+        value = B * M / (ms / 1e3)
+        oplan = orc.plan_nufft(coord, (N, N), width=4, oversamp=2.0)
+        xc = x.cpu().numpy()
+        orc.nufft_adj(orc.nufft_fwd(xc, oplan), oplan)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            orc.nufft_adj(orc.nufft_fwd(xc, oplan), oplan)
+        cpu_s = (time.perf_counter() - t0) / 3
+        line.update(metric="NUFFT fwd+adj non-uniform samples/s (2D golden-angle radial, 8 coils)", value=value,
+                    unit="samples/s", ms_per_step=ms,
+                    config={"workload": "2D radial NUFFT fwd+adj", "image": [N, N], "coils": B, "spokes": 201,
+                            "readout": 256, "oversamp": 2.0, "width": 4, "l2": "fits in L2 (4 MB grids)"},
+                    cpu_baseline={"value": B * M / cpu_s, "unit": "samples/s", "cores": orc.lib().orc_num_threads(),
+                                  "kind": "port", "sample": "all 8 coils, median of 3 fwd+adj"})
+    elif args.workload == "cfg3":
+        N, B, F, K = 220, 16, 48, 4
+        coord = np.stack([vd_spiral(16, 2048, N, rot=f * np.pi * (3 - 5 ** 0.5)) for f in range(F)])
+        basis = exp_recovery_basis(K, nt=F)
+        t0 = time.perf_counter()
+        gm = pf.plan_spgram(torch.as_tensor(coord, device=dev), (N, N), basis=torch.as_tensor(basis, device=dev),
+                            device=dev)
+        torch.cuda.synchronize()
+        plan_s = time.perf_counter() - t0
+        g = torch.Generator(device="cpu").manual_seed(0)
+        x = torch.complex(torch.randn(B, K, N, N, generator=g), torch.randn(B, K, N, N, generator=g)).to(dev)
+        step = lambda: pf.sparse_gram(x, gm)  # noqa: E731
+        clocks.start()
+        ms = time_device(torch, step, args.steps, args.warmup)
+        clk = clocks.stop()
+        og = orc.plan_spgram(coord, (N, N), basis=basis)
+        xc = x.cpu().numpy()
+        orc.sparse_gram(xc, og)
+        t1 = time.perf_counter()
+        orc.sparse_gram(xc, og)
+        cpu_s = time.perf_counter() - t1
+        line.update(metric="Toeplitz Gram applies/s (2D VD spiral, K=4 subspace, 16 coils)", value=1e3 / ms,
+                    unit="applies/s", ms_per_step=ms,
+                    config={"workload": "Toeplitz Gram with per-voxel 4x4 mixing", "image": [N, N], "coils": B,
+                            "frames": F, "interleaves": 16, "samples_per_interleave": 2048, "K": K,
+                            "embedding": [2 * N, 2 * N], "plan_seconds": round(plan_s, 3)},
+                    cpu_baseline={"value": 1.0 / cpu_s, "unit": "applies/s", "cores": orc.lib().orc_num_threads(),
+                                  "kind": "port", "sample": "one full apply (NumPy einsum + pocketfft)"})
+    elif args.workload == "cfg4":
+        N, B, F, Lseg, nread = 192, 12, 64, 8, 256
+        rng = np.random.default_rng(0)
+        nsp = rng.integers(5, 56, F)
+        starts = np.concatenate([[0], np.cumsum(nsp)[:-1]])
+        frames = [radial_2d(int(n), nread, N, start=int(s0)) for n, s0 in zip(nsp, starts)]
+        b0 = smooth_field(N)
+        dt = 5e-3 / nread
+        kw = dict(width=4, oversamp=1.25, zmap=torch.as_tensor(b0, device=dev), L=Lseg, nbins=40, dt=dt, device=dev)
+        plans = [pf.plan_nufft(torch.as_tensor(c, device=dev), (N, N), **kw) for c in frames]
+        bplan = pf.plan_nufft([torch.as_tensor(c, device=dev) for c in frames], (N, N), **kw)
+        maps = maps_2d(torch, N, B, dev)
+        x = torch.stack([maps * phantom_2d(torch, N, dev, seed=f)[None] for f in range(F)], 1).contiguous()
+        Mtot = int(nsp.sum()) * nread
+
+        def plain():
+            for f in range(F):
+                pf.nufft_adj(pf.nufft(x[:, f], nufft_plan=plans[f]), nufft_plan=plans[f])
+
+        def batched():
+            return pf.nufft_adj(pf.nufft(x, nufft_plan=bplan), nufft_plan=bplan)
+
+        ms_plain = time_device(torch, plain, args.steps, args.warmup)
+        ms_batch = time_device(torch, batched, args.steps, args.warmup)
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(2):
+                batched()
+        torch.cuda.current_stream().wait_stream(s)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            batched()
+        clocks.start()
+        ms_graph = time_device(torch, graph.replay, args.steps, args.warmup)
+        clk = clocks.stop()
+        value = B * Mtot / (ms_graph / 1e3)
+        line.update(metric="B0-corrected NUFFT fwd+adj samples/s, batched graph-captured (2D radial, 64 uneven frames)",
+                    value=value, unit="samples/s", ms_per_step=ms_graph,
+                    config={"workload": "B0 time-segmented dynamic radial fwd+adj", "image": [N, N], "coils": B,
+                            "frames": F, "spokes_per_frame": [int(v) for v in nsp], "readout": nread,
+                            "segments": Lseg, "oversamp": 1.25, "width": 4,
+                            "plain_ms": ms_plain, "batched_ms": ms_batch, "batched_graph_ms": ms_graph,
+                            "plain_samples_per_s": B * Mtot / (ms_plain / 1e3),
+                            "batched_over_plain": ms_plain / ms_graph},
+                    cpu_baseline=None)
+    elif args.workload == "cfg5":
+        N, B, nimg = 256, 8, 32
+        coord = vd_spiral(16, 4096, N)
+        ct = torch.as_tensor(coord, device=dev).requires_grad_(True)
+        plan = pf.plan_nufft(ct.detach(), (N, N), width=4, oversamp=2.0, device=dev)
+        g = torch.Generator(device="cpu").manual_seed(0)
+        x = torch.complex(torch.randn(nimg, B, N, N, generator=g), torch.randn(nimg, B, N, N, generator=g)).to(dev)
+        x.requires_grad_(True)
+
+        def step():
+            y = pf.nufft(x, ct, nufft_plan=plan, norm="ortho")
+            z = pf.nufft_adj(y, ct, nufft_plan=plan, norm="ortho")
+            loss = torch.sum(torch.abs(z - x) ** 2)
+            loss.backward()
+            return loss
+
+        clocks.start()
+        ms = time_device(torch, step, args.steps, args.warmup)
+        clk = clocks.stop()
+        M = 16 * 4096
+        line.update(metric="differentiable NUFFT step samples/s (fwd+adj+backward incl. trajectory gradient)",
+                    value=nimg * B * M / (ms / 1e3), unit="samples/s", ms_per_step=ms,
+                    config={"workload": "loss ||A^H A x - x||^2 with image and trajectory gradients",
+                            "image": [N, N], "coils": B, "images": nimg, "interleaves": 16, "samples": 4096},
+                    cpu_baseline=None)
+    line["clocks"] = clk
+    print(json.dumps(line), flush=True)
 
 
 # DRAM bytes (read + write) per launch from one ncu capture of the named
@@ -338,10 +556,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg1", "cfg3", "cfg4", "cfg5"])
     ap.add_argument("--cpu-coils", type=int, default=2, help="coils in the bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload in ("cfg1", "cfg3", "cfg4", "cfg5"):
+        extra_workload(args)
+        return
     wl = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

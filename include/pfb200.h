@@ -131,6 +131,13 @@ int pfb_plan_tables(const pfb_plan *plan, int axis, int32_t *index, float *value
  * (nplanes = nseg * batch * ncoeff).  May create the cuFFT plan. */
 int pfb_workspace_size(pfb_plan *plan, int64_t nplanes, size_t *bytes);
 
+/* Workspace bytes for pfb_nufft_fwd / pfb_nufft_adj / pfb_nufft_traj_grad with
+ * these options on their fastest path (the channel-interleaved grid plus a
+ * bin-sorted sample buffer).  A workspace of pfb_workspace_size bytes is also
+ * accepted by those calls; they then take the slower planar path.  May create
+ * the cuFFT plan. */
+int pfb_apply_workspace_size(pfb_plan *plan, const pfb_apply_t *opt, size_t *bytes);
+
 /* Forward NUFFT: image (batch, ncoeff, *shape) -> kspace (batch, total samples).
  * Replaces _nufft_fwd / _do_nufft (src/pyfourier/_nufft/_nufft.py:11-90, :218-251):
  * apodize -> zero-pad -> centred FFT -> interpolate / scale, B0 segment sum,
@@ -202,6 +209,41 @@ int pfb_grid_fft(pfb_plan *plan, void *grid, int64_t nplanes, int direction, voi
  * discretised operator.  grad is overwritten. */
 int pfb_traj_grad(pfb_plan *plan, const pfb_apply_t *opt, const void *grid, const void *values,
                   float *grad, int fft_layout, void *stream);
+
+/* Trajectory gradient of a forward NUFFT, from the image side: grad (total, ndim)
+ * float32 = d/dk sum_b Re(conj(A(k) x)_b v_b) where A(k) x is the forward NUFFT
+ * of `image` (batch, ncoeff, *shape) with the deapodisation / scaling `factor`
+ * given here (1/scale, times 1/sqrt(prod(os_shape)) for "ortho"), and v =
+ * `values` (batch, total).  Padding, cuFFT and the gradient kernel in one call;
+ * the kernel weights are recomputed, nothing is stored.  grad is overwritten
+ * (or accumulated with PFB_FLAG_ACCUMULATE). */
+int pfb_nufft_traj_grad(pfb_plan *plan, const pfb_apply_t *opt, const void *image, const void *values,
+                        float *grad, float factor, void *workspace, size_t workspace_bytes, void *stream);
+
+/* One stage of the fast pipelines, for per-kernel timing and for callers that
+ * interleave their own work between stages.  The workspace (of
+ * pfb_apply_workspace_size bytes) carries the intermediates between calls:
+ * forward = PAD, FFT, TRANSPOSE, INTERP, OUT; adjoint = VALS, SPREAD, IFFT, CROP.
+ *   PAD:    src image -> planar grid (deapodised, padded, times `factor`)
+ *   FFT / IFFT: the planar grid in place
+ *   TRANSPOSE: planar grid -> channel-interleaved grid
+ *   INTERP: interleaved grid -> per-channel sample results;  OUT: results -> dst k-space
+ *   VALS:   src k-space -> per-channel sample values;  SPREAD: values -> grid
+ *   CROP:   grid -> dst image (cropped, deapodised, times `factor`)
+ * Stages of the forward path replace _do_nufft's steps
+ * (src/pyfourier/_nufft/_nufft.py:235-246), those of the adjoint _do_nufft_adj's
+ * (:271-282). */
+#define PFB_STAGE_PAD 0
+#define PFB_STAGE_FFT 1
+#define PFB_STAGE_INTERP 2
+#define PFB_STAGE_OUT 3
+#define PFB_STAGE_VALS 4
+#define PFB_STAGE_SPREAD 5
+#define PFB_STAGE_IFFT 6
+#define PFB_STAGE_CROP 7
+#define PFB_STAGE_TRANSPOSE 8
+int pfb_nufft_stage(pfb_plan *plan, const pfb_apply_t *opt, int stage, const void *src, void *dst,
+                    float factor, void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---- Toeplitz Gram (src/pyfourier/_sparsegram) ------------------------------------ */
 

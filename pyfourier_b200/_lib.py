@@ -22,6 +22,8 @@ PFB_ERR_WORKSPACE = 6
 PFB_NORM_NONE = 0
 PFB_NORM_ORTHO = 1
 PFB_FLAG_ACCUMULATE = 1
+STAGES = {"pad": 0, "fft": 1, "interp": 2, "out": 3, "vals": 4, "spread": 5, "ifft": 6, "crop": 7,
+          "transpose": 8}
 
 # Every symbol exported by the C ABI (kept in sync with include/pfb200.h).
 EXPORTS = (
@@ -30,6 +32,7 @@ EXPORTS = (
     "pfb_nufft_fwd", "pfb_nufft_adj", "pfb_spread", "pfb_interp", "pfb_deapod_pad",
     "pfb_crop_deapod", "pfb_grid_fft", "pfb_traj_grad", "pfb_gram_create", "pfb_gram_destroy",
     "pfb_gram_workspace_size", "pfb_gram_apply", "pfb_nufft_adj_noalloc",
+    "pfb_apply_workspace_size", "pfb_nufft_traj_grad", "pfb_nufft_stage",
 )
 
 
@@ -110,6 +113,9 @@ def load(path=LIB_PATH):
         "pfb_gram_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),
         "pfb_gram_apply": (i32, [vp, vp, vp, i64, vp, ctypes.c_size_t, vp]),
         "pfb_nufft_adj_noalloc": (i32, [vp, P(ApplyT), vp, vp, vp]),
+        "pfb_apply_workspace_size": (i32, [vp, P(ApplyT), P(ctypes.c_size_t)]),
+        "pfb_nufft_traj_grad": (i32, [vp, P(ApplyT), vp, vp, vp, f32, vp, ctypes.c_size_t, vp]),
+        "pfb_nufft_stage": (i32, [vp, P(ApplyT), i32, vp, vp, f32, vp, ctypes.c_size_t, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

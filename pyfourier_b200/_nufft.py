@@ -83,10 +83,11 @@ class _Ctx:
         o.flags = flags
         return o
 
-    def workspace(self, nplanes):
+    def workspace(self, opts):
+        """Workspace of the fastest path for these apply options (caching allocator)."""
         n = ctypes.c_size_t()
-        _lib.check(_lib.load().pfb_workspace_size(self.interp.handle, int(nplanes), ctypes.byref(n)))
-        return torch.empty(int(n.value), dtype=torch.uint8, device=self.dev)
+        _lib.check(_lib.load().pfb_apply_workspace_size(self.interp.handle, ctypes.byref(opts), ctypes.byref(n)))
+        return torch.empty(max(int(n.value), 1), dtype=torch.uint8, device=self.dev)
 
 
 def fwd_core(ctx: _Ctx, image):
@@ -99,7 +100,7 @@ def fwd_core(ctx: _Ctx, image):
     st = _stream(ctx.dev)
     for i, seg in enumerate(ctx.segments()):
         o = ctx.opts(B, seg, 0 if i == 0 else _lib.PFB_FLAG_ACCUMULATE)
-        ws = ctx.workspace(o.nseg * B * ctx.C)
+        ws = ctx.workspace(o)
         _lib.check(L.pfb_nufft_fwd(ctx.interp.handle, ctypes.byref(o), _ptr(image), _ptr(out),
                                    _ptr(ws), ws.numel(), st))
     return out
@@ -117,7 +118,7 @@ def adj_core(ctx: _Ctx, kspace):
     st = _stream(ctx.dev)
     for i, seg in enumerate(ctx.segments()):
         o = ctx.opts(B, seg, 0 if i == 0 else _lib.PFB_FLAG_ACCUMULATE)
-        ws = ctx.workspace(o.nseg * B * ctx.C)
+        ws = ctx.workspace(o)
         _lib.check(L.pfb_nufft_adj(ctx.interp.handle, ctypes.byref(o), _ptr(kspace), _ptr(out),
                                    _ptr(ws), ws.numel(), st))
     return out
@@ -137,17 +138,10 @@ def traj_grad_core(ctx: _Ctx, image_side, values, factor):
     st = _stream(ctx.dev)
     for seg in ctx.segments():
         o = ctx.opts(B, seg, _lib.PFB_FLAG_ACCUMULATE)
-        nplanes = o.nseg * B * ctx.C
-        ws = ctx.workspace(nplanes)
-        gbytes = nplanes * int(np.prod(ctx.plan.os_shape)) * 8
-        goff = (gbytes + 255) // 256 * 256
-        grid = ws[:gbytes]
-        _lib.check(L.pfb_deapod_pad(ctx.interp.handle, ctypes.byref(o), _ptr(image_side), _ptr(grid),
-                                    ctypes.c_float(factor), st))
-        work = ws[goff:]
-        _lib.check(L.pfb_grid_fft(ctx.interp.handle, _ptr(grid), nplanes, -1, _ptr(work), work.numel(), st))
-        _lib.check(L.pfb_traj_grad(ctx.interp.handle, ctypes.byref(o), _ptr(grid), _ptr(values),
-                                   ctypes.c_void_p(grad.data_ptr()), 1, st))
+        ws = ctx.workspace(o)
+        _lib.check(L.pfb_nufft_traj_grad(ctx.interp.handle, ctypes.byref(o), _ptr(image_side), _ptr(values),
+                                         ctypes.c_void_p(grad.data_ptr()), ctypes.c_float(factor), _ptr(ws),
+                                         ws.numel(), st))
     return grad
 
 

@@ -34,6 +34,8 @@ struct DeviceGuard {
 constexpr size_t kAlign = 256;
 size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
+}  // namespace
+
 // cuFFT plan over `nplanes` batched grids of extent dims (slowest first).
 int get_fft_plan(std::mutex &mu, std::map<int64_t, cufftHandle> &plans, std::map<int64_t, size_t> &work,
                  int ndim, const int *nos_xyz, int64_t nplanes, cufftHandle *out, size_t *wbytes) {
@@ -75,6 +77,8 @@ int run_fft(cufftHandle h, size_t wbytes, float2 *data, int direction, void *wor
                                direction < 0 ? CUFFT_FORWARD : CUFFT_INVERSE));
     return PFB_OK;
 }
+
+namespace {
 
 int to_desc(const pfb_plan *p, const pfb_apply_t *o, ApplyDesc &d) {
     if (!o) return fail(PFB_ERR_INVALID, "apply options are NULL");
@@ -230,13 +234,18 @@ int pfb_nufft_fwd(pfb_plan *p, const pfb_apply_t *opt, const void *image, void *
     cufftHandle h;
     size_t wb = 0;
     if ((st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, &h, &wb))) return st;
+    // forward: unnormalised FFT ("ortho": 1/sqrt(G)), and 1/scale of _cart2noncart:110
+    double fac = 1.0 / p->scale;
+    if (d.norm == PFB_NORM_ORTHO) fac /= std::sqrt((double)p->g.gvol);
+    // channel-interleaved path when the workspace holds it, else the planar path
+    size_t fast_bytes = 0;
+    if (fast_supported(p, d, nullptr) && fast_workspace(p, d, &fast_bytes) == PFB_OK && workspace_bytes >= fast_bytes)
+        return fast_fwd(p, d, static_cast<const float2 *>(image), static_cast<float2 *>(kspace), workspace,
+                        workspace_bytes, (float)fac, opt->flags & PFB_FLAG_ACCUMULATE, s);
     size_t gbytes = align_up((size_t)P * p->g.gvol * sizeof(float2));
     if (workspace_bytes < gbytes + wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
     float2 *grid = static_cast<float2 *>(workspace);
     void *work = static_cast<char *>(workspace) + gbytes;
-    // forward: unnormalised FFT ("ortho": 1/sqrt(G)), and 1/scale of _cart2noncart:110
-    double fac = 1.0 / p->scale;
-    if (d.norm == PFB_NORM_ORTHO) fac /= std::sqrt((double)p->g.gvol);
     if ((st = launch_deapod_pad(p, d, static_cast<const float2 *>(image), grid, (float)fac, s))) return st;
     if ((st = run_fft(h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
     return launch_interp(p, d, grid, static_cast<float2 *>(kspace), true, s, opt->flags & PFB_FLAG_ACCUMULATE);
@@ -255,17 +264,85 @@ int pfb_nufft_adj(pfb_plan *p, const pfb_apply_t *opt, const void *kspace, void 
     cufftHandle h;
     size_t wb = 0;
     if ((st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, &h, &wb))) return st;
+    // adjoint: inverse FFT scaled 1/G (None) or 1/sqrt(G) (ortho), and 1/scale of _noncart2cart:119
+    double fac = 1.0 / p->scale;
+    fac /= (d.norm == PFB_NORM_ORTHO) ? std::sqrt((double)p->g.gvol) : (double)p->g.gvol;
+    size_t fast_bytes = 0;
+    if (fast_supported(p, d, nullptr) && fast_workspace(p, d, &fast_bytes) == PFB_OK && workspace_bytes >= fast_bytes)
+        return fast_adj(p, d, static_cast<const float2 *>(kspace), static_cast<float2 *>(image), workspace,
+                        workspace_bytes, (float)fac, opt->flags & PFB_FLAG_ACCUMULATE, s);
     size_t gbytes = align_up((size_t)P * p->g.gvol * sizeof(float2));
     if (workspace_bytes < gbytes + wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
     float2 *grid = static_cast<float2 *>(workspace);
     void *work = static_cast<char *>(workspace) + gbytes;
-    // adjoint: inverse FFT scaled 1/G (None) or 1/sqrt(G) (ortho), and 1/scale of _noncart2cart:119
-    double fac = 1.0 / p->scale;
-    fac /= (d.norm == PFB_NORM_ORTHO) ? std::sqrt((double)p->g.gvol) : (double)p->g.gvol;
     if ((st = launch_spread(p, d, static_cast<const float2 *>(kspace), grid, true, s))) return st;
     if ((st = run_fft(h, wb, grid, +1, work, workspace_bytes - gbytes, s))) return st;
     return launch_crop_deapod(p, d, grid, static_cast<float2 *>(image), (float)fac, s,
                               opt->flags & PFB_FLAG_ACCUMULATE);
+}
+
+int pfb_apply_workspace_size(pfb_plan *p, const pfb_apply_t *opt, size_t *bytes) {
+    if (!p || !bytes) return fail(PFB_ERR_INVALID, "NULL argument");
+    DeviceGuard dg(p->device);
+    ApplyDesc d;
+    int st = to_desc(p, opt, d);
+    if (st) return st;
+    if (d.batch == 0) {
+        *bytes = 0;
+        return PFB_OK;
+    }
+    if (fast_supported(p, d, nullptr)) return fast_workspace(p, d, bytes);
+    cufftHandle h;
+    size_t wb = 0;
+    int64_t P = planes_of(d);
+    if ((st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, &h, &wb))) return st;
+    *bytes = align_up((size_t)P * p->g.gvol * sizeof(float2)) + align_up(wb);
+    return PFB_OK;
+}
+
+int pfb_nufft_traj_grad(pfb_plan *p, const pfb_apply_t *opt, const void *image, const void *values, float *grad,
+                        float factor, void *workspace, size_t workspace_bytes, void *stream) {
+    if (!p || !image || !values || !grad || !workspace) return fail(PFB_ERR_INVALID, "NULL argument");
+    DeviceGuard dg(p->device);
+    ApplyDesc d;
+    int st = to_desc(p, opt, d);
+    if (st) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool acc = opt->flags & PFB_FLAG_ACCUMULATE;
+    if (d.batch == 0 || p->mtot == 0) {
+        if (!acc && p->mtot > 0) PFB_CUDA_TRY(cudaMemsetAsync(grad, 0, p->mtot * p->g.ndim * sizeof(float), s));
+        return PFB_OK;
+    }
+    size_t fast_bytes = 0;
+    if (fast_supported(p, d, nullptr) && fast_workspace(p, d, &fast_bytes) == PFB_OK && workspace_bytes >= fast_bytes)
+        return fast_traj_grad(p, d, static_cast<const float2 *>(image), static_cast<const float2 *>(values), grad,
+                              workspace, workspace_bytes, factor, acc, s);
+    int64_t P = planes_of(d);
+    cufftHandle h;
+    size_t wb = 0;
+    if ((st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, &h, &wb))) return st;
+    size_t gbytes = align_up((size_t)P * p->g.gvol * sizeof(float2));
+    if (workspace_bytes < gbytes + wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
+    float2 *grid = static_cast<float2 *>(workspace);
+    void *work = static_cast<char *>(workspace) + gbytes;
+    if ((st = launch_deapod_pad(p, d, static_cast<const float2 *>(image), grid, factor, s))) return st;
+    if ((st = run_fft(h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
+    return launch_traj_grad(p, d, grid, static_cast<const float2 *>(values), grad, true, s, acc);
+}
+
+int pfb_nufft_stage(pfb_plan *p, const pfb_apply_t *opt, int stage, const void *src, void *dst, float factor,
+                    void *workspace, size_t workspace_bytes, void *stream) {
+    if (!p || !workspace) return fail(PFB_ERR_INVALID, "NULL argument");
+    DeviceGuard dg(p->device);
+    ApplyDesc d;
+    int st = to_desc(p, opt, d);
+    if (st) return st;
+    if (d.batch == 0) return PFB_OK;
+    if (!fast_supported(p, d, nullptr)) return fail(PFB_ERR_UNSUPPORTED, "options outside the interleaved path");
+    if ((stage == PFB_STAGE_PAD || stage == PFB_STAGE_VALS) && !src) return fail(PFB_ERR_INVALID, "src is NULL");
+    if ((stage == PFB_STAGE_OUT || stage == PFB_STAGE_CROP) && !dst) return fail(PFB_ERR_INVALID, "dst is NULL");
+    return fast_stage(p, d, stage, src, dst, workspace, workspace_bytes, factor, opt->flags & PFB_FLAG_ACCUMULATE,
+                      static_cast<cudaStream_t>(stream));
 }
 
 int pfb_spread(pfb_plan *p, const pfb_apply_t *opt, const void *kspace, void *grid, int fft_layout, void *stream) {

@@ -65,6 +65,15 @@ struct SpreadItem {
     int begin, end, bin, frame;
 };
 
+// Work item of the owner-computes spread: output tile `tile` (of frame
+// `frame`, or all frames when < 0) gathers the samples of its 2^d lower
+// neighbour bins, virtual positions [v0, v1) of their concatenation.
+// atomic = 1 when the tile is split over several items (combined with
+// float2 atomics after the tile was zeroed).
+struct OwnerItem {
+    int tile, frame, v0, v1, atomic;
+};
+
 // Arguments describing the "channels" of an apply: coils (B), subspace
 // coefficients / frames (C), B0 segments (L).
 struct ApplyDesc {
@@ -109,6 +118,14 @@ struct pfb_plan {
     int spread_threads = 256;
     int interp_threads = 256;
     int spread_channels = 0;     // channels per CTA (0 = automatic)
+    // channel-interleaved pipeline
+    pfb::OwnerItem *d_own_frame = nullptr, *d_zero_frame = nullptr;
+    int n_own_frame = 0, n_zero_frame = 0;
+    pfb::OwnerItem *d_own_all = nullptr, *d_zero_all = nullptr;
+    int n_own_all = 0, n_zero_all = 0;
+    int own_chunk = 0;
+    std::map<int, cufftHandle> fft_plans_il;   // keyed by channels per group
+    std::map<int, size_t> fft_work_il;
 };
 
 namespace pfb {
@@ -172,7 +189,11 @@ __device__ __forceinline__ float kb_eval_deriv(float u, float beta, float *dval)
     return val;
 }
 
+// a mod n in [0, n); the common cases (|a| within one period) avoid the 64-bit division
 __host__ __device__ __forceinline__ int pmod(long long a, int n) {
+    if (a >= 0 && a < n) return (int)a;
+    if (a < 0 && a >= -(long long)n) return (int)(a + n);
+    if (a >= n && a < 2LL * n) return (int)(a - n);
     long long r = a % n;
     return (int)(r < 0 ? r + n : r);
 }
@@ -261,5 +282,25 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
 int plan_tables(const pfb_plan *p, int axis_zyx, int32_t *index, float *value, cudaStream_t s);
 void plan_free(pfb_plan *p);
 int rebuild_items(pfb_plan *p, int chunk);
+
+// capi.cu: planar batched cuFFT plans (cached per plane count) and execution
+int get_fft_plan(std::mutex &mu, std::map<int64_t, cufftHandle> &plans, std::map<int64_t, size_t> &work,
+                 int ndim, const int *nos_xyz, int64_t nplanes, cufftHandle *out, size_t *wbytes);
+int run_fft(cufftHandle h, size_t wbytes, float2 *data, int direction, void *work, size_t work_avail,
+            cudaStream_t s);
+
+// fast.cu (channel-interleaved pipeline)
+int fast_supported(const pfb_plan *p, const ApplyDesc &d, std::string *why);
+int fast_workspace(pfb_plan *p, const ApplyDesc &d, size_t *bytes);
+int fast_fwd(pfb_plan *p, const ApplyDesc &d, const float2 *img, float2 *ksp, void *ws, size_t wsb, float factor,
+             bool accumulate, cudaStream_t s);
+int fast_adj(pfb_plan *p, const ApplyDesc &d, const float2 *ksp, float2 *img, void *ws, size_t wsb, float factor,
+             bool accumulate, cudaStream_t s);
+int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const float2 *vals, float *grad, void *ws,
+                   size_t wsb, float factor, bool accumulate, cudaStream_t s);
+int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void *dst, void *ws, size_t wsb,
+               float factor, bool accumulate, cudaStream_t s);
+int build_owner_items(pfb_plan *p, int chunk);
+void free_owner_items(pfb_plan *p);
 
 }  // namespace pfb

@@ -1,0 +1,1194 @@
+// Channel-interleaved NUFFT pipeline (the path behind pfb_nufft_fwd / pfb_nufft_adj).
+//
+// Two grid layouts share the workspace:
+//   planar       [group][channel][point]  -- what cuFFT transforms (batched planes)
+//   interleaved  [group][point][channel]  -- what the interp gathers from
+//   without a basis: group = frame f, channel = l * B + b        (B0 segment l, batch b)
+//   with a basis:    group = 0,       channel = (l * B + b) * K + k
+// point is the FFT-layout position ((centred index - n_os//2) mod n_os, x fastest).
+// In the interleaved layout a tap of a sample is one contiguous run of
+// channels, so a warp whose lanes are channels gathers it with one coalesced
+// access.  cuFFT is far faster on planar batches than on channel-strided
+// data, so the forward path transposes the transformed grid once, and the
+// spread writes its finished tiles straight into planar planes.
+//
+// Kernels:
+//   pad_pl       image (B, C, *N) -> planar grid, deapodised, zero-padded, times C_l (B0)
+//   transpose    planar grid -> interleaved grid
+//   interp_il    interleaved grid -> res[j][channel] (one warp per sample, lanes = channels)
+//   out_il       res -> k-space (B, M): sum over segments / coefficients with
+//                B_l(t) basis[f, k], density weight
+//   vals_il      k-space (B, M) -> vals[j][channel] in bin-sorted order, with the
+//                density weight and conj(B_l(t)) conj(basis[f, k]) factors
+//   spread_il    vals -> planar grid, owner-computes: one CTA per output tile (and
+//                sample chunk) accumulates in shared memory the contributions of
+//                the samples whose first tap lies in the tile or in its 2^d - 1
+//                lower neighbours, then stores the tile (plain stores; tiles too
+//                crowded for one CTA are split and combined with float2 atomics
+//                after a zeroing pass)
+//   crop_pl      planar grid -> image, cropped, deapodised, sum_l conj(C_l) (B0)
+//   traj_il      d/dk of sum_b Re(conj(A x)_b v_b) (analytic Kaiser-Bessel derivative)
+#include <cmath>
+
+#include "pfb_common.cuh"
+
+namespace pfb {
+
+namespace {
+
+constexpr int kTileWarps = 8;        // warps per CTA of the sample kernels
+constexpr int kOutRows = 32;         // samples per CTA in the transposing kernels
+constexpr int kSpreadWarps = 16;     // warps per CTA of the spread
+
+struct Chan {
+    int nch;       // channels per group
+    int ngrp;      // groups
+    int B, L, K;   // batch, segments, coefficients (K = 0 without basis)
+    int F;
+};
+
+Chan make_chan(const pfb_plan *p, const ApplyDesc &d) {
+    Chan c;
+    c.B = (int)d.batch;
+    c.L = d.nseg;
+    c.K = d.basis ? d.ncoeff : 0;
+    c.F = p->nframes;
+    c.nch = c.L * c.B * (c.K ? c.K : 1);
+    c.ngrp = c.K ? 1 : p->nframes;
+    return c;
+}
+
+__device__ __forceinline__ int log2i(int v) { return 31 - __clz(v); }
+
+// ------------------------------------------------------------------------------------
+// pad / crop on the planar grid
+// ------------------------------------------------------------------------------------
+struct PadPL {
+    Geom g;
+    const float2 *src;      // pad: image (B, C, nvol);     crop: planar grid
+    float2 *dst;            // pad: planar grid;            crop: image (B, C, nvol)
+    const float *apod0, *apod1, *apod2;
+    const float2 *Cl;       // (L, nvol) or null
+    Chan ch;
+    int C;                  // image planes per batch item (F or K)
+    float factor;
+    int accumulate;
+};
+
+// grid plane (grp, ch), FFT-layout position p -> image pixel r = (p + N//2) mod n_os, valid if r < N
+__global__ void __launch_bounds__(256) pad_pl_kernel(const PadPL P) {
+    const int64_t gvol = P.g.gvol;
+    const int64_t total = (int64_t)P.ch.ngrp * P.ch.nch * gvol;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int Kc = P.ch.K ? P.ch.K : 1, B = P.ch.B;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
+        const int64_t plane = e / gvol;
+        const int64_t pos = e - plane * gvol;
+        const int grp = (int)(plane / P.ch.nch), ch = (int)(plane - (int64_t)grp * P.ch.nch);
+        const int p0 = (int)(pos % P.g.nos[0]);
+        const int64_t rest = pos / P.g.nos[0];
+        const int p1 = (int)(rest % P.g.nos[1]);
+        const int p2 = (int)(rest / P.g.nos[1]);
+        int r0 = p0 + P.g.n[0] / 2; r0 = r0 >= P.g.nos[0] ? r0 - P.g.nos[0] : r0;
+        int r1 = p1 + P.g.n[1] / 2; r1 = r1 >= P.g.nos[1] ? r1 - P.g.nos[1] : r1;
+        int r2 = p2 + P.g.n[2] / 2; r2 = r2 >= P.g.nos[2] ? r2 - P.g.nos[2] : r2;
+        float2 out = make_float2(0.f, 0.f);
+        if (r0 < P.g.n[0] && r1 < P.g.n[1] && r2 < P.g.n[2]) {
+            const int k = ch % Kc, lb = ch / Kc, b = lb % B, l = lb / B;
+            const int c = P.ch.K ? k : grp;
+            const int64_t rl = ((int64_t)r2 * P.g.n[1] + r1) * P.g.n[0] + r0;
+            float2 v = P.src[((int64_t)b * P.C + c) * P.g.nvol + rl];
+            float a = P.factor;
+            if (P.apod0) a *= P.apod0[r0];
+            if (P.apod1) a *= P.apod1[r1];
+            if (P.apod2) a *= P.apod2[r2];
+            if (P.Cl) v = cmul(v, P.Cl[(int64_t)l * P.g.nvol + rl]);
+            out = make_float2(v.x * a, v.y * a);
+        }
+        P.dst[e] = out;
+    }
+}
+
+// image (b, c, r) = factor * apod(r) * sum_l conj(C_l(r)) * grid[plane(l, b, c)][(r - N//2) mod n_os]
+__global__ void __launch_bounds__(256) crop_pl_kernel(const PadPL P) {
+    const int64_t nvol = P.g.nvol;
+    const int B = P.ch.B, L = P.ch.L, Kc = P.ch.K ? P.ch.K : 1;
+    const int64_t total = (int64_t)B * P.C * nvol;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
+        const int64_t bc = e / nvol;
+        const int64_t rl = e - bc * nvol;
+        const int b = (int)(bc / P.C), c = (int)(bc - (int64_t)b * P.C);
+        const int r0 = (int)(rl % P.g.n[0]);
+        const int64_t rest = rl / P.g.n[0];
+        const int r1 = (int)(rest % P.g.n[1]);
+        const int r2 = (int)(rest / P.g.n[1]);
+        int p0 = r0 - P.g.n[0] / 2; p0 = p0 < 0 ? p0 + P.g.nos[0] : p0;
+        int p1 = r1 - P.g.n[1] / 2; p1 = p1 < 0 ? p1 + P.g.nos[1] : p1;
+        int p2 = r2 - P.g.n[2] / 2; p2 = p2 < 0 ? p2 + P.g.nos[2] : p2;
+        const int64_t pos = ((int64_t)p2 * P.g.nos[1] + p1) * P.g.nos[0] + p0;
+        const int grp = P.ch.K ? 0 : c;
+        float2 acc = make_float2(0.f, 0.f);
+        for (int l = 0; l < L; ++l) {
+            const int ch = P.ch.K ? (l * B + b) * Kc + c : l * B + b;
+            float2 v = P.src[((int64_t)grp * P.ch.nch + ch) * P.g.gvol + pos];
+            if (P.Cl) v = cmulc(v, P.Cl[(int64_t)l * nvol + rl]);
+            acc.x += v.x;
+            acc.y += v.y;
+        }
+        float a = P.factor;
+        if (P.apod0) a *= P.apod0[r0];
+        if (P.apod1) a *= P.apod1[r1];
+        if (P.apod2) a *= P.apod2[r2];
+        acc.x *= a;
+        acc.y *= a;
+        if (P.accumulate) {
+            float2 o = P.dst[e];
+            acc.x += o.x;
+            acc.y += o.y;
+        }
+        P.dst[e] = acc;
+    }
+}
+
+// planar [grp][ch][point] -> interleaved [grp][point][ch], through a shared tile of
+// tc channels x tp points (tc * tp = 1024); loads coalesced along points, stores along channels.
+__global__ void __launch_bounds__(256) transpose_kernel(const float2 *__restrict__ src, float2 *__restrict__ dst,
+                                                        int64_t gvol, int nch, int tc) {
+    __shared__ float2 sm[1024 + 32];
+    const int tp = 1024 / tc;
+    const int grp = blockIdx.z;
+    const int64_t p0 = (int64_t)blockIdx.x * tp;
+    const int c0 = blockIdx.y * tc;
+    const float2 *S = src + (int64_t)grp * nch * gvol;
+    float2 *Dd = dst + (int64_t)grp * nch * gvol;
+    for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+        int cl = e / tp, pl = e - cl * tp;
+        int c = c0 + cl;
+        int64_t p = p0 + pl;
+        if (c < nch && p < gvol) sm[cl * (tp + 1) + pl] = S[(int64_t)c * gvol + p];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 1024; e += blockDim.x) {
+        int pl = e / tc, cl = e - pl * tc;
+        int c = c0 + cl;
+        int64_t p = p0 + pl;
+        if (c < nch && p < gvol) Dd[p * nch + c] = sm[cl * (tp + 1) + pl];
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// sample-side transposes
+// ------------------------------------------------------------------------------------
+struct SampIL {
+    const int *perm, *sframe;
+    const int64_t *frame_off;
+    int64_t mtot;
+    int readout;
+    const float *weight;
+    const float2 *basis;
+    const float2 *tB;
+    Chan ch;
+    const float2 *src;  // vals_il: k-space (B, M);  out_il: res [M][nch]
+    float2 *dst;        // vals_il: vals [M][nch];   out_il: k-space (B, M)
+    int factors;        // vals_il: apply conj(tB) conj(basis) (1) or only the weight (0)
+    int accumulate;
+};
+
+// vals[j][ch] = y[b][perm[j]] * w[g] * conj(B_l(t)) * conj(basis[f, k])
+__global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
+    extern __shared__ float2 sm[];  // [32][B]
+    const int64_t j0 = (int64_t)blockIdx.x * kOutRows;
+    const int B = P.ch.B;
+    for (int e = threadIdx.x; e < kOutRows * B; e += blockDim.x) {
+        int b = e / kOutRows, jj = e - b * kOutRows;
+        int64_t j = j0 + jj;
+        float2 v = make_float2(0.f, 0.f);
+        if (j < P.mtot) {
+            int g = P.perm[j];
+            v = P.src[(int64_t)b * P.mtot + g];
+            if (P.weight) {
+                float w = P.weight[g];
+                v.x *= w;
+                v.y *= w;
+            }
+        }
+        sm[jj * B + b] = v;
+    }
+    __syncthreads();
+    const int nch = P.ch.nch, Kc = P.ch.K ? P.ch.K : 1;
+    for (int e = threadIdx.x; e < kOutRows * nch; e += blockDim.x) {
+        int jj = e / nch, c = e - jj * nch;
+        int64_t j = j0 + jj;
+        if (j >= P.mtot) continue;
+        int k = c % Kc, lb = c / Kc, b = lb % B, l = lb / B;
+        float2 v = sm[jj * B + b];
+        if (P.factors) {
+            if (P.tB || P.ch.K) {
+                int g = P.perm[j], f = P.sframe[j];
+                if (P.tB) {
+                    int t = (int)((g - P.frame_off[f]) % P.readout);
+                    v = cmulc(v, P.tB[(int64_t)l * P.readout + t]);
+                }
+                if (P.ch.K) v = cmulc(v, P.basis[(int64_t)f * P.ch.K + k]);
+            }
+        }
+        P.dst[j * nch + c] = v;
+    }
+}
+
+// y[b][perm[j]] (+)= w[g] * sum_{l,k} B_l(t) basis[f, k] res[j][(l, b, k)]
+__global__ void __launch_bounds__(256) out_il_kernel(const SampIL P) {
+    extern __shared__ float2 sm[];  // [32][nch]
+    const int64_t j0 = (int64_t)blockIdx.x * kOutRows;
+    const int nch = P.ch.nch;
+    for (int e = threadIdx.x; e < kOutRows * nch; e += blockDim.x) {
+        int jj = e / nch, c = e - jj * nch;
+        int64_t j = j0 + jj;
+        sm[e] = j < P.mtot ? P.src[j * nch + c] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int B = P.ch.B, L = P.ch.L, Kc = P.ch.K ? P.ch.K : 1;
+    for (int e = threadIdx.x; e < kOutRows * B; e += blockDim.x) {
+        int b = e / kOutRows, jj = e - b * kOutRows;
+        int64_t j = j0 + jj;
+        if (j >= P.mtot) continue;
+        int g = P.perm[j];
+        float2 acc = make_float2(0.f, 0.f);
+        if (L == 1 && !P.ch.K) {
+            acc = sm[jj * nch + b];
+        } else {
+            int f = P.sframe[j];
+            int t = P.tB ? (int)((g - P.frame_off[f]) % P.readout) : 0;
+            for (int l = 0; l < L; ++l) {
+                float2 accl = make_float2(0.f, 0.f);
+                for (int k = 0; k < Kc; ++k) {
+                    float2 v = sm[jj * nch + (l * B + b) * Kc + k];
+                    if (P.ch.K) v = cmul(v, P.basis[(int64_t)f * P.ch.K + k]);
+                    accl.x += v.x;
+                    accl.y += v.y;
+                }
+                if (P.tB) accl = cmul(accl, P.tB[(int64_t)l * P.readout + t]);
+                acc.x += accl.x;
+                acc.y += accl.y;
+            }
+        }
+        if (P.weight) {
+            float w = P.weight[g];
+            acc.x *= w;
+            acc.y *= w;
+        }
+        float2 *dst = P.dst + (int64_t)b * P.mtot + g;
+        if (P.accumulate) {
+            float2 o = *dst;
+            acc.x += o.x;
+            acc.y += o.y;
+        }
+        *dst = acc;
+    }
+}
+
+
+// ------------------------------------------------------------------------------------
+// interp: one warp per bin-sorted sample, lanes = (tap group, channel)
+// ------------------------------------------------------------------------------------
+struct InterpIL {
+    Geom g;
+    const float *cos0, *cos1, *cos2;
+    const int *sframe;
+    int64_t mtot;
+    const float2 *grid;   // interleaved
+    float2 *res;          // [M][nch]
+    Chan ch;
+    int cw;               // lanes per channel chunk (power of two <= 32)
+    // trajectory gradient
+    const float2 *vt;     // [M][B] values (weight applied)
+    const float2 *basis;
+    const float2 *tB;
+    const int *perm;
+    const int64_t *frame_off;
+    int readout;
+    float chain[kMaxDim];
+    float *grad;          // (M, ndim) in original sample order
+    int accumulate;
+};
+
+// Per-sample tap weights and FFT-layout positions, computed by lanes (axis, i)
+// and left in shared memory for the warp: w[a][i], p[a][i] (and dw/dc).
+template <int D, int WM, bool DERIV>
+__device__ __forceinline__ void warp_taps(const InterpIL &P, int64_t j, float *sw, int *sp, float *sd, int lane) {
+    if (lane < D * WM) {
+        int a = lane / WM, i = lane - a * WM;
+        const float *cs = a == 0 ? P.cos0 : (a == 1 ? P.cos1 : P.cos2);
+        float c = cs[j];
+        int w = P.g.w[a];
+        long long x0 = start_index(c, w, P.g.cart[a]);
+        float wv = 0.f, dv = 0.f;
+        if (P.g.cart[a]) {
+            wv = i == 0 ? 1.f : 0.f;
+        } else if (i < w) {
+            float halfw = 0.5f * (float)w;
+            float u = ((float)(x0 + i) - c) / halfw;
+            if (DERIV) {
+                float d;
+                wv = kb_eval_deriv(u, P.g.beta[a], &d);
+                dv = -d / halfw;
+            } else {
+                wv = kb_eval(u, P.g.beta[a]);
+            }
+        }
+        int q = pmod(x0 + i - P.g.sh[a], P.g.nos[a]);
+        sw[a * WM + i] = wv;
+        sp[a * WM + i] = q;
+        if (DERIV) sd[a * WM + i] = dv;
+    }
+}
+
+template <int D, int WM>
+__global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const InterpIL P) {
+    __shared__ float s_w[kTileWarps][3 * WM];
+    __shared__ int s_p[kTileWarps][3 * WM];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cw = P.cw, lcw = log2i(cw), tg_n = 32 >> lcw;
+    const int cl = lane & (cw - 1), tg = lane >> lcw;
+    const int nch = P.ch.nch;
+    const int64_t nx = P.g.nos[0], nxy = (int64_t)P.g.nos[0] * P.g.nos[1];
+    const int wx_ = P.g.w[0], wy_ = D > 1 ? P.g.w[1] : 1, wz_ = D > 2 ? P.g.w[2] : 1;
+    constexpr int WY = D > 1 ? WM : 1, WZ = D > 2 ? WM : 1;
+    (void)WZ;
+    // each CTA takes a contiguous run of bin-sorted samples: its warps gather
+    // from the same few tiles, which stay in L1
+    const int64_t per = (P.mtot + gridDim.x - 1) / gridDim.x;
+    const int64_t jbeg = (int64_t)blockIdx.x * per, jend = min(P.mtot, jbeg + per);
+    for (int64_t j = jbeg + warp; j < jend; j += kTileWarps) {
+        warp_taps<D, WM, false>(P, j, s_w[warp], s_p[warp], nullptr, lane);
+        __syncwarp();
+        const int grp = P.ch.K ? 0 : P.sframe[j];
+        const float2 *G = P.grid + (int64_t)grp * P.g.gvol * nch;
+        // this lane's x taps: ix = tg, tg + tg_n, ... (weight 0 beyond the width)
+        float wxr[WM];
+        int pxr[WM];
+#pragma unroll
+        for (int m = 0; m < WM; ++m) {
+            int ix = tg + m * tg_n;
+            bool ok = ix < wx_;
+            wxr[m] = ok ? s_w[warp][ix] : 0.f;
+            pxr[m] = ok ? s_p[warp][ix] : 0;
+        }
+        for (int c0 = 0; c0 < nch; c0 += cw) {
+            const int c = c0 + cl;
+            const int cc = c < nch ? c : nch - 1;  // in-bounds address; result discarded
+            float2 acc = make_float2(0.f, 0.f);
+            const float2 *Gc = G + cc;
+            if constexpr (WM == 4) {
+                // all taps unrolled: every gather is issued before the FMAs need it
+#pragma unroll
+                for (int r = 0; r < WZ * WY; ++r) {
+                    const int iz = r / WY, iy = r - (r / WY) * WY;
+                    const bool ok = iz < wz_ && iy < wy_;
+                    const float wzy = ok ? (D > 2 ? s_w[warp][2 * WM + iz] : 1.f) * (D > 1 ? s_w[warp][WM + iy] : 1.f) : 0.f;
+                    const int prow = ok ? (D > 2 ? s_p[warp][2 * WM + iz] * (int)nxy : 0) + (D > 1 ? s_p[warp][WM + iy] * (int)nx : 0) : 0;
+#pragma unroll
+                    for (int m = 0; m < WM; ++m) {
+                        if (tg + m * tg_n < WM) {
+                            const float2 v = __ldg(Gc + (int64_t)(prow + pxr[m]) * nch);
+                            acc = cfma(wzy * wxr[m], v, acc);
+                        }
+                    }
+                }
+            } else {
+                for (int iz = 0; iz < wz_; ++iz) {
+                    const float wz = D > 2 ? s_w[warp][2 * WM + iz] : 1.f;
+                    const int pz = D > 2 ? s_p[warp][2 * WM + iz] * (int)nxy : 0;
+                    for (int iy = 0; iy < wy_; ++iy) {
+                        const float wzy = wz * (D > 1 ? s_w[warp][WM + iy] : 1.f);
+                        const int prow = pz + (D > 1 ? s_p[warp][WM + iy] * (int)nx : 0);
+#pragma unroll
+                        for (int m = 0; m < WM; ++m) {
+                            if (tg + m * tg_n < WM) {
+                                const float2 v = __ldg(Gc + (int64_t)(prow + pxr[m]) * nch);
+                                acc = cfma(wzy * wxr[m], v, acc);
+                            }
+                        }
+                    }
+                }
+            }
+            // reduce over tap groups (lanes that share the channel)
+            for (int off = cw; off < 32; off <<= 1) {
+                acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+                acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+            }
+            if (tg == 0 && c < nch) P.res[j * nch + c] = acc;
+        }
+        __syncwarp();
+    }
+}
+
+template <int D, int WM>
+__global__ void __launch_bounds__(kTileWarps * 32) traj_il_kernel(const InterpIL P) {
+    __shared__ float s_w[kTileWarps][3 * WM];
+    __shared__ float s_d[kTileWarps][3 * WM];
+    __shared__ int s_p[kTileWarps][3 * WM];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cw = P.cw, lcw = log2i(cw), tg_n = 32 >> lcw;
+    const int cl = lane & (cw - 1), tg = lane >> lcw;
+    const int nch = P.ch.nch, B = P.ch.B, Kc = P.ch.K ? P.ch.K : 1;
+    const int64_t nx = P.g.nos[0], nxy = (int64_t)P.g.nos[0] * P.g.nos[1];
+    const int wa[3] = {P.g.w[0], D > 1 ? P.g.w[1] : 1, D > 2 ? P.g.w[2] : 1};
+    const int64_t per = (P.mtot + gridDim.x - 1) / gridDim.x;
+    const int64_t jbeg = (int64_t)blockIdx.x * per, jend = min(P.mtot, jbeg + per);
+    for (int64_t j = jbeg + warp; j < jend; j += kTileWarps) {
+        warp_taps<D, WM, true>(P, j, s_w[warp], s_p[warp], s_d[warp], lane);
+        __syncwarp();
+        const int f = P.sframe[j];
+        const int gs = P.perm[j];
+        const int grp = P.ch.K ? 0 : f;
+        const int t = P.tB ? (int)((gs - P.frame_off[f]) % P.readout) : 0;
+        const float2 *G = P.grid + (int64_t)grp * P.g.gvol * nch;
+        float gacc[3] = {0.f, 0.f, 0.f};
+        for (int c0 = 0; c0 < nch; c0 += cw) {
+            const int c = c0 + cl;
+            float2 dsum[3] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+            if (c < nch) {
+                for (int iz = 0; iz < wa[2]; ++iz) {
+                    const float wz = D > 2 ? s_w[warp][2 * WM + iz] : 1.f;
+                    const float dz = D > 2 ? s_d[warp][2 * WM + iz] : 0.f;
+                    const int64_t pz = D > 2 ? s_p[warp][2 * WM + iz] * nxy : 0;
+                    for (int iy = 0; iy < wa[1]; ++iy) {
+                        const float wy = D > 1 ? s_w[warp][WM + iy] : 1.f;
+                        const float dy = D > 1 ? s_d[warp][WM + iy] : 0.f;
+                        const int64_t rowp = pz + (D > 1 ? s_p[warp][WM + iy] * nx : 0);
+                        for (int ix = tg; ix < wa[0]; ix += tg_n) {
+                            const float wx = s_w[warp][ix], dx = s_d[warp][ix];
+                            const float2 h = __ldg(G + (rowp + s_p[warp][ix]) * nch + c);
+                            dsum[0] = cfma(wz * wy * dx, h, dsum[0]);
+                            if (D > 1) dsum[1] = cfma(wz * dy * wx, h, dsum[1]);
+                            if (D > 2) dsum[2] = cfma(dz * wy * wx, h, dsum[2]);
+                        }
+                    }
+                }
+                // channel factor B_l(t) basis[f, k] and the value v_b
+                const int k = c % Kc, lb = c / Kc, b = lb % B, l = lb / B;
+                float2 fac = make_float2(1.f, 0.f);
+                if (P.tB) fac = P.tB[(int64_t)l * P.readout + t];
+                if (P.ch.K) fac = cmul(fac, P.basis[(int64_t)f * P.ch.K + k]);
+                const float2 v = P.vt[j * B + b];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    float2 dd = cmul(dsum[a], fac);
+                    gacc[a] += dd.x * v.x + dd.y * v.y;  // Re(conj(D) v)
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            for (int off = 16; off > 0; off >>= 1) gacc[a] += __shfl_xor_sync(0xffffffffu, gacc[a], off);
+        if (lane < D) {
+            float r = (lane == 0 ? gacc[0] : (lane == 1 ? gacc[1] : gacc[2])) * P.chain[lane];
+            float *dst = P.grad + (int64_t)gs * D + lane;
+            *dst = P.accumulate ? *dst + r : r;
+        }
+        __syncwarp();
+    }
+}
+
+
+// ------------------------------------------------------------------------------------
+// spread: owner-computes tiles
+// ------------------------------------------------------------------------------------
+struct SpreadIL {
+    Geom g;
+    const float *cos0, *cos1, *cos2;
+    const int *bin_start;
+    int nframes;
+    const OwnerItem *items;
+    const float2 *vals;   // [M][nch]
+    const float *wtap;    // [M][D * WM] kernel weights per sample
+    const int *xtap;      // [M][D] wrapped first tap per sample
+    float2 *grid;         // planar [grp][ch][point]
+    Chan ch;
+    int cw;               // channels per CTA (power of two <= 32)
+    int per_frame;        // 1: bins per (tile, frame); 0: bins merged over frames
+};
+
+__device__ __forceinline__ int tile_coord(int bin, int a, const Geom &g) {
+    if (a == 0) return bin % g.nbins[0];
+    if (a == 1) return (bin / g.nbins[0]) % g.nbins[1];
+    return bin / (g.nbins[0] * g.nbins[1]);
+}
+
+// the sorted-order range of bin `bin` for frame f (per_frame) or all frames
+__device__ __forceinline__ void bin_range(const SpreadIL &P, int bin, int f, int *s0, int *s1) {
+    if (P.per_frame) {
+        *s0 = P.bin_start[bin * P.nframes + f];
+        *s1 = P.bin_start[bin * P.nframes + f + 1];
+    } else {
+        *s0 = P.bin_start[bin * P.nframes];
+        *s1 = P.bin_start[(bin + 1) * P.nframes];
+    }
+}
+
+// Per-sample kernel taps for the spread, computed once per apply: weights
+// w[j][a * WM + i] and the wrapped first tap x0m[j][a] (bin-sorted order).
+template <int D, int WM>
+__global__ void __launch_bounds__(256) taps_prep_kernel(Geom g, const float *__restrict__ cos0,
+                                                        const float *__restrict__ cos1,
+                                                        const float *__restrict__ cos2, int64_t mtot,
+                                                        float *__restrict__ wout, int *__restrict__ xout) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < mtot; j += stride) {
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            const float c = (a == 0 ? cos0 : (a == 1 ? cos1 : cos2))[j];
+            const int w = g.w[a];
+            const long long x0 = start_index(c, w, g.cart[a]);
+            const float inv_halfw = 2.0f / (float)w;
+#pragma unroll
+            for (int i = 0; i < WM; ++i) {
+                float wv = 0.f;
+                if (g.cart[a]) wv = i == 0 ? 1.f : 0.f;
+                else if (i < w) wv = kb_eval(((float)(x0 + i) - c) * inv_halfw, g.beta[a]);
+                wout[j * (D * WM) + a * WM + i] = wv;
+            }
+            xout[j * D + a] = pmod(x0, g.nos[a]);
+        }
+    }
+}
+
+// Shared tile: for each tile point the real parts of its cw channels, then the
+// imaginary parts, then one pad word (pitch 2*cw + 1 floats).  Lanes that are
+// channels hit consecutive words in the accumulation; lanes that are points
+// hit words an odd pitch apart in the store.
+template <int D, int WM>
+__global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const SpreadIL P) {
+    extern __shared__ float acc[];
+    __shared__ float s_w[kSpreadWarps][3 * WM];
+    __shared__ int s_x[kSpreadWarps][3];
+    __shared__ int s_pre[(1 << D) + 1];   // prefix sums of the neighbour range sizes
+    __shared__ int s_beg[1 << D];
+    const OwnerItem it = P.items[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cw = P.cw, lcw = log2i(cw), tg_n = 32 >> lcw;
+    const int cl = lane & (cw - 1), tg = lane >> lcw;
+    const int pitch = 2 * cw + 1;
+    const int c0 = blockIdx.y * cw;
+    const int nch = P.ch.nch;
+    const int c = c0 + cl;
+    // tile geometry
+    int org[3], text[3], wrap[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (a < D) {
+            int tc = tile_coord(it.tile, a, P.g);
+            org[a] = tc * P.g.tile[a];
+            text[a] = min(P.g.tile[a], P.g.nos[a] - org[a]);
+            wrap[a] = P.g.nbins[a] == 1 ? text[a] : 0;
+        } else {
+            org[a] = 0;
+            text[a] = 1;
+            wrap[a] = 0;
+        }
+    }
+    const int T0 = P.g.tile[0], T1 = D > 1 ? P.g.tile[1] : 1, T2 = D > 2 ? P.g.tile[2] : 1;
+    const int tpts = T0 * T1 * T2;
+    int *s_pos = reinterpret_cast<int *>(acc + tpts * pitch);  // FFT-layout position of each tile point
+    for (int e = threadIdx.x; e < tpts * pitch; e += blockDim.x) acc[e] = 0.f;
+    for (int pt = threadIdx.x; pt < tpts; pt += blockDim.x) {
+        int t0 = pt % T0, rest = pt / T0, t1 = rest % T1, t2 = rest / T1;
+        int pos = -1;
+        if (t0 < text[0] && t1 < text[1] && t2 < text[2]) {
+            pos = pmod(org[0] + t0 - P.g.sh[0], P.g.nos[0]);
+            if (D > 1) pos += pmod(org[1] + t1 - P.g.sh[1], P.g.nos[1]) * P.g.nos[0];
+            if (D > 2) pos += pmod(org[2] + t2 - P.g.sh[2], P.g.nos[2]) * P.g.nos[0] * P.g.nos[1];
+        }
+        s_pos[pt] = pos;
+    }
+    // neighbour bins: tile minus delta, delta in {0,1}^D (no wrap onto itself)
+    const int nrng = 1 << D;
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int dlt = 0; dlt < nrng; ++dlt) {
+            int bin = 0, stride = 1;
+            bool ok = true;
+            for (int a = 0; a < D; ++a) {
+                int da = (dlt >> a) & 1;
+                int nb = P.g.nbins[a];
+                if (da && nb == 1) ok = false;
+                int tc = tile_coord(it.tile, a, P.g) - da;
+                tc = tc < 0 ? tc + nb : tc;
+                bin += tc * stride;
+                stride *= nb;
+            }
+            int s0 = 0, s1 = 0;
+            if (ok) bin_range(P, bin, it.frame < 0 ? 0 : it.frame, &s0, &s1);
+            s_pre[dlt] = run;
+            s_beg[dlt] = s0;
+            run += s1 - s0;
+        }
+        s_pre[nrng] = run;
+    }
+    __syncthreads();
+    constexpr int DW = D * WM;
+    constexpr int MX = WM;  // x taps a lane may own (all of them when it is the only tap group)
+    // virtual index v in [it.v0, it.v1) over the concatenated neighbour ranges
+    for (int v = it.v0 + warp; v < it.v1; v += kSpreadWarps) {
+        int r = 0;
+#pragma unroll
+        for (int q = 1; q < (1 << D); ++q) r += v >= s_pre[q] ? 1 : 0;
+        const int64_t j = (int64_t)s_beg[r] + (v - s_pre[r]);
+        if (lane < DW) s_w[warp][lane] = P.wtap[j * DW + lane];
+        if (lane < D) s_x[warp][lane] = P.xtap[j * D + lane];
+        float2 val = make_float2(0.f, 0.f);
+        if (c < nch) val = P.vals[j * nch + c];
+        __syncwarp();
+        // tile-local offset of x0 per axis; a sample of the lower neighbour (bit a
+        // of r) lies before the origin, across the periodic wrap for the first tile
+        int lo[3], ilo[3], ihi[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (a < D) {
+                int d = s_x[warp][a] - org[a];
+                if (((r >> a) & 1) && d >= 0) d -= P.g.nos[a];
+                lo[a] = d;
+                const int w = P.g.w[a];
+                ilo[a] = wrap[a] ? 0 : max(0, -d);
+                ihi[a] = wrap[a] ? w : min(w, text[a] - d);
+            } else {
+                lo[a] = 0;
+                ilo[a] = 0;
+                ihi[a] = 1;
+            }
+        }
+        if (c < nch) {
+            for (int iz = ilo[2]; iz < ihi[2]; ++iz) {
+                const float wz = D > 2 ? s_w[warp][2 * WM + iz] : 1.f;
+                int z = lo[2] + iz;
+                if (wrap[2] && z >= wrap[2]) z -= wrap[2];
+                for (int iy = ilo[1]; iy < ihi[1]; ++iy) {
+                    const float wyz = wz * (D > 1 ? s_w[warp][WM + iy] : 1.f);
+                    int y = lo[1] + iy;
+                    if (wrap[1] && y >= wrap[1]) y -= wrap[1];
+                    float *row = acc + (z * T1 + y) * T0 * pitch + cl;
+#pragma unroll
+                    for (int m = 0; m < MX; ++m) {
+                        const int ix = tg + m * tg_n;
+                        if (ix >= ilo[0] && ix < ihi[0]) {
+                            const float w = wyz * s_w[warp][ix];
+                            int x = lo[0] + ix;
+                            if (wrap[0] && x >= wrap[0]) x -= wrap[0];
+                            float *dst = row + x * pitch;
+                            atomicAdd(dst, w * val.x);
+                            atomicAdd(dst + cw, w * val.y);
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // write the tile into the planar grid: plain stores (sole owner) or float2
+    // atomics (split tile); consecutive threads take consecutive tile points
+    const int grp = P.ch.K ? 0 : (it.frame < 0 ? 0 : it.frame);
+    for (int ccl = 0; ccl < cw; ++ccl) {
+        const int ch = c0 + ccl;
+        if (ch >= nch) break;
+        float2 *G = P.grid + ((int64_t)grp * nch + ch) * P.g.gvol;
+        for (int pt = threadIdx.x; pt < tpts; pt += blockDim.x) {
+            const int pos = s_pos[pt];
+            if (pos < 0) continue;
+            const float2 vv = make_float2(acc[pt * pitch + ccl], acc[pt * pitch + cw + ccl]);
+            if (it.atomic) atomicAdd(G + pos, vv);
+            else G[pos] = vv;
+        }
+    }
+}
+
+// zero the tiles that several CTAs combine with atomics (planar grid)
+template <int D>
+__global__ void zero_tiles_kernel(Geom g, const OwnerItem *zero, int nch, float2 *grid, int basis) {
+    const OwnerItem it = zero[blockIdx.x];
+    int org[3], text[3];
+    for (int a = 0; a < 3; ++a) {
+        if (a < D) {
+            int tc = a == 0 ? it.tile % g.nbins[0]
+                            : (a == 1 ? (it.tile / g.nbins[0]) % g.nbins[1] : it.tile / (g.nbins[0] * g.nbins[1]));
+            org[a] = tc * g.tile[a];
+            text[a] = min(g.tile[a], g.nos[a] - org[a]);
+        } else {
+            org[a] = 0;
+            text[a] = 1;
+        }
+    }
+    const int grp = basis ? 0 : (it.frame < 0 ? 0 : it.frame);
+    const int tp = text[0] * text[1] * text[2];
+    for (int e = threadIdx.x; e < tp * nch; e += blockDim.x) {
+        int ch = e / tp, pt = e - ch * tp;
+        int t0 = pt % text[0], rest = pt / text[0], t1 = rest % text[1], t2 = rest / text[1];
+        int64_t pos = pmod(org[0] + t0 - g.sh[0], g.nos[0]);
+        if (D > 1) pos += (int64_t)pmod(org[1] + t1 - g.sh[1], g.nos[1]) * g.nos[0];
+        if (D > 2) pos += (int64_t)pmod(org[2] + t2 - g.sh[2], g.nos[2]) * g.nos[0] * g.nos[1];
+        grid[((int64_t)grp * nch + ch) * g.gvol + pos] = make_float2(0.f, 0.f);
+    }
+}
+
+int pow2ceil(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+size_t up256(size_t x) { return (x + 255) / 256 * 256; }
+
+struct WsLayout {
+    size_t gridp, gridi, samp, taps, work, total;
+};
+
+int wm_of(const Geom &g) { return std::max(g.w[0], std::max(g.w[1], g.w[2])) <= 4 ? 4 : 8; }
+
+int layout_ws(pfb_plan *p, const Chan &c, WsLayout *L, cufftHandle *h, size_t *wb) {
+    const int64_t P = (int64_t)c.ngrp * c.nch;
+    int st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, h, wb);
+    if (st) return st;
+    L->gridp = up256((size_t)P * p->g.gvol * sizeof(float2));
+    L->gridi = L->gridp;
+    L->samp = up256((size_t)p->mtot * c.nch * sizeof(float2));
+    const int D = p->g.ndim, WM = wm_of(p->g);
+    L->taps = up256((size_t)p->mtot * D * WM * sizeof(float)) + up256((size_t)p->mtot * D * sizeof(int));
+    L->work = up256(*wb);
+    L->total = L->gridp + L->gridi + L->samp + L->taps + L->work;
+    return PFB_OK;
+}
+
+template <int D, int WM>
+int launch_interp_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
+    interp_il_kernel<D, WM><<<blocks, kTileWarps * 32, 0, s>>>(P);
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
+template <int D, int WM>
+int launch_traj_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
+    traj_il_kernel<D, WM><<<blocks, kTileWarps * 32, 0, s>>>(P);
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
+template <int D, int WM>
+int launch_spread_il_t(const SpreadIL &P, int nitems, int nchunks, size_t smem, cudaStream_t s) {
+    auto k = spread_il_kernel<D, WM>;
+    if (smem > 48 * 1024) PFB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(nitems, nchunks);
+    k<<<grid, kSpreadWarps * 32, smem, s>>>(P);
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
+int sample_blocks(int64_t mtot) {
+    int64_t b = (mtot + kTileWarps - 1) / kTileWarps;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148LL * 64));
+}
+
+int flat_blocks(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148LL * 32));
+}
+
+void fill_interp(const pfb_plan *p, const Chan &c, InterpIL &P) {
+    P.g = p->g;
+    P.cos0 = p->d_cos[0];
+    P.cos1 = p->d_cos[1];
+    P.cos2 = p->d_cos[2];
+    P.sframe = p->d_sframe;
+    P.perm = p->d_perm;
+    P.mtot = p->mtot;
+    P.ch = c;
+    P.cw = std::min(32, pow2ceil(c.nch));
+    P.frame_off = p->d_frame_off;
+    P.readout = p->readout;
+    for (int a = 0; a < kMaxDim; ++a) P.chain[a] = (float)p->g.nos[a] / (float)p->g.n[a];
+}
+
+int wmax_of(const Geom &g) { return std::max(g.w[0], std::max(g.w[1], g.w[2])); }
+
+size_t tile_points(const pfb_plan *p) {
+    return (size_t)p->g.tile[0] * (p->g.ndim > 1 ? p->g.tile[1] : 1) * (p->g.ndim > 2 ? p->g.tile[2] : 1);
+}
+
+constexpr size_t kSpreadSmem = 200 * 1024;
+
+// the spread's channel chunk: as many of the (power-of-two) lanes as fit
+int spread_cw(const pfb_plan *p, const Chan &c) {
+    const size_t tpts = tile_points(p);
+    int cw = std::min(32, pow2ceil(c.nch));
+    while (cw > 1 && tpts * ((2 * cw + 1) * sizeof(float) + sizeof(int)) > kSpreadSmem) cw >>= 1;
+    return cw;
+}
+
+#define PFB_DISPATCH_DW(ND, W4, CALL4, CALL8)                 \
+    switch (ND) {                                             \
+        case 1: return (W4) ? CALL4(1) : CALL8(1);            \
+        case 2: return (W4) ? CALL4(2) : CALL8(2);            \
+        default: return (W4) ? CALL4(3) : CALL8(3);           \
+    }
+
+}  // namespace
+
+int fast_supported(const pfb_plan *p, const ApplyDesc &d, std::string *why) {
+    Chan c = make_chan(p, d);
+    // shared-memory staging of the sample transposes: 32 rows x channels
+    if ((size_t)kOutRows * c.nch * sizeof(float2) > 96 * 1024 ||
+        (size_t)kOutRows * (size_t)c.B * sizeof(float2) > 96 * 1024) {
+        if (why) *why = "too many channels for the interleaved path";
+        return 0;
+    }
+    if (tile_points(p) * (3 * sizeof(float) + sizeof(int)) > kSpreadSmem) {
+        if (why) *why = "tile too large";
+        return 0;
+    }
+    if (p->g.gvol >= (1LL << 31)) {
+        if (why) *why = "grid too large";
+        return 0;
+    }
+    return 1;
+}
+
+int fast_workspace(pfb_plan *p, const ApplyDesc &d, size_t *bytes) {
+    Chan c = make_chan(p, d);
+    WsLayout L;
+    cufftHandle h;
+    size_t wb;
+    int st = layout_ws(p, c, &L, &h, &wb);
+    if (st) return st;
+    *bytes = L.total;
+    return PFB_OK;
+}
+
+// One stage of the pipeline.  The workspace holds the planar grid, the
+// interleaved grid, the bin-sorted sample buffer and cuFFT's work area.
+//   PFB_STAGE_PAD        src image      -> planar grid
+//   PFB_STAGE_FFT        planar grid forward FFT (in place)
+//   PFB_STAGE_TRANSPOSE  planar grid    -> interleaved grid
+//   PFB_STAGE_INTERP     interleaved grid -> sample buffer (per-channel results)
+//   PFB_STAGE_OUT        sample buffer  -> dst k-space
+//   PFB_STAGE_VALS       src k-space    -> sample buffer (per-channel values)
+//   PFB_STAGE_SPREAD     sample buffer  -> planar grid (owner tiles)
+//   PFB_STAGE_IFFT       planar grid inverse FFT (in place)
+//   PFB_STAGE_CROP       planar grid    -> dst image
+int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void *dst, void *ws, size_t wsb,
+               float factor, bool accumulate, cudaStream_t s) {
+    Chan c = make_chan(p, d);
+    WsLayout L;
+    cufftHandle h;
+    size_t wb;
+    int st = layout_ws(p, c, &L, &h, &wb);
+    if (st) return st;
+    if (wsb < L.total) return fail(PFB_ERR_WORKSPACE, "workspace too small");
+    float2 *gridp = static_cast<float2 *>(ws);
+    float2 *gridi = reinterpret_cast<float2 *>(static_cast<char *>(ws) + L.gridp);
+    float2 *samp = reinterpret_cast<float2 *>(static_cast<char *>(ws) + L.gridp + L.gridi);
+    float *wtap = reinterpret_cast<float *>(static_cast<char *>(ws) + L.gridp + L.gridi + L.samp);
+    int *xtap = reinterpret_cast<int *>(reinterpret_cast<char *>(wtap) +
+                                        up256((size_t)p->mtot * p->g.ndim * wm_of(p->g) * sizeof(float)));
+    void *work = static_cast<char *>(ws) + L.gridp + L.gridi + L.samp + L.taps;
+    const bool basis = d.basis != nullptr;
+    const bool w4 = wmax_of(p->g) <= 4;
+    const int64_t P = (int64_t)c.ngrp * c.nch;
+    switch (stage) {
+        case PFB_STAGE_PAD:
+        case PFB_STAGE_CROP: {
+            PadPL Q{};
+            Q.g = p->g;
+            Q.apod0 = p->d_apod[0];
+            Q.apod1 = p->d_apod[1];
+            Q.apod2 = p->d_apod[2];
+            Q.Cl = d.b0_space;
+            Q.ch = c;
+            Q.C = d.ncoeff;
+            Q.factor = factor;
+            Q.accumulate = accumulate ? 1 : 0;
+            if (stage == PFB_STAGE_PAD) {
+                Q.src = static_cast<const float2 *>(src);
+                Q.dst = gridp;
+                pad_pl_kernel<<<flat_blocks(P * p->g.gvol), 256, 0, s>>>(Q);
+            } else {
+                Q.src = gridp;
+                Q.dst = static_cast<float2 *>(dst);
+                crop_pl_kernel<<<flat_blocks((int64_t)c.B * d.ncoeff * p->g.nvol), 256, 0, s>>>(Q);
+            }
+            PFB_CHECK_LAUNCH();
+            return PFB_OK;
+        }
+        case PFB_STAGE_FFT:
+        case PFB_STAGE_IFFT:
+            return run_fft(h, wb, gridp, stage == PFB_STAGE_FFT ? -1 : +1, work, L.work, s);
+        case PFB_STAGE_TRANSPOSE: {
+            const int tc = std::min(32, pow2ceil(c.nch));
+            const int tp = 1024 / tc;
+            dim3 g3((unsigned)((p->g.gvol + tp - 1) / tp), (unsigned)((c.nch + tc - 1) / tc), (unsigned)c.ngrp);
+            transpose_kernel<<<g3, 256, 0, s>>>(gridp, gridi, p->g.gvol, c.nch, tc);
+            PFB_CHECK_LAUNCH();
+            return PFB_OK;
+        }
+        case PFB_STAGE_INTERP: {
+            if (p->mtot == 0) return PFB_OK;
+            InterpIL Q{};
+            fill_interp(p, c, Q);
+            Q.grid = gridi;
+            Q.res = samp;
+            int blocks = sample_blocks(p->mtot);
+#define PFB_I4(DD) launch_interp_il_t<DD, 4>(Q, blocks, s)
+#define PFB_I8(DD) launch_interp_il_t<DD, 8>(Q, blocks, s)
+            PFB_DISPATCH_DW(p->g.ndim, w4, PFB_I4, PFB_I8)
+#undef PFB_I4
+#undef PFB_I8
+        }
+        case PFB_STAGE_OUT:
+        case PFB_STAGE_VALS: {
+            if (p->mtot == 0) return PFB_OK;
+            SampIL O{};
+            O.perm = p->d_perm;
+            O.sframe = p->d_sframe;
+            O.frame_off = p->d_frame_off;
+            O.mtot = p->mtot;
+            O.readout = p->readout;
+            O.weight = d.weight;
+            O.basis = d.basis;
+            O.tB = d.b0_time;
+            O.ch = c;
+            O.accumulate = accumulate ? 1 : 0;
+            const unsigned blocks = (unsigned)((p->mtot + kOutRows - 1) / kOutRows);
+            if (stage == PFB_STAGE_OUT) {
+                O.src = samp;
+                O.dst = static_cast<float2 *>(dst);
+                size_t smem = (size_t)kOutRows * c.nch * sizeof(float2);
+                if (smem > 48 * 1024)
+                    PFB_CUDA_TRY(cudaFuncSetAttribute(out_il_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                out_il_kernel<<<blocks, 256, smem, s>>>(O);
+            } else {
+                O.src = static_cast<const float2 *>(src);
+                O.dst = samp;
+                O.factors = 1;
+                size_t smem = (size_t)kOutRows * c.B * sizeof(float2);
+                if (smem > 48 * 1024)
+                    PFB_CUDA_TRY(cudaFuncSetAttribute(vals_il_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                vals_il_kernel<<<blocks, 256, smem, s>>>(O);
+            }
+            PFB_CHECK_LAUNCH();
+            return PFB_OK;
+        }
+        case PFB_STAGE_SPREAD: {
+            const OwnerItem *items = basis ? p->d_own_all : p->d_own_frame;
+            const int nitems = basis ? p->n_own_all : p->n_own_frame;
+            const OwnerItem *zero = basis ? p->d_zero_all : p->d_zero_frame;
+            const int nzero = basis ? p->n_zero_all : p->n_zero_frame;
+            if (nzero > 0) {
+                switch (p->g.ndim) {
+                    case 1: zero_tiles_kernel<1><<<nzero, 256, 0, s>>>(p->g, zero, c.nch, gridp, basis); break;
+                    case 2: zero_tiles_kernel<2><<<nzero, 256, 0, s>>>(p->g, zero, c.nch, gridp, basis); break;
+                    default: zero_tiles_kernel<3><<<nzero, 256, 0, s>>>(p->g, zero, c.nch, gridp, basis); break;
+                }
+                PFB_CHECK_LAUNCH();
+            }
+            if (nitems == 0) return PFB_OK;
+            if (p->mtot > 0) {
+                const int tb = flat_blocks(p->mtot);
+                switch (p->g.ndim * 10 + wm_of(p->g)) {
+                    case 14: taps_prep_kernel<1, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
+                    case 18: taps_prep_kernel<1, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
+                    case 24: taps_prep_kernel<2, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
+                    case 28: taps_prep_kernel<2, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
+                    case 34: taps_prep_kernel<3, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
+                    default: taps_prep_kernel<3, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
+                }
+                PFB_CHECK_LAUNCH();
+            }
+            SpreadIL S{};
+            S.g = p->g;
+            S.cos0 = p->d_cos[0];
+            S.cos1 = p->d_cos[1];
+            S.cos2 = p->d_cos[2];
+            S.bin_start = p->d_bin_start;
+            S.nframes = p->nframes;
+            S.items = items;
+            S.vals = samp;
+            S.wtap = wtap;
+            S.xtap = xtap;
+            S.grid = gridp;
+            S.ch = c;
+            S.cw = spread_cw(p, c);
+            S.per_frame = basis ? 0 : 1;
+            const size_t smem = tile_points(p) * ((2 * S.cw + 1) * sizeof(float) + sizeof(int));
+            const int nchunks = (c.nch + S.cw - 1) / S.cw;
+#define PFB_S4(DD) launch_spread_il_t<DD, 4>(S, nitems, nchunks, smem, s)
+#define PFB_S8(DD) launch_spread_il_t<DD, 8>(S, nitems, nchunks, smem, s)
+            PFB_DISPATCH_DW(p->g.ndim, w4, PFB_S4, PFB_S8)
+#undef PFB_S4
+#undef PFB_S8
+        }
+        default:
+            return fail(PFB_ERR_INVALID, "unknown stage");
+    }
+}
+
+int fast_fwd(pfb_plan *p, const ApplyDesc &d, const float2 *img, float2 *ksp, void *ws, size_t wsb, float factor,
+             bool accumulate, cudaStream_t s) {
+    int st;
+    if ((st = fast_stage(p, d, PFB_STAGE_PAD, img, nullptr, ws, wsb, factor, false, s))) return st;
+    if ((st = fast_stage(p, d, PFB_STAGE_FFT, nullptr, nullptr, ws, wsb, 1.f, false, s))) return st;
+    if ((st = fast_stage(p, d, PFB_STAGE_TRANSPOSE, nullptr, nullptr, ws, wsb, 1.f, false, s))) return st;
+    if ((st = fast_stage(p, d, PFB_STAGE_INTERP, nullptr, nullptr, ws, wsb, 1.f, false, s))) return st;
+    return fast_stage(p, d, PFB_STAGE_OUT, nullptr, ksp, ws, wsb, 1.f, accumulate, s);
+}
+
+int fast_adj(pfb_plan *p, const ApplyDesc &d, const float2 *ksp, float2 *img, void *ws, size_t wsb, float factor,
+             bool accumulate, cudaStream_t s) {
+    int st;
+    if ((st = fast_stage(p, d, PFB_STAGE_VALS, ksp, nullptr, ws, wsb, 1.f, false, s))) return st;
+    if ((st = fast_stage(p, d, PFB_STAGE_SPREAD, nullptr, nullptr, ws, wsb, 1.f, false, s))) return st;
+    if ((st = fast_stage(p, d, PFB_STAGE_IFFT, nullptr, nullptr, ws, wsb, 1.f, false, s))) return st;
+    return fast_stage(p, d, PFB_STAGE_CROP, nullptr, img, ws, wsb, factor, accumulate, s);
+}
+
+int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const float2 *vals, float *grad, void *ws,
+                   size_t wsb, float factor, bool accumulate, cudaStream_t s) {
+    Chan c = make_chan(p, d);
+    WsLayout L;
+    cufftHandle h;
+    size_t wb;
+    int st = layout_ws(p, c, &L, &h, &wb);
+    if (st) return st;
+    if (wsb < L.total) return fail(PFB_ERR_WORKSPACE, "workspace too small");
+    if ((st = fast_stage(p, d, PFB_STAGE_PAD, img, nullptr, ws, wsb, factor, false, s))) return st;
+    if ((st = fast_stage(p, d, PFB_STAGE_FFT, nullptr, nullptr, ws, wsb, 1.f, false, s))) return st;
+    if ((st = fast_stage(p, d, PFB_STAGE_TRANSPOSE, nullptr, nullptr, ws, wsb, 1.f, false, s))) return st;
+    if (p->mtot == 0) return PFB_OK;
+    float2 *gridi = reinterpret_cast<float2 *>(static_cast<char *>(ws) + L.gridp);
+    float2 *samp = reinterpret_cast<float2 *>(static_cast<char *>(ws) + L.gridp + L.gridi);
+    // v transposed to [j][b] with the density weight (no channel factors)
+    Chan cb = c;
+    cb.L = 1;
+    cb.K = 0;
+    cb.nch = c.B;
+    SampIL V{};
+    V.perm = p->d_perm;
+    V.sframe = p->d_sframe;
+    V.frame_off = p->d_frame_off;
+    V.mtot = p->mtot;
+    V.readout = p->readout;
+    V.weight = d.weight;
+    V.ch = cb;
+    V.src = vals;
+    V.dst = samp;
+    V.factors = 0;
+    size_t smem = (size_t)kOutRows * c.B * sizeof(float2);
+    if (smem > 48 * 1024) PFB_CUDA_TRY(cudaFuncSetAttribute(vals_il_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    vals_il_kernel<<<(unsigned)((p->mtot + kOutRows - 1) / kOutRows), 256, smem, s>>>(V);
+    PFB_CHECK_LAUNCH();
+    InterpIL Q{};
+    fill_interp(p, c, Q);
+    Q.grid = gridi;
+    Q.vt = samp;
+    Q.basis = d.basis;
+    Q.tB = d.b0_time;
+    Q.grad = grad;
+    Q.accumulate = accumulate ? 1 : 0;
+    bool w4 = wmax_of(p->g) <= 4;
+    int blocks = sample_blocks(p->mtot);
+#define PFB_T4(DD) launch_traj_il_t<DD, 4>(Q, blocks, s)
+#define PFB_T8(DD) launch_traj_il_t<DD, 8>(Q, blocks, s)
+    PFB_DISPATCH_DW(p->g.ndim, w4, PFB_T4, PFB_T8)
+#undef PFB_T4
+#undef PFB_T8
+}
+
+// ------------------------------------------------------------------------------------
+// plan-time owner items
+// ------------------------------------------------------------------------------------
+namespace {
+
+void owner_items_for(const pfb_plan *p, bool per_frame, int chunk, std::vector<OwnerItem> &items,
+                     std::vector<OwnerItem> &zero) {
+    const Geom &g = p->g;
+    const int D = g.ndim;
+    const int F = p->nframes;
+    const auto &bs = p->bin_start;
+    items.clear();
+    zero.clear();
+    const int nfr = per_frame ? F : 1;
+    for (int t = 0; t < p->nbins_total; ++t) {
+        int tc[3] = {0, 0, 0};
+        tc[0] = t % g.nbins[0];
+        if (D > 1) tc[1] = (t / g.nbins[0]) % g.nbins[1];
+        if (D > 2) tc[2] = t / (g.nbins[0] * g.nbins[1]);
+        for (int f = 0; f < nfr; ++f) {
+            long long total = 0;
+            for (int dlt = 0; dlt < (1 << D); ++dlt) {
+                int bin = 0, stride = 1;
+                bool ok = true;
+                for (int a = 0; a < D; ++a) {
+                    int da = (dlt >> a) & 1;
+                    if (da && g.nbins[a] == 1) ok = false;
+                    int c = tc[a] - da;
+                    c = c < 0 ? c + g.nbins[a] : c;
+                    bin += c * stride;
+                    stride *= g.nbins[a];
+                }
+                if (!ok) continue;
+                if (per_frame) total += bs[bin * F + f + 1] - bs[bin * F + f];
+                else total += bs[(bin + 1) * F] - bs[bin * F];
+            }
+            int fr = per_frame ? f : -1;
+            if (total <= chunk) {
+                items.push_back({t, fr, 0, (int)total, 0});
+            } else {
+                for (long long v = 0; v < total; v += chunk)
+                    items.push_back({t, fr, (int)v, (int)std::min<long long>(total, v + chunk), 1});
+                zero.push_back({t, fr, 0, 0, 1});
+            }
+        }
+    }
+}
+
+template <typename T>
+int upload(const std::vector<T> &h, T **d) {
+    cudaFree(*d);
+    *d = nullptr;
+    size_t n = std::max<size_t>(h.size(), 1);
+    cudaError_t e = cudaMalloc((void **)d, n * sizeof(T));
+    if (e != cudaSuccess) return fail(PFB_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    if (!h.empty()) PFB_CUDA_TRY(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return PFB_OK;
+}
+
+}  // namespace
+
+int build_owner_items(pfb_plan *p, int chunk) {
+    std::vector<OwnerItem> it, z;
+    int st;
+    owner_items_for(p, true, chunk, it, z);
+    if ((st = upload(it, &p->d_own_frame))) return st;
+    if ((st = upload(z, &p->d_zero_frame))) return st;
+    p->n_own_frame = (int)it.size();
+    p->n_zero_frame = (int)z.size();
+    owner_items_for(p, false, chunk, it, z);
+    if ((st = upload(it, &p->d_own_all))) return st;
+    if ((st = upload(z, &p->d_zero_all))) return st;
+    p->n_own_all = (int)it.size();
+    p->n_zero_all = (int)z.size();
+    p->own_chunk = chunk;
+    return PFB_OK;
+}
+
+void free_owner_items(pfb_plan *p) {
+    cudaFree(p->d_own_frame);
+    cudaFree(p->d_zero_frame);
+    cudaFree(p->d_own_all);
+    cudaFree(p->d_zero_all);
+    p->d_own_frame = p->d_zero_frame = p->d_own_all = p->d_zero_all = nullptr;
+    std::lock_guard<std::mutex> lk(p->fft_mu);
+    for (auto &kv : p->fft_plans_il) cufftDestroy(kv.second);
+    p->fft_plans_il.clear();
+}
+
+}  // namespace pfb

@@ -121,6 +121,20 @@ double kb_host(double x, double beta) {
             ti * (-0.01647633 + ti * 0.00392377))))))));
 }
 
+// A tile must be at least W - 1 wide, and so must the last (partial) tile, so
+// that a kernel footprint spans at most two consecutive tiles per axis (the
+// owner-computes spread gathers from the tile and its lower neighbour only).
+int fit_tile(int t, int w, int nos) {
+    t = std::max(1, std::min(t, nos));
+    if (w <= 1) return t;
+    auto ok = [&](int tt) { int r = nos % tt; return tt >= w - 1 && (r == 0 || r >= w - 1); };
+    for (int d = 0; d < nos; ++d) {
+        if (t - d >= 1 && ok(t - d)) return t - d;
+        if (t + d <= nos && ok(t + d)) return t + d;
+    }
+    return nos;
+}
+
 int default_tile(int ndim, int nos) {
     int t = ndim == 1 ? 1024 : (ndim == 2 ? 32 : 8);
     return std::max(1, std::min(t, nos));
@@ -233,7 +247,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
             g.cart[a] = (is_cart && is_cart[z] != 0) || width[z] == 1;
             g.w[a] = g.cart[a] ? 1 : width[z];
             g.beta[a] = beta[z];
-            g.tile[a] = tile && tile[z] > 0 ? std::min(tile[z], g.nos[a]) : default_tile(ndim, g.nos[a]);
+            g.tile[a] = fit_tile(tile && tile[z] > 0 ? tile[z] : default_tile(ndim, g.nos[a]), g.w[a], g.nos[a]);
         } else {
             g.n[a] = g.nos[a] = g.w[a] = g.tile[a] = 1;
             g.cart[a] = 1;
@@ -289,6 +303,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
         cudaFree(d_bad);
         cudaFree(d_temp);
         if (code != PFB_OK) {
+            free_owner_items(p);
             free_plan_buffers(p);
             delete p;
         }
@@ -378,6 +393,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
     p->max_bin = maxbin;
     int chunk = ndim == 3 ? 256 : 512;
     PFB_TRY_ST(rebuild_items(p, chunk));
+    PFB_TRY_ST(build_owner_items(p, ndim == 3 ? 2048 : 4096));
 #undef PFB_TRY_ST
 #undef PFB_TRY_CU
     cleanup(PFB_OK);
@@ -402,6 +418,7 @@ void plan_free(pfb_plan *p) {
         for (auto &kv : p->fft_plans) cufftDestroy(kv.second);
         p->fft_plans.clear();
     }
+    free_owner_items(p);
     free_plan_buffers(p);
     delete p;
 }

@@ -122,3 +122,80 @@ def test_spread_is_deterministic_in_layout_and_fft_shift(golden):
     L.check(lib.pfb_spread(h, ctypes.byref(o), ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(g1.data_ptr()), 1, _stream()))
     rolled = torch.fft.ifftshift(g0, dim=(-2, -1))
     assert rel(g1.cpu(), rolled.cpu()) < 1e-6
+
+
+def _pipeline_both(plan, x, y, basis=None, zs=None, zt=None, L=1):
+    """pfb_nufft_fwd / adj with a planar-size workspace (planar kernels) and with
+    pfb_apply_workspace_size bytes (channel-interleaved kernels)."""
+    Lb = _lib()
+    lib = Lb.load()
+    h = plan.interpolator.handle
+    B, C = x.shape[0], x.shape[1]
+    o = _opts(B, C, basis)
+    if zs is not None:
+        o.nseg, o.b0_time, o.b0_space = L, zt.data_ptr(), zs.data_ptr()
+    nplanes = o.nseg * B * C
+    small, big = ctypes.c_size_t(), ctypes.c_size_t()
+    Lb.check(lib.pfb_workspace_size(h, nplanes, ctypes.byref(small)))
+    Lb.check(lib.pfb_apply_workspace_size(h, ctypes.byref(o), ctypes.byref(big)))
+    assert big.value > small.value
+    res = {}
+    for name, n in (("planar", small.value), ("fast", big.value)):
+        ws = torch.empty(n, dtype=torch.uint8, device="cuda")
+        k = torch.empty((B, plan.interpolator.total_samples), dtype=torch.complex64, device="cuda")
+        im = torch.empty_like(x)
+        Lb.check(lib.pfb_nufft_fwd(h, ctypes.byref(o), ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(k.data_ptr()),
+                                   ctypes.c_void_p(ws.data_ptr()), n, _stream()))
+        Lb.check(lib.pfb_nufft_adj(h, ctypes.byref(o), ctypes.c_void_p(y.data_ptr()), ctypes.c_void_p(im.data_ptr()),
+                                   ctypes.c_void_p(ws.data_ptr()), n, _stream()))
+        res[name] = (k, im)
+    assert rel(res["fast"][0].cpu(), res["planar"][0].cpu().numpy()) < 1e-5
+    assert rel(res["fast"][1].cpu(), res["planar"][1].cpu().numpy()) < 1e-5
+
+
+@pytest.mark.parametrize("case", ["2d_coils", "2d_frames", "3d", "basis", "b0", "3d_w6_odd", "2d_single_tile"])
+def test_interleaved_pipeline_matches_planar(case):
+    rng = np.random.default_rng(21)
+    crn = lambda *s: torch.as_tensor((rng.standard_normal(s) + 1j * rng.standard_normal(s)).astype(np.complex64)).cuda()  # noqa: E731
+    if case == "2d_coils":
+        N = (96, 96)
+        coord = ((rng.random((1, 60, 192, 2)) - 0.5) * 96).astype(np.float32)
+        plan = _plan(coord, N, (2.0, 2.0), (4, 4))
+        _pipeline_both(plan, crn(12, 1, *N), crn(12, 60 * 192))
+    elif case == "2d_frames":
+        N = (40, 48)
+        coord = ((rng.random((5, 7, 64, 2)) - 0.5) * np.array([48, 40])).astype(np.float32)
+        plan = _plan(coord, N, (1.25, 1.5), (5, 4))
+        _pipeline_both(plan, crn(3, 5, *N), crn(3, 5 * 7 * 64))
+    elif case == "3d":
+        N = (30, 28, 26)
+        coord = ((rng.random((1, 50, 80, 3)) - 0.5) * np.array([26, 28, 30])).astype(np.float32)
+        plan = _plan(coord, N, (1.25, 1.25, 1.25), (4, 4, 4))
+        _pipeline_both(plan, crn(33, 1, *N), crn(33, 50 * 80))
+    elif case == "2d_single_tile":
+        # a 24 x 24 oversampled grid is one tile: taps wrap around inside the tile
+        N = (12, 12)
+        coord = np.concatenate([((rng.random((1, 1, 60, 2)) - 0.5) * 12),
+                                np.full((1, 1, 4, 2), -6.0), np.full((1, 1, 4, 2), 5.9)], axis=2).astype(np.float32)
+        plan = _plan(coord, N, (2.0, 2.0), (4, 4))
+        _pipeline_both(plan, crn(3, 1, *N), crn(3, 68))
+    elif case == "3d_w6_odd":
+        N = (17, 21, 19)
+        coord = ((rng.random((1, 20, 50, 3)) - 0.5) * np.array([19, 21, 17])).astype(np.float32)
+        plan = _plan(coord, N, (2.0, 1.5, 2.0), (6, 5, 7))
+        _pipeline_both(plan, crn(5, 1, *N), crn(5, 20 * 50))
+    elif case == "basis":
+        N = (32, 32)
+        F, K = 6, 3
+        coord = ((rng.random((F, 9, 48, 2)) - 0.5) * 32).astype(np.float32)
+        plan = _plan(coord, N, (2.0, 2.0), (4, 4))
+        basis = crn(F, K)
+        _pipeline_both(plan, crn(4, K, *N), crn(4, F * 9 * 48), basis=basis)
+    else:
+        N = (32, 32)
+        Lseg = 5
+        coord = ((rng.random((1, 12, 64, 2)) - 0.5) * 32).astype(np.float32)
+        plan = _plan(coord, N, (1.25, 1.25), (4, 4))
+        zt = crn(Lseg, 64)
+        zs = crn(Lseg, 32 * 32)
+        _pipeline_both(plan, crn(6, 1, *N), crn(6, 12 * 64), zs=zs, zt=zt, L=Lseg)
