@@ -197,10 +197,10 @@ def stage_times(torch, pf, plan, x, iters):
     L = _lib.load()
     ctx = _Ctx(plan, None, None, _lib.PFB_NORM_NONE)
     B = x.shape[0]
-    o = ctx.opts(B, (0, 1))
+    o = ctx.opts(B, next(ctx.segments()))
     h = plan.interpolator.handle
     ws = ctx.workspace(o)
-    y = torch.empty((B, plan.interpolator.total_samples), dtype=torch.complex64, device=x.device)
+    y = torch.zeros((B, plan.interpolator.total_samples), dtype=torch.complex64, device=x.device)
     xa = torch.empty_like(x)
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     P = lambda t: ctypes.c_void_p(t.data_ptr()) if t is not None else None  # noqa: E731
@@ -507,6 +507,7 @@ def extra_workload(args):
         ms_graph = time_device(torch, graph.replay, args.steps, args.warmup)
         clk = clocks.stop()
         value = B * Mtot / (ms_graph / 1e3)
+        stages = stage_times(torch, pf, bplan, x, 5)
         line.update(metric="B0-corrected NUFFT fwd+adj samples/s, batched graph-captured (2D radial, 64 uneven frames)",
                     value=value, unit="samples/s", ms_per_step=ms_graph,
                     config={"workload": "B0 time-segmented dynamic radial fwd+adj", "image": [N, N], "coils": B,
@@ -514,7 +515,8 @@ def extra_workload(args):
                             "segments": Lseg, "oversamp": 1.25, "width": 4,
                             "plain_ms": ms_plain, "batched_ms": ms_batch, "batched_graph_ms": ms_graph,
                             "plain_samples_per_s": B * Mtot / (ms_plain / 1e3),
-                            "batched_over_plain": ms_plain / ms_graph},
+                            "batched_over_plain": ms_plain / ms_graph,
+                            "batched_stages_ms": {k: round(v, 4) for k, v in stages.items()}},
                     cpu_baseline=None)
     elif args.workload == "cfg5":
         N, B, nimg = 256, 8, 32

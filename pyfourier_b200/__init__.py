@@ -8,6 +8,7 @@ fallback and importing an operator without the library raises.
 """
 
 from . import _lib
+from ._autotune import autotune
 from ._b0 import mri_exp_approx
 from ._gram import GramMatrix, plan_spgram, sparse_gram
 from ._nufft import nufft, nufft_adj
@@ -17,5 +18,5 @@ __version__ = "0.1.0"
 
 __all__ = [
     "nufft", "nufft_adj", "plan_nufft", "NUFFTPlan", "Interpolator",
-    "plan_spgram", "sparse_gram", "GramMatrix", "mri_exp_approx",
+    "plan_spgram", "sparse_gram", "GramMatrix", "mri_exp_approx", "autotune",
 ]

@@ -123,6 +123,24 @@ class Interpolator:
             self._build()
         return self
 
+    def retile(self, tile):
+        """Rebuild the device plan with another tile extent ((z, y, x) order)."""
+        tile = tuple(int(t) for t in tile)
+        if len(tile) != self.ndim:
+            raise ValueError("tile needs one extent per axis")
+        if self._handle is not None and tuple(self._tile or ()) == tile:
+            return self
+        old = self._tile
+        self._destroy()
+        self._tile = tile
+        try:
+            self._build()
+        except Exception:
+            self._tile = old
+            self._build()
+            raise
+        return self
+
     def set_tuning(self, spread_threads=0, interp_threads=0, spread_channels=0, chunk=None):
         L = _lib.load()
         _lib.check(L.pfb_plan_set_tuning(self._handle, int(spread_threads), int(interp_threads),
@@ -220,7 +238,7 @@ def _frames_from_coord(coord):
 
 
 def plan_nufft(coord, shape, width=4, oversamp=1.25, zmap=None, L=6, nbins=(40, 40), dt=None,
-               T=None, L_batch_size=None, device=None, tile=None):
+               T=None, L_batch_size=None, device=None, tile=None, autotune_batch=None):
     """Precompute a NUFFT plan (src/pyfourier/_nufft/_plan.py:20-199).
 
     ``coord``: (ncontrasts, nviews, nsamples, ndim), (nviews, nsamples, ndim)
@@ -229,7 +247,9 @@ def plan_nufft(coord, shape, width=4, oversamp=1.25, zmap=None, L=6, nbins=(40, 
     are (z, y, x).  Coordinates in [-N/2, N/2) are used as given (the
     reference's ``normalize_coordinates`` is the identity for them by its
     documented contract).  ``device`` selects the CUDA device of the plan
-    (default: coord's device if CUDA, else the current device).
+    (default: coord's device if CUDA, else the current device).  ``tile``
+    overrides the tile extent ((z, y, x)); ``autotune_batch=B`` times the tile /
+    chunk candidates for B coils and keeps the fastest (cached on disk).
     """
     flat, offs, readout, dshape = _frames_from_coord(coord)
     ndim = int(flat.shape[-1])
@@ -259,6 +279,11 @@ def plan_nufft(coord, shape, width=4, oversamp=1.25, zmap=None, L=6, nbins=(40, 
         zs = c.to(torch.complex64).contiguous()
         if L_batch_size is None:
             L_batch_size = L
-    return NUFFTPlan(ndim, tuple(float(o) for o in oversamp), tuple(int(w) for w in width),
+    plan = NUFFTPlan(ndim, tuple(float(o) for o in oversamp), tuple(int(w) for w in width),
                      tuple(float(b) for b in beta), tuple(os_shape), tuple(int(s) for s in shape),
                      interp, zt, zs, L_batch_size, dev)
+    if autotune_batch:
+        from ._autotune import autotune
+
+        autotune(plan, batch=int(autotune_batch))
+    return plan

@@ -102,8 +102,9 @@ struct pfb_plan {
     float *d_cos[pfb::kMaxDim] = {nullptr, nullptr, nullptr};  // bin-sorted oversampled coords
     int *d_perm = nullptr;       // sorted position -> global sample index
     int *d_sframe = nullptr;     // sorted position -> frame
-    int *d_bin_start = nullptr;  // (nbins_total * F + 1) offsets into the sorted order
+    int *d_bin_start = nullptr;  // (nbins_total * ncode * F + 1) offsets into the sorted order
     int nbins_total = 0;
+    int ncode = 1;               // 2^ndim edge codes per tile (which next tiles a footprint reaches)
     std::vector<int> bin_start;  // host copy
     pfb::SpreadItem *d_items_frame = nullptr;  // per (bin, frame) runs
     int n_items_frame = 0;
@@ -268,9 +269,9 @@ int launch_crop_deapod(const pfb_plan *p, const ApplyDesc &d, const float2 *grid
 
 // Gram helpers
 int launch_embed(int ndim, const int *n, const int *nos, const float2 *img, float2 *grid,
-                 int64_t nplanes, cudaStream_t s);
+                 int64_t nplanes, const float2 *Cl, int L, cudaStream_t s);
 int launch_extract(int ndim, const int *n, const int *nos, const float2 *grid, float2 *img,
-                   int64_t nplanes, float factor, cudaStream_t s);
+                   int64_t nplanes, float factor, const float2 *Cl, int L, cudaStream_t s);
 int launch_mix(int64_t gvol, int K, int lowrank, int64_t batch, const float2 *T, float2 *grid,
                cudaStream_t s);
 

@@ -344,18 +344,42 @@ __device__ __forceinline__ void warp_taps(const InterpIL &P, int64_t j, float *s
     }
 }
 
+template <int D>
+__host__ __device__ constexpr int ipow(int b) { return D == 1 ? b : (D == 2 ? b * b : b * b * b); }
+
+// Per-sample tap list in the warp's shared memory: element offset (point * nch)
+// and weight of every tap of the WM^D box; taps beyond the kernel widths get
+// weight 0 and offset 0 (an in-bounds address).  Lanes build 32 taps at a time.
+template <int D, int WM>
+__device__ __forceinline__ void build_tap_list(const InterpIL &P, const float *sw, const int *sp, int nch,
+                                               int *s_off, float *s_wt, int lane) {
+    constexpr int NT = ipow<D>(WM);
+    const int nx = P.g.nos[0], nxy = P.g.nos[0] * P.g.nos[1];
+    for (int t = lane; t < NT; t += 32) {
+        const int ix = t % WM, iy = (t / WM) % WM, iz = t / (WM * WM);
+        const bool ok = ix < P.g.w[0] && (D < 2 || iy < P.g.w[1]) && (D < 3 || iz < P.g.w[2]);
+        float w = 0.f;
+        int off = 0;
+        if (ok) {
+            w = sw[ix] * (D > 1 ? sw[WM + iy] : 1.f) * (D > 2 ? sw[2 * WM + iz] : 1.f);
+            off = (sp[ix] + (D > 1 ? sp[WM + iy] * nx : 0) + (D > 2 ? sp[2 * WM + iz] * nxy : 0)) * nch;
+        }
+        s_off[t] = off;
+        s_wt[t] = w;
+    }
+}
+
 template <int D, int WM>
 __global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const InterpIL P) {
+    constexpr int NT = ipow<D>(WM);
     __shared__ float s_w[kTileWarps][3 * WM];
     __shared__ int s_p[kTileWarps][3 * WM];
+    __shared__ int s_off[kTileWarps][NT];
+    __shared__ float s_wt[kTileWarps][NT];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cw = P.cw, lcw = log2i(cw), tg_n = 32 >> lcw;
     const int cl = lane & (cw - 1), tg = lane >> lcw;
     const int nch = P.ch.nch;
-    const int64_t nx = P.g.nos[0], nxy = (int64_t)P.g.nos[0] * P.g.nos[1];
-    const int wx_ = P.g.w[0], wy_ = D > 1 ? P.g.w[1] : 1, wz_ = D > 2 ? P.g.w[2] : 1;
-    constexpr int WY = D > 1 ? WM : 1, WZ = D > 2 ? WM : 1;
-    (void)WZ;
     // each CTA takes a contiguous run of bin-sorted samples: its warps gather
     // from the same few tiles, which stay in L1
     const int64_t per = (P.mtot + gridDim.x - 1) / gridDim.x;
@@ -363,55 +387,18 @@ __global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const Interp
     for (int64_t j = jbeg + warp; j < jend; j += kTileWarps) {
         warp_taps<D, WM, false>(P, j, s_w[warp], s_p[warp], nullptr, lane);
         __syncwarp();
+        build_tap_list<D, WM>(P, s_w[warp], s_p[warp], nch, s_off[warp], s_wt[warp], lane);
+        __syncwarp();
         const int grp = P.ch.K ? 0 : P.sframe[j];
         const float2 *G = P.grid + (int64_t)grp * P.g.gvol * nch;
-        // this lane's x taps: ix = tg, tg + tg_n, ... (weight 0 beyond the width)
-        float wxr[WM];
-        int pxr[WM];
-#pragma unroll
-        for (int m = 0; m < WM; ++m) {
-            int ix = tg + m * tg_n;
-            bool ok = ix < wx_;
-            wxr[m] = ok ? s_w[warp][ix] : 0.f;
-            pxr[m] = ok ? s_p[warp][ix] : 0;
-        }
         for (int c0 = 0; c0 < nch; c0 += cw) {
             const int c = c0 + cl;
-            const int cc = c < nch ? c : nch - 1;  // in-bounds address; result discarded
+            const float2 *Gc = G + (c < nch ? c : nch - 1);  // in-bounds address; result discarded
             float2 acc = make_float2(0.f, 0.f);
-            const float2 *Gc = G + cc;
-            if constexpr (WM == 4) {
-                // all taps unrolled: every gather is issued before the FMAs need it
-#pragma unroll
-                for (int r = 0; r < WZ * WY; ++r) {
-                    const int iz = r / WY, iy = r - (r / WY) * WY;
-                    const bool ok = iz < wz_ && iy < wy_;
-                    const float wzy = ok ? (D > 2 ? s_w[warp][2 * WM + iz] : 1.f) * (D > 1 ? s_w[warp][WM + iy] : 1.f) : 0.f;
-                    const int prow = ok ? (D > 2 ? s_p[warp][2 * WM + iz] * (int)nxy : 0) + (D > 1 ? s_p[warp][WM + iy] * (int)nx : 0) : 0;
-#pragma unroll
-                    for (int m = 0; m < WM; ++m) {
-                        if (tg + m * tg_n < WM) {
-                            const float2 v = __ldg(Gc + (int64_t)(prow + pxr[m]) * nch);
-                            acc = cfma(wzy * wxr[m], v, acc);
-                        }
-                    }
-                }
-            } else {
-                for (int iz = 0; iz < wz_; ++iz) {
-                    const float wz = D > 2 ? s_w[warp][2 * WM + iz] : 1.f;
-                    const int pz = D > 2 ? s_p[warp][2 * WM + iz] * (int)nxy : 0;
-                    for (int iy = 0; iy < wy_; ++iy) {
-                        const float wzy = wz * (D > 1 ? s_w[warp][WM + iy] : 1.f);
-                        const int prow = pz + (D > 1 ? s_p[warp][WM + iy] * (int)nx : 0);
-#pragma unroll
-                        for (int m = 0; m < WM; ++m) {
-                            if (tg + m * tg_n < WM) {
-                                const float2 v = __ldg(Gc + (int64_t)(prow + pxr[m]) * nch);
-                                acc = cfma(wzy * wxr[m], v, acc);
-                            }
-                        }
-                    }
-                }
+#pragma unroll 8
+            for (int t = tg; t < NT; t += tg_n) {
+                const float2 v = __ldg(Gc + s_off[warp][t]);
+                acc = cfma(s_wt[warp][t], v, acc);
             }
             // reduce over tap groups (lanes that share the channel)
             for (int off = cw; off < 32; off <<= 1) {
@@ -501,6 +488,7 @@ struct SpreadIL {
     const float *cos0, *cos1, *cos2;
     const int *bin_start;
     int nframes;
+    int ncode;
     const OwnerItem *items;
     const float2 *vals;   // [M][nch]
     const float *wtap;    // [M][D * WM] kernel weights per sample
@@ -517,14 +505,15 @@ __device__ __forceinline__ int tile_coord(int bin, int a, const Geom &g) {
     return bin / (g.nbins[0] * g.nbins[1]);
 }
 
-// the sorted-order range of bin `bin` for frame f (per_frame) or all frames
-__device__ __forceinline__ void bin_range(const SpreadIL &P, int bin, int f, int *s0, int *s1) {
+// the sorted-order range of key (bin, code) for frame f (per_frame) or all frames
+__device__ __forceinline__ void bin_range(const SpreadIL &P, int bin, int code, int f, int *s0, int *s1) {
+    const int k0 = (bin * P.ncode + code) * P.nframes;
     if (P.per_frame) {
-        *s0 = P.bin_start[bin * P.nframes + f];
-        *s1 = P.bin_start[bin * P.nframes + f + 1];
+        *s0 = P.bin_start[k0 + f];
+        *s1 = P.bin_start[k0 + f + 1];
     } else {
-        *s0 = P.bin_start[bin * P.nframes];
-        *s1 = P.bin_start[(bin + 1) * P.nframes];
+        *s0 = P.bin_start[k0];
+        *s1 = P.bin_start[k0 + P.nframes];
     }
 }
 
@@ -562,10 +551,13 @@ __global__ void __launch_bounds__(256) taps_prep_kernel(Geom g, const float *__r
 template <int D, int WM>
 __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const SpreadIL P) {
     extern __shared__ float acc[];
+    constexpr int NT = ipow<D>(WM);
     __shared__ float s_w[kSpreadWarps][3 * WM];
     __shared__ int s_x[kSpreadWarps][3];
-    __shared__ int s_pre[(1 << D) + 1];   // prefix sums of the neighbour range sizes
-    __shared__ int s_beg[1 << D];
+    constexpr int NR = D == 1 ? 3 : (D == 2 ? 9 : 27);  // (neighbour, edge code) ranges
+    __shared__ int s_pre[NR + 1];   // prefix sums of the range sizes
+    __shared__ int s_beg[NR];
+    __shared__ int s_dlt[NR];
     const OwnerItem it = P.items[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cw = P.cw, lcw = log2i(cw), tg_n = 32 >> lcw;
@@ -592,6 +584,11 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
     const int T0 = P.g.tile[0], T1 = D > 1 ? P.g.tile[1] : 1, T2 = D > 2 ? P.g.tile[2] : 1;
     const int tpts = T0 * T1 * T2;
     int *s_pos = reinterpret_cast<int *>(acc + tpts * pitch);  // FFT-layout position of each tile point
+    // per-warp compact tap lists (after the tile and the position table)
+    int *s_li_base = s_pos + tpts;
+    float *s_tw_base = reinterpret_cast<float *>(s_li_base + kSpreadWarps * NT);
+    int *s_li_w = s_li_base + warp * NT;
+    float *s_tw_w = s_tw_base + warp * NT;
     for (int e = threadIdx.x; e < tpts * pitch; e += blockDim.x) acc[e] = 0.f;
     for (int pt = threadIdx.x; pt < tpts; pt += blockDim.x) {
         int t0 = pt % T0, rest = pt / T0, t1 = rest % T1, t2 = rest / T1;
@@ -603,11 +600,12 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
         }
         s_pos[pt] = pos;
     }
-    // neighbour bins: tile minus delta, delta in {0,1}^D (no wrap onto itself)
-    const int nrng = 1 << D;
+    // samples of the neighbour bins t - delta, delta in {0,1}^D (no wrap onto
+    // itself), whose edge code contains delta: exactly those reaching this tile
+    int nrng = 0;
     if (threadIdx.x == 0) {
         int run = 0;
-        for (int dlt = 0; dlt < nrng; ++dlt) {
+        for (int dlt = 0; dlt < (1 << D); ++dlt) {
             int bin = 0, stride = 1;
             bool ok = true;
             for (int a = 0; a < D; ++a) {
@@ -619,22 +617,33 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
                 bin += tc * stride;
                 stride *= nb;
             }
-            int s0 = 0, s1 = 0;
-            if (ok) bin_range(P, bin, it.frame < 0 ? 0 : it.frame, &s0, &s1);
-            s_pre[dlt] = run;
-            s_beg[dlt] = s0;
-            run += s1 - s0;
+            if (!ok) continue;
+            for (int code = 0; code < (1 << D); ++code) {
+                if ((code & dlt) != dlt) continue;
+                int s0, s1;
+                bin_range(P, bin, code, it.frame < 0 ? 0 : it.frame, &s0, &s1);
+                s_pre[nrng] = run;
+                s_beg[nrng] = s0;
+                s_dlt[nrng] = dlt;
+                run += s1 - s0;
+                ++nrng;
+            }
         }
-        s_pre[nrng] = run;
+        for (int q = nrng; q <= NR; ++q) s_pre[q] = run;
     }
     __syncthreads();
     constexpr int DW = D * WM;
-    constexpr int MX = WM;  // x taps a lane may own (all of them when it is the only tap group)
     // virtual index v in [it.v0, it.v1) over the concatenated neighbour ranges
     for (int v = it.v0 + warp; v < it.v1; v += kSpreadWarps) {
-        int r = 0;
-#pragma unroll
-        for (int q = 1; q < (1 << D); ++q) r += v >= s_pre[q] ? 1 : 0;
+        // range r: the last one whose prefix is <= v (binary search; empty
+        // ranges share their prefix with the next one and are skipped)
+        int lo_r = 0, hi_r = NR;  // s_pre[lo_r] <= v < s_pre[hi_r]
+        while (hi_r - lo_r > 1) {
+            const int mid = (lo_r + hi_r) >> 1;
+            if (s_pre[mid] <= v) lo_r = mid; else hi_r = mid;
+        }
+        const int r = lo_r;
+        const int dl = s_dlt[r];
         const int64_t j = (int64_t)s_beg[r] + (v - s_pre[r]);
         if (lane < DW) s_w[warp][lane] = P.wtap[j * DW + lane];
         if (lane < D) s_x[warp][lane] = P.xtap[j * D + lane];
@@ -643,45 +652,46 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
         __syncwarp();
         // tile-local offset of x0 per axis; a sample of the lower neighbour (bit a
         // of r) lies before the origin, across the periodic wrap for the first tile
-        int lo[3], ilo[3], ihi[3];
+        int lo[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
+            lo[a] = 0;
             if (a < D) {
                 int d = s_x[warp][a] - org[a];
-                if (((r >> a) & 1) && d >= 0) d -= P.g.nos[a];
+                if (((dl >> a) & 1) && d >= 0) d -= P.g.nos[a];
                 lo[a] = d;
-                const int w = P.g.w[a];
-                ilo[a] = wrap[a] ? 0 : max(0, -d);
-                ihi[a] = wrap[a] ? w : min(w, text[a] - d);
-            } else {
-                lo[a] = 0;
-                ilo[a] = 0;
-                ihi[a] = 1;
             }
         }
+        // compact list of this sample's taps that fall inside the tile:
+        // (shared-memory row index * pitch, weight)
+        int n_in = 0;
+        for (int base = 0; base < NT; base += 32) {
+            const int t = base + lane;
+            const int ix = t % WM, iy = (t / WM) % WM, iz = t / (WM * WM);
+            bool ok = t < NT && ix < P.g.w[0] && (D < 2 || iy < P.g.w[1]) && (D < 3 || iz < P.g.w[2]);
+            int x = lo[0] + ix, y = D > 1 ? lo[1] + iy : 0, z = D > 2 ? lo[2] + iz : 0;
+            if (wrap[0] && x >= wrap[0]) x -= wrap[0];
+            if (D > 1 && wrap[1] && y >= wrap[1]) y -= wrap[1];
+            if (D > 2 && wrap[2] && z >= wrap[2]) z -= wrap[2];
+            ok = ok && x >= 0 && x < text[0] && y >= 0 && y < text[1] && z >= 0 && z < text[2];
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int k = n_in + __popc(m & ((1u << lane) - 1u));
+                s_li_w[k] = ((z * T1 + y) * T0 + x) * pitch;
+                s_tw_w[k] = s_w[warp][ix] * (D > 1 ? s_w[warp][WM + iy] : 1.f) *
+                                (D > 2 ? s_w[warp][2 * WM + iz] : 1.f);
+            }
+            n_in += __popc(m);
+        }
+        __syncwarp();
         if (c < nch) {
-            for (int iz = ilo[2]; iz < ihi[2]; ++iz) {
-                const float wz = D > 2 ? s_w[warp][2 * WM + iz] : 1.f;
-                int z = lo[2] + iz;
-                if (wrap[2] && z >= wrap[2]) z -= wrap[2];
-                for (int iy = ilo[1]; iy < ihi[1]; ++iy) {
-                    const float wyz = wz * (D > 1 ? s_w[warp][WM + iy] : 1.f);
-                    int y = lo[1] + iy;
-                    if (wrap[1] && y >= wrap[1]) y -= wrap[1];
-                    float *row = acc + (z * T1 + y) * T0 * pitch + cl;
-#pragma unroll
-                    for (int m = 0; m < MX; ++m) {
-                        const int ix = tg + m * tg_n;
-                        if (ix >= ilo[0] && ix < ihi[0]) {
-                            const float w = wyz * s_w[warp][ix];
-                            int x = lo[0] + ix;
-                            if (wrap[0] && x >= wrap[0]) x -= wrap[0];
-                            float *dst = row + x * pitch;
-                            atomicAdd(dst, w * val.x);
-                            atomicAdd(dst + cw, w * val.y);
-                        }
-                    }
-                }
+            float *a0 = acc + cl;
+#pragma unroll 4
+            for (int k = tg; k < n_in; k += tg_n) {
+                const int li = s_li_w[k];
+                const float w = s_tw_w[k];
+                atomicAdd(a0 + li, w * val.x);
+                atomicAdd(a0 + li + cw, w * val.y);
             }
         }
         __syncwarp();
@@ -818,10 +828,20 @@ size_t tile_points(const pfb_plan *p) {
 constexpr size_t kSpreadSmem = 200 * 1024;
 
 // the spread's channel chunk: as many of the (power-of-two) lanes as fit
+// bytes of the per-warp tap lists of the spread (WM^D taps, offset + weight)
+size_t spread_list_bytes(const pfb_plan *p) {
+    int nt = 1, wm = wm_of(p->g);
+    for (int a = 0; a < p->g.ndim; ++a) nt *= wm;
+    return (size_t)kSpreadWarps * nt * (sizeof(int) + sizeof(float));
+}
+
+size_t spread_smem(const pfb_plan *p, int cw) {
+    return tile_points(p) * ((2 * cw + 1) * sizeof(float) + sizeof(int)) + spread_list_bytes(p);
+}
+
 int spread_cw(const pfb_plan *p, const Chan &c) {
-    const size_t tpts = tile_points(p);
     int cw = std::min(32, pow2ceil(c.nch));
-    while (cw > 1 && tpts * ((2 * cw + 1) * sizeof(float) + sizeof(int)) > kSpreadSmem) cw >>= 1;
+    while (cw > 1 && spread_smem(p, cw) > kSpreadSmem) cw >>= 1;
     return cw;
 }
 
@@ -842,7 +862,7 @@ int fast_supported(const pfb_plan *p, const ApplyDesc &d, std::string *why) {
         if (why) *why = "too many channels for the interleaved path";
         return 0;
     }
-    if (tile_points(p) * (3 * sizeof(float) + sizeof(int)) > kSpreadSmem) {
+    if (spread_smem(p, 1) > kSpreadSmem) {
         if (why) *why = "tile too large";
         return 0;
     }
@@ -1010,6 +1030,7 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             S.cos2 = p->d_cos[2];
             S.bin_start = p->d_bin_start;
             S.nframes = p->nframes;
+            S.ncode = p->ncode;
             S.items = items;
             S.vals = samp;
             S.wtap = wtap;
@@ -1018,7 +1039,7 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             S.ch = c;
             S.cw = spread_cw(p, c);
             S.per_frame = basis ? 0 : 1;
-            const size_t smem = tile_points(p) * ((2 * S.cw + 1) * sizeof(float) + sizeof(int));
+            const size_t smem = spread_smem(p, S.cw);
             const int nchunks = (c.nch + S.cw - 1) / S.cw;
 #define PFB_S4(DD) launch_spread_il_t<DD, 4>(S, nitems, nchunks, smem, s)
 #define PFB_S8(DD) launch_spread_il_t<DD, 8>(S, nitems, nchunks, smem, s)
@@ -1135,8 +1156,14 @@ void owner_items_for(const pfb_plan *p, bool per_frame, int chunk, std::vector<O
                     stride *= g.nbins[a];
                 }
                 if (!ok) continue;
-                if (per_frame) total += bs[bin * F + f + 1] - bs[bin * F + f];
-                else total += bs[(bin + 1) * F] - bs[bin * F];
+                // only the samples whose footprint crosses into this tile along
+                // every axis of delta: edge codes that contain delta
+                for (int code = 0; code < (1 << D); ++code) {
+                    if ((code & dlt) != dlt) continue;
+                    const int k0 = (bin * p->ncode + code) * F;
+                    if (per_frame) total += bs[k0 + f + 1] - bs[k0 + f];
+                    else total += bs[k0 + F] - bs[k0];
+                }
             }
             int fr = per_frame ? f : -1;
             if (total <= chunk) {

@@ -45,6 +45,7 @@ __global__ void scale_and_key_kernel(ScaleParams P, const float *__restrict__ co
     }
     int bin = 0;
     int stride = 1;
+    int code = 0;  // bit a: the kernel footprint crosses into the next tile along axis a
     for (int a = 0; a < P.ndim; ++a) {
         float c = coord[g * P.ndim + a];
         // float32 multiply then add, each rounded (no contraction into an FMA)
@@ -56,10 +57,15 @@ __global__ void scale_and_key_kernel(ScaleParams P, const float *__restrict__ co
         }
         long long x0 = start_index(cos_, P.w[a], P.cart[a]);
         int x0m = pmod(x0, P.nos[a]);
-        bin += (x0m / P.tile[a]) * stride;
+        const int tb = x0m / P.tile[a];
+        bin += tb * stride;
         stride *= P.nbins[a];
+        const int local = x0m - tb * P.tile[a];
+        const int text = min(P.tile[a], P.nos[a] - tb * P.tile[a]);
+        if (P.nbins[a] > 1 && local + P.w[a] - 1 >= text) code |= 1 << a;
     }
-    keys[g] = bin * P.nframes + lo;
+    // sort key: (tile, edge code) major, frame minor
+    keys[g] = ((bin << P.ndim) | code) * P.nframes + lo;
     vals[g] = (int)g;
 }
 
@@ -169,20 +175,25 @@ void free_plan_buffers(pfb_plan *p) {
     p->d_frame_off = nullptr;
 }
 
-void build_items(const std::vector<int> &bs, int nbins, int nframes, int chunk, bool per_frame,
+// keys are ((bin * ncode + code) * nframes + frame): the samples of one tile
+// and frame sit in ncode runs (one per edge code)
+void build_items(const std::vector<int> &bs, int nbins, int ncode, int nframes, int chunk, bool per_frame,
                  std::vector<SpreadItem> &items) {
     items.clear();
     for (int b = 0; b < nbins; ++b) {
-        if (per_frame) {
-            for (int f = 0; f < nframes; ++f) {
-                int s0 = bs[b * nframes + f], s1 = bs[b * nframes + f + 1];
+        for (int c = 0; c < ncode; ++c) {
+            const int k0 = (b * ncode + c) * nframes;
+            if (per_frame) {
+                for (int f = 0; f < nframes; ++f) {
+                    int s0 = bs[k0 + f], s1 = bs[k0 + f + 1];
+                    for (int s = s0; s < s1; s += chunk)
+                        items.push_back({s, std::min(s1, s + chunk), b, f});
+                }
+            } else {
+                int s0 = bs[k0], s1 = bs[k0 + nframes];
                 for (int s = s0; s < s1; s += chunk)
-                    items.push_back({s, std::min(s1, s + chunk), b, f});
+                    items.push_back({s, std::min(s1, s + chunk), b, -1});
             }
-        } else {
-            int s0 = bs[b * nframes], s1 = bs[(b + 1) * nframes];
-            for (int s = s0; s < s1; s += chunk)
-                items.push_back({s, std::min(s1, s + chunk), b, -1});
         }
     }
 }
@@ -191,8 +202,8 @@ void build_items(const std::vector<int> &bs, int nbins, int nframes, int chunk, 
 
 int rebuild_items(pfb_plan *p, int chunk) {
     std::vector<SpreadItem> a, b;
-    build_items(p->bin_start, p->nbins_total, p->nframes, chunk, true, a);
-    build_items(p->bin_start, p->nbins_total, p->nframes, chunk, false, b);
+    build_items(p->bin_start, p->nbins_total, p->ncode, p->nframes, chunk, true, a);
+    build_items(p->bin_start, p->nbins_total, p->ncode, p->nframes, chunk, false, b);
     cudaFree(p->d_items_frame);
     cudaFree(p->d_items_all);
     p->d_items_frame = p->d_items_all = nullptr;
@@ -271,7 +282,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
         g.nvol *= g.n[a];
         nbins_total *= g.nbins[a];
     }
-    if (nbins_total * nframes >= (int64_t)1 << 30) {
+    if ((nbins_total << ndim) * nframes >= (int64_t)1 << 30) {
         delete p;
         return fail(PFB_ERR_INVALID, "too many (tile, frame) bins; use a larger tile");
     }
@@ -292,7 +303,8 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
     int *d_keys = nullptr, *d_vals = nullptr, *d_keys_sorted = nullptr, *d_bad = nullptr;
     void *d_temp = nullptr;
     size_t temp_bytes = 0;
-    int nkeys = (int)(nbins_total * nframes);
+    p->ncode = 1 << ndim;
+    int nkeys = (int)(nbins_total * p->ncode * nframes);
     const int T = 256;
 
     auto cleanup = [&](int code) {

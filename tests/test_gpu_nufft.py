@@ -103,7 +103,7 @@ def test_all_samples_in_one_tile_and_chunking():
     # every first tap x0 = ceil(2c + 62) in [56, 63]: one 32-wide tile on both axes
     coord = ((rng.random((1, 4000, 2)) - 1.0) * 3.0 + 0.49).astype(np.float32)
     gplan = check_pair(coord, (N, N), crandn(rng, 3, N, N), crandn(rng, 3, 1, 4000), oversamp=2.0)
-    assert gplan.interpolator.max_bin >= 3000
+    assert gplan.interpolator.max_bin >= 1000  # 4000 samples in one tile, split over <= 4 edge codes
 
 
 def test_multiframe_and_weights():
@@ -256,3 +256,28 @@ def test_cuda_graph_capture():
     g.replay()
     torch.cuda.synchronize()
     assert rel(out, ref.cpu().numpy()) < 1e-6
+
+
+def test_autotune_keeps_results_and_caches(tmp_path, monkeypatch):
+    """Tuning changes the tile / chunk, never the result; the choice is cached."""
+    import json
+
+    P = pf()
+    monkeypatch.setenv("PYFOURIER_B200_CACHE", str(tmp_path / "tune.json"))
+    rng = np.random.default_rng(16)
+    N = 64
+    coord = radial(40, 128, N)
+    x = crandn(rng, 3, N, N)
+    y = crandn(rng, 3, 40, 128)
+    oplan = orc.plan_nufft(coord, (N, N), width=4, oversamp=2.0)
+    plan = P.plan_nufft(torch.as_tensor(coord), (N, N), width=4, oversamp=2.0, device="cuda:0")
+    res = P.autotune(plan, batch=3, tiles=[(16, 16), (32, 32)], chunks=[256, 4096], iters=1)
+    assert res["cached"] is False and tuple(res["tile"]) in {(16, 16), (32, 32)}
+    assert rel(P.nufft(torch.as_tensor(x).cuda(), nufft_plan=plan), orc.nufft_fwd(x, oplan)) < TOL
+    assert rel(P.nufft_adj(torch.as_tensor(y).cuda(), nufft_plan=plan), orc.nufft_adj(y, oplan)) < TOL
+    cache = json.loads((tmp_path / "tune.json").read_text())
+    assert len(cache) == 1
+    plan2 = P.plan_nufft(torch.as_tensor(coord), (N, N), width=4, oversamp=2.0, device="cuda:0")
+    res2 = P.autotune(plan2, batch=3)
+    assert res2["cached"] is True and list(res2["tile"]) == list(res["tile"])
+    assert rel(P.nufft(torch.as_tensor(x).cuda(), nufft_plan=plan2), orc.nufft_fwd(x, oplan)) < TOL
