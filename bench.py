@@ -186,6 +186,20 @@ def cpu_baseline(wl, coord, coils_sample, steps=1):
 # --------------------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------------------
+def count_launches(torch, fn):
+    """Kernels one call of ``fn`` launches, from a CUDA activity trace taken
+    outside the timed region: (this library's kernels, all kernels)."""
+    from torch.profiler import ProfilerActivity, profile
+
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    names = [e.name for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA
+             and "memcpy" not in e.name.lower() and "memset" not in e.name.lower()]
+    return sum("pfb::" in n for n in names), len(names)
+
+
 def stage_times(torch, pf, plan, x, iters):
     """Per-kernel CUDA-event timings of one forward + adjoint, stage by stage
     through the C ABI (pfb_nufft_stage), on the launching stream."""
@@ -312,6 +326,7 @@ def gpu_arm(args, wl, rank, world, local_rank):
     d2h = yk.numel() * 8 + xa.numel() * 8
     del x_host, yk, xa
 
+    mine_l, all_l = (None, None) if args.no_launch_trace else count_launches(torch, lambda: step(x))
     stages = stage_times(torch, pf, plan, x, max(3, args.steps))
     alg = algorithmic_bytes(wl, plan, B)
     mine = {k: v for k, v in stages.items() if k in alg}
@@ -323,7 +338,8 @@ def gpu_arm(args, wl, rank, world, local_rank):
                 "traffic": NCU_TRAFFIC.get((args.workload, dom)),
                 "algorithmic_bytes": alg[dom]}
     return dict(ms=ms, value=value, e2e=world * samples_per_step / e2e_s, h2d=h2d, d2h=d2h, stages=stages,
-                roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=8)
+                roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=mine_l,
+                kernels_per_step=all_l)
 
 
 # --------------------------------------------------------------------------------------
@@ -543,6 +559,11 @@ def extra_workload(args):
                     config={"workload": "loss ||A^H A x - x||^2 with image and trajectory gradients",
                             "image": [N, N], "coils": B, "images": nimg, "interleaves": 16, "samples": 4096},
                     cpu_baseline=None)
+    launch_fn = batched if args.workload == "cfg4" else step
+    if not args.no_launch_trace:
+        mine_l, all_l = count_launches(torch, launch_fn)
+        line["gpu_launches"] = mine_l * args.steps
+        line["kernels_per_step"] = {"pyfourier_b200": mine_l, "all (incl. cuFFT, torch)": all_l}
     line["clocks"] = clk
     print(json.dumps(line), flush=True)
 
@@ -561,6 +582,8 @@ def main():
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg1", "cfg3", "cfg4", "cfg5"])
     ap.add_argument("--cpu-coils", type=int, default=2, help="coils in the bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-launch-trace", action="store_true",
+                    help="skip the CUDA activity trace that counts launches (for runs under ncu)")
     args = ap.parse_args()
     if args.workload in ("cfg1", "cfg3", "cfg4", "cfg5"):
         extra_workload(args)
@@ -616,7 +639,9 @@ def main():
                 "vs_baseline": None, "dtype": "complex64", "data": "synthetic (seeded)", "config": config,
                 "e2e": {"value": r["e2e"], "unit": "samples/s", "h2d_bytes_per_step": r["h2d"],
                         "d2h_bytes_per_step": r["d2h"]},
-                "gpu_launches": r["launches_per_step"] * args.steps,
+                "gpu_launches": (r["launches_per_step"] or 0) * args.steps,
+                "kernels_per_step": {"pyfourier_b200": r["launches_per_step"],
+                                     "all (incl. cuFFT)": r["kernels_per_step"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "clocks": r["clocks"]}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -252,18 +252,22 @@ int pfb_nufft_stage(pfb_plan *plan, const pfb_apply_t *opt, int stage, const voi
  *   ncoeff  K (low rank) or number of kernel planes (elementwise);
  *   lowrank 1: kernel is (prod(os_shape), K, K) with out[v] = T[v] @ in[v];
  *           0: kernel is (ncoeff, prod(os_shape)) applied elementwise;
+ *   nseg    B0 time segments L (1 without field map): the kernel then holds
+ *           L such kernels, one per segment;
  *   kernel  device complex64, uncentred (ifftshift-ed) layout, copied.
  * Replaces GramMatrix (src/pyfourier/_sparsegram/_plan.py:253-270). */
 int pfb_gram_create(int ndim, const int *shape, const int *os_shape, int ncoeff, int lowrank,
-                    const void *kernel, int device, void *stream, pfb_gram **out);
+                    int nseg, const void *kernel, int device, void *stream, pfb_gram **out);
 int pfb_gram_destroy(pfb_gram *gram);
 int pfb_gram_workspace_size(pfb_gram *gram, int64_t batch, size_t *bytes);
 
 /* Apply: image (batch, ncoeff, *shape) -> out (same).  Zero-pad into the 2x grid,
- * FFT, per-voxel K x K mix (or elementwise product), inverse FFT, crop.
+ * FFT, per-voxel K x K mix (or elementwise product), inverse FFT, crop.  With
+ * B0 segments, out = sum_l conj(C_l) G_l(C_l x) with b0_space = C (L, prod(shape)),
+ * complex64 (NULL without segments).
  * Replaces _sparsegram / _do_sparsegram / _bdot
  * (src/pyfourier/_sparsegram/_sparsegram.py:11-81, _bmatvec/_bdot.py:16-115). */
-int pfb_gram_apply(pfb_gram *gram, const void *image, void *out, int64_t batch,
+int pfb_gram_apply(pfb_gram *gram, const void *image, void *out, int64_t batch, const void *b0_space,
                    void *workspace, size_t workspace_bytes, void *stream);
 
 #ifdef __cplusplus

@@ -272,7 +272,30 @@ def ifft_c(x, ndim, norm=None, centered=True):
 # --------------------------------------------------------------------------------------
 # B0 time segmentation
 # --------------------------------------------------------------------------------------
-def mri_exp_approx(zmap, t, L=6, bins=(40, 40)):
+def _acorr_hist(hk, c0, c1=None):
+    """Histogram of z(r') + conj(z(r)) over pixel pairs, from the histogram of z.
+
+    Real (B0) axis: differences c0[i] - c0[j] (an autocorrelation).  R2* axis:
+    sums c1[i] + c1[j] (a self-convolution).  This is the Toeplitz form of the
+    histogram (the commented ``acorr`` branch of _subroutines/_b0.py:86-106).
+    """
+    if c1 is None:
+        h = np.correlate(hk, hk, mode="full")  # index i - j + n - 1
+        d0 = c0[1] - c0[0]
+        zk = 1j * d0 * np.arange(-(len(c0) - 1), len(c0))
+        return h, zk
+    n0, n1 = hk.shape
+    h = np.zeros((2 * n0 - 1, 2 * n1 - 1))
+    i0, i1 = np.nonzero(hk)
+    for a0, a1 in zip(i0, i1):
+        # pixel pairs (a, b): B0 index a0 - b0 + n0 - 1, R2* index a1 + b1
+        h[a0 - np.arange(n0)[:, None] + n0 - 1, a1 + np.arange(n1)[None, :]] += hk[a0, a1] * hk
+    d0, d1 = c0[1] - c0[0], (c1[1] - c1[0]) if n1 > 1 else 0.0
+    zk = 1j * d0 * np.arange(-(n0 - 1), n0)[:, None] + (2 * c1[0] + d1 * np.arange(2 * n1 - 1))[None, :]
+    return h, zk
+
+
+def mri_exp_approx(zmap, t, L=6, bins=(40, 40), acorr=False):
     """_subroutines/_b0.py:10-135 in float64, with three intent fixes.
 
     * bin centres are the midpoints of the histogram edges (the shipped
@@ -281,6 +304,8 @@ def mri_exp_approx(zmap, t, L=6, bins=(40, 40)):
       coefficients C_l = exp(-z t_l) (the shipped code fits exp(+z t));
     * a real map is histogrammed on its values (the shipped code histograms the
       complexified map).
+    ``acorr=True`` fits the basis over the histogram of z(r') + conj(z(r))
+    (for the Toeplitz Gram), the reference's commented branch.
     Returns (B (L, nt) complex128, C (L, *zmap.shape) complex128).
     """
     zmap = np.asarray(zmap)
@@ -290,13 +315,20 @@ def mri_exp_approx(zmap, t, L=6, bins=(40, 40)):
     if np.isrealobj(zmap):
         z = 2 * math.pi * 1j * zmap.astype(np.float64)
         hk, ze = np.histogram(2 * math.pi * zmap.ravel().astype(np.float64), bins=int(bins[0]))
-        zk = 1j * 0.5 * (ze[1:] + ze[:-1])
+        c0 = 0.5 * (ze[1:] + ze[:-1])
+        if acorr:
+            hk, zk = _acorr_hist(hk.astype(np.float64), c0)
+        else:
+            zk = 1j * c0
     else:
         z = 2 * math.pi * zmap.astype(np.complex128)
         zz = z.ravel()
         hk, e0, e1 = np.histogram2d(zz.imag, zz.real, bins=[int(bins[0]), int(bins[1])])
         c0, c1 = 0.5 * (e0[1:] + e0[:-1]), 0.5 * (e1[1:] + e1[:-1])
-        zk = (1j * c0[:, None] + c1[None, :])
+        if acorr:
+            hk, zk = _acorr_hist(hk.astype(np.float64), c0, c1)
+        else:
+            zk = (1j * c0[:, None] + c1[None, :])
     hk = hk.ravel().astype(np.float64)
     zk = zk.ravel()
     tl = np.linspace(0, L, L) / L * t[-1]
@@ -475,13 +507,15 @@ def nufft_adj(kspace, plan, basis=None, weight=None, norm=None):
 # --------------------------------------------------------------------------------------
 @dataclass
 class OracleGram:
-    value: object  # (F, *os) elementwise, or (nvox, K, K) per-voxel matrices
+    value: object  # (F, *os) elementwise, or (nvox, K, K) per-voxel matrices; leading L with a field map
     shape: tuple
     ndim: int
     islowrank: bool
+    zmap_s_kernel: object = None  # (L, *shape) spatial B0 coefficients C_l
 
 
-def plan_spgram(coord, shape, basis=None, weight=None, width=6, normalize="reference"):
+def plan_spgram(coord, shape, basis=None, weight=None, width=6, normalize="reference", zmap=None, L=6,
+                nbins=(40, 40), dt=None, T=None):
     """_sparsegram/_plan.py:20-249 with its intent fixes.
 
     PSF = adjoint NUFFT of ``weight * delta`` at 2x coordinates onto the 2N
@@ -491,6 +525,11 @@ def plan_spgram(coord, shape, basis=None, weight=None, width=6, normalize="refer
     evident intent of _bmatvec/_bdot.py).  ``normalize="reference"`` divides by
     mean(|T| over T != 0) (:242); ``normalize=None`` scales T so that the Gram
     equals A^H W A with A = nufft(norm=None) and A^H its exact adjoint.
+    With a field map (:162-182, :26-53 of _sparsegram.py) there is one kernel per
+    time segment, built with the sample weights B_l(t), and the apply is
+    sum_l conj(C_l) G_l(C_l x); B and C come from the autocorrelated histogram
+    (``mri_exp_approx(..., acorr=True)``), which approximates the pairwise
+    phase exp(-(z(r') + conj(z(r))) t) that the Gram needs.
     """
     coord = np.asarray(coord, np.float32)
     ndim = coord.shape[-1]
@@ -507,6 +546,15 @@ def plan_spgram(coord, shape, basis=None, weight=None, width=6, normalize="refer
                                 (K, *coord.shape[:-1])).astype(np.complex64)
     else:
         delta = np.ones(coord.shape[:-1], np.complex64)
+    Cl = None
+    if zmap is not None:
+        if T is None:
+            T = dt * np.arange(coord.shape[-2], dtype=np.float32)
+        Bt, Cl = mri_exp_approx(zmap, T, L, nbins, acorr=True)
+        # segment l weights each sample by B_l(t) of its readout position (last axis)
+        Bl = Bt.astype(np.complex64).reshape(L, *([1] * (delta.ndim - 1)), Bt.shape[-1])
+        delta = delta[None] * Bl
+        Cl = Cl.astype(np.complex64)
     pplan = plan_nufft(coord * osf[::-1], os_shape, width=width, oversamp=1.25)
     psf = nufft_adj((wgt * delta).astype(np.complex64), pplan, basis)
     G_os = float(np.prod(pplan.os_shape))
@@ -515,21 +563,39 @@ def plan_spgram(coord, shape, basis=None, weight=None, width=6, normalize="refer
         T = fft_c(psf, ndim, norm=None)
     else:
         T = fft_c(psf, ndim, norm="ortho")
-    if basis is None and T.ndim > ndim and T.shape[0] == 1:
-        T = T[0]
+    nlead = 1 if zmap is not None else 0
+    if basis is None and T.ndim > ndim + nlead and T.shape[nlead] == 1:
+        T = T[:, 0] if nlead else T[0]
     T = np.fft.ifftshift(T, axes=tuple(range(-ndim, 0)))
     if basis is not None:
         K = basis.shape[1]
-        T = np.ascontiguousarray(T.reshape(K, K, -1).transpose(2, 1, 0))  # (nvox, k2, k1)
+        T = T.reshape(-1, K, K, int(np.prod(os_shape)))
+        T = np.ascontiguousarray(T.transpose(0, 3, 2, 1))  # (L, nvox, k2, k1)
+        if not nlead:
+            T = T[0]
     if normalize == "reference":
         nz = T[T != 0]
         T = T / np.mean(np.abs(nz))
     T = np.nan_to_num(T).astype(np.complex64)
-    return OracleGram(T, tuple(os_shape), ndim, basis is not None)
+    return OracleGram(T, tuple(os_shape), ndim, basis is not None, Cl)
 
 
 def sparse_gram(image, gram, norm=None):
-    """_sparsegram/_sparsegram.py:59-81 with the per-voxel product out = T[v] @ in."""
+    """_sparsegram/_sparsegram.py:11-81 with the per-voxel product out = T[v] @ in;
+    with a field map sum_l conj(C_l) G_l(C_l x)."""
+    image = np.asarray(image, np.complex64)
+    if gram.zmap_s_kernel is not None:
+        C = gram.zmap_s_kernel
+        nd = gram.ndim
+        out = 0
+        for l in range(C.shape[0]):
+            gl = OracleGram(gram.value[l], gram.shape, gram.ndim, gram.islowrank)
+            out = out + np.conj(C[l]) * _sparse_gram1(C[l] * image, gl, norm)
+        return np.asarray(out, np.complex64)
+    return _sparse_gram1(image, gram, norm)
+
+
+def _sparse_gram1(image, gram, norm=None):
     image = np.asarray(image, np.complex64)
     nd = gram.ndim
     shape = image.shape[-nd:]

@@ -22,11 +22,31 @@ import numpy as np
 import torch
 
 
-def mri_exp_approx(zmap, t, lseg=6, bins=(40, 40), mask=None):
+def _pair_histogram(hk, c0, c1=None):
+    """Histogram of z(r') + conj(z(r)) over pixel pairs, from the histogram of z:
+    differences of the B0 values (an autocorrelation of the histogram) and sums
+    of the R2* values (a self-convolution).  Returns (counts, complex values)."""
+    if c1 is None:
+        h = np.correlate(hk, hk, mode="full")
+        zk = 1j * (c0[1] - c0[0]) * np.arange(-(len(c0) - 1), len(c0))
+        return h, zk
+    n0, n1 = hk.shape
+    h = np.zeros((2 * n0 - 1, 2 * n1 - 1))
+    for a0, a1 in zip(*np.nonzero(hk)):
+        h[a0 - np.arange(n0)[:, None] + n0 - 1, a1 + np.arange(n1)[None, :]] += hk[a0, a1] * hk
+    d1 = (c1[1] - c1[0]) if n1 > 1 else 0.0
+    zk = 1j * (c0[1] - c0[0]) * np.arange(-(n0 - 1), n0)[:, None] + (2 * c1[0] + d1 * np.arange(2 * n1 - 1))[None, :]
+    return h, zk
+
+
+def mri_exp_approx(zmap, t, lseg=6, bins=(40, 40), mask=None, acorr=False):
     """Return ``(B, C)``: B (lseg, nt) complex128 and C (lseg, *zmap.shape) complex128.
 
     ``zmap`` and ``t`` may be numpy arrays or torch tensors; B is returned as a
     numpy array, C as a torch tensor on zmap's device (numpy if zmap is numpy).
+    ``acorr=True`` fits B over the pair histogram of z(r') + conj(z(r)) instead
+    of the histogram of z, the form the Toeplitz Gram needs (the reference
+    keeps this branch commented out, src/pyfourier/_subroutines/_b0.py:86-106).
     """
     is_torch = isinstance(zmap, torch.Tensor)
     zt = zmap if is_torch else torch.as_tensor(np.asarray(zmap))
@@ -41,13 +61,20 @@ def mri_exp_approx(zmap, t, lseg=6, bins=(40, 40), mask=None):
         vals = 2 * math.pi * np.asarray(zc, np.float64)
         vals = vals[mask] if mask is not None else vals.ravel()
         hk, ze = np.histogram(vals, bins=int(bins[0]))
-        zk = 1j * 0.5 * (ze[1:] + ze[:-1])
+        c0 = 0.5 * (ze[1:] + ze[:-1])
+        if acorr:
+            hk, zk = _pair_histogram(np.asarray(hk, np.float64), c0)
+        else:
+            zk = 1j * c0
     else:
         z = 2 * math.pi * np.asarray(zc, np.complex128)
         z = z[mask] if mask is not None else z.ravel()
         hk, e0, e1 = np.histogram2d(z.imag, z.real, bins=[int(bins[0]), int(bins[1])])
         c0, c1 = 0.5 * (e0[1:] + e0[:-1]), 0.5 * (e1[1:] + e1[:-1])
-        zk = 1j * c0[:, None] + c1[None, :]
+        if acorr:
+            hk, zk = _pair_histogram(np.asarray(hk, np.float64), c0, c1)
+        else:
+            zk = 1j * c0[:, None] + c1[None, :]
     hk = np.asarray(hk, np.float64).ravel()
     zk = np.asarray(zk, np.complex128).ravel()
     t64 = tt.numpy()

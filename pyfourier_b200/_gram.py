@@ -27,12 +27,13 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._b0 import mri_exp_approx
 from ._nufft import nufft_adj
 from ._plan import _as_tensor, plan_nufft, resolve_device
 
 
 class _GramHandle:
-    def __init__(self, ndim, shape, os_shape, ncoeff, lowrank, kernel, device):
+    def __init__(self, ndim, shape, os_shape, ncoeff, lowrank, nseg, kernel, device):
         L = _lib.load()
         self.device = torch.device(device)
         h = ctypes.c_void_p()
@@ -40,8 +41,8 @@ class _GramHandle:
         with torch.cuda.device(self.device):
             s = torch.cuda.current_stream(self.device)
             _lib.check(L.pfb_gram_create(ndim, _lib.int_array(shape), _lib.int_array(os_shape), int(ncoeff),
-                                         int(lowrank), ctypes.c_void_p(k.data_ptr()), self.device.index,
-                                         ctypes.c_void_p(s.cuda_stream), ctypes.byref(h)))
+                                         int(lowrank), int(nseg), ctypes.c_void_p(k.data_ptr()),
+                                         self.device.index, ctypes.c_void_p(s.cuda_stream), ctypes.byref(h)))
         self.handle = h
 
     def __del__(self):
@@ -76,27 +77,42 @@ class GramMatrix:
         device = resolve_device(device, self.device)
         if self.device is None or device != self.device or self._handle is None:
             self.value = self.value.to(device)
+            if self.zmap_s_kernel is not None:
+                self.zmap_s_kernel = self.zmap_s_kernel.to(device)
             self.device = device
             self._handle = None
         return self
 
+    @property
+    def nseg(self):
+        return 1 if self.zmap_s_kernel is None else int(self.zmap_s_kernel.shape[0])
+
+    @property
+    def ncoeff(self):
+        """Image planes per batch item: K (low rank) or frames (elementwise, 1 if none)."""
+        if self.islowrank:
+            return int(self.value.shape[-1])
+        lead = 1 if self.zmap_s_kernel is not None else 0
+        return 1 if self.value.ndim == self.ndim + lead else int(self.value.shape[lead])
+
     def handle(self):
         if self._handle is None:
-            if self.islowrank:
-                ncoeff = self.value.shape[-1]
-            else:
-                ncoeff = 1 if self.value.ndim == self.ndim else self.value.shape[0]
-            self._handle = _GramHandle(self.ndim, self.image_shape, self.shape, ncoeff, self.islowrank,
-                                       self.value, self.device)
+            self._handle = _GramHandle(self.ndim, self.image_shape, self.shape, self.ncoeff, self.islowrank,
+                                       self.nseg, self.value, self.device)
         return self._handle
 
 
 def plan_spgram(coord, shape, basis=None, zmap=None, L=6, nbins=(40, 40), dt=None, T=None,
                 L_batch_size=None, weight=None, oversamp=None, width=6, device="cpu",
                 normalize="reference"):
-    """Toeplitz kernel of A^H W A (src/pyfourier/_sparsegram/_plan.py:20-249)."""
-    if zmap is not None:
-        raise NotImplementedError("plan_spgram with a field map is not implemented in this build")
+    """Toeplitz kernel of A^H W A (src/pyfourier/_sparsegram/_plan.py:20-249).
+
+    With a field map (:162-182) there is one kernel per time segment l, built
+    from the sample weights B_l(t), and the apply is sum_l conj(C_l) G_l(C_l x)
+    (_sparsegram/_sparsegram.py:26-53); B and C are fitted over the pair
+    histogram of the field map (``mri_exp_approx(..., acorr=True)``), which is
+    what the Gram's pairwise phase exp(-(z(r') + conj(z(r))) t) needs.
+    """
     coord_t = _as_tensor(coord, torch.float32)
     dev = resolve_device(device, coord_t.device)
     coord_t = coord_t.to(dev)
@@ -119,6 +135,18 @@ def plan_spgram(coord, shape, basis=None, zmap=None, L=6, nbins=(40, 40), dt=Non
     else:
         basis_t = None
         delta = torch.ones(coord_t.shape[:-1], dtype=torch.complex64, device=dev)
+    zs = None
+    if zmap is not None:
+        if T is None:
+            if dt is None:
+                raise ValueError("Please provide raster time dt if T is not known")
+            T = dt * np.arange(coord_t.shape[-2], dtype=np.float32)
+        bt, zs = mri_exp_approx(_as_tensor(zmap).to(dev), T, L, nbins, acorr=True)
+        # segment l weights each sample by B_l(t) of its readout position (last axis)
+        bl = torch.as_tensor(bt, dtype=torch.complex64, device=dev)
+        bl = bl.reshape(L, *([1] * (delta.ndim - 1)), bl.shape[-1])
+        delta = delta[None] * bl
+        zs = zs.to(torch.complex64).contiguous()
     scale_xyz = torch.as_tensor(osf[::-1].copy(), device=dev)
     pplan = plan_nufft(coord_t * scale_xyz, os_shape, width=width, oversamp=1.25, device=dev)
     psf = nufft_adj((wgt * delta).to(torch.complex64), nufft_plan=pplan, basis=basis_t, device=dev)
@@ -129,18 +157,20 @@ def plan_spgram(coord, shape, basis=None, zmap=None, L=6, nbins=(40, 40), dt=Non
     else:
         Tk = torch.fft.fftshift(torch.fft.fftn(torch.fft.ifftshift(psf, dim=axes), dim=axes, norm="ortho"),
                                 dim=axes)
-    if basis_t is None and Tk.ndim > ndim and Tk.shape[0] == 1:
-        Tk = Tk[0]
+    nlead = 1 if zs is not None else 0
+    if basis_t is None and Tk.ndim > ndim + nlead and Tk.shape[nlead] == 1:
+        Tk = Tk[:, 0] if nlead else Tk[0]
     Tk = torch.fft.ifftshift(Tk, dim=axes)
     if basis_t is not None:
         K = basis_t.shape[1]
-        Tk = Tk.reshape(K, K, -1).permute(2, 1, 0).contiguous()  # (nvox, k2, k1)
+        Tk = Tk.reshape(-1, K, K, int(np.prod(os_shape))).permute(0, 3, 2, 1)  # (L, nvox, k2, k1)
+        Tk = Tk if nlead else Tk[0]
     if normalize == "reference":
         Tk = Tk / torch.mean(torch.abs(Tk[Tk != 0]))
     elif normalize is not None:
         raise ValueError("normalize must be 'reference' or None")
     Tk = torch.nan_to_num(Tk).to(torch.complex64).contiguous()
-    return GramMatrix(Tk, tuple(os_shape), ndim, basis_t is not None, None, L_batch_size, dev,
+    return GramMatrix(Tk, tuple(os_shape), ndim, basis_t is not None, zs, L_batch_size, dev,
                       image_shape=tuple(shape))
 
 
@@ -156,8 +186,10 @@ def _gram_core(gm: GramMatrix, x):
     _lib.check(L.pfb_gram_workspace_size(h.handle, B, ctypes.byref(n)))
     ws = torch.empty(int(n.value), dtype=torch.uint8, device=gm.device)
     st = ctypes.c_void_p(torch.cuda.current_stream(gm.device).cuda_stream)
+    zs = gm.zmap_s_kernel
+    zp = ctypes.c_void_p(zs.data_ptr()) if zs is not None else None
     _lib.check(L.pfb_gram_apply(h.handle, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()), B,
-                                ctypes.c_void_p(ws.data_ptr()), ws.numel(), st))
+                                zp, ctypes.c_void_p(ws.data_ptr()), ws.numel(), st))
     return out
 
 
@@ -192,10 +224,7 @@ def sparse_gram(image, gram_matrix, norm=None, device="cpu", threadsperblock=128
     if gm.image_shape is None:
         raise ValueError("GramMatrix has no image shape")
     nd = gm.ndim
-    if gm.islowrank:
-        C = gm.value.shape[-1]
-    else:
-        C = 1 if gm.value.ndim == nd else gm.value.shape[0]
+    C = gm.ncoeff
     xc = x_t.to(dev)
     xc = xc.to(torch.complex64) if torch.is_complex(xc) else xc.to(torch.float32).to(torch.complex64)
     if tuple(xc.shape[xc.ndim - nd:]) != tuple(gm.image_shape):

@@ -108,10 +108,10 @@ def load(path=LIB_PATH):
         "pfb_crop_deapod": (i32, [vp, P(ApplyT), vp, vp, f32, vp]),
         "pfb_grid_fft": (i32, [vp, vp, i64, i32, vp, ctypes.c_size_t, vp]),
         "pfb_traj_grad": (i32, [vp, P(ApplyT), vp, vp, vp, i32, vp]),
-        "pfb_gram_create": (i32, [i32, P(ctypes.c_int), P(ctypes.c_int), i32, i32, vp, i32, vp, P(vp)]),
+        "pfb_gram_create": (i32, [i32, P(ctypes.c_int), P(ctypes.c_int), i32, i32, i32, vp, i32, vp, P(vp)]),
         "pfb_gram_destroy": (i32, [vp]),
         "pfb_gram_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),
-        "pfb_gram_apply": (i32, [vp, vp, vp, i64, vp, ctypes.c_size_t, vp]),
+        "pfb_gram_apply": (i32, [vp, vp, vp, i64, vp, vp, ctypes.c_size_t, vp]),
         "pfb_nufft_adj_noalloc": (i32, [vp, P(ApplyT), vp, vp, vp]),
         "pfb_apply_workspace_size": (i32, [vp, P(ApplyT), P(ctypes.c_size_t)]),
         "pfb_nufft_traj_grad": (i32, [vp, P(ApplyT), vp, vp, vp, f32, vp, ctypes.c_size_t, vp]),

@@ -118,6 +118,7 @@ struct pfb_gram {
     int64_t nvol = 1, gvol = 1;
     int K = 1;
     int lowrank = 0;
+    int nseg = 1;          // B0 time segments (one kernel each)
     float2 *d_T = nullptr;
     std::mutex fft_mu;
     std::map<int64_t, cufftHandle> fft_plans;
@@ -189,7 +190,9 @@ int pfb_plan_set_tuning(pfb_plan *p, int spread_threads, int interp_threads, int
 int pfb_plan_set_chunk(pfb_plan *p, int chunk) {
     if (!p || chunk < 1) return fail(PFB_ERR_INVALID, "chunk must be >= 1");
     DeviceGuard dg(p->device);
-    return rebuild_items(p, chunk);
+    int st = rebuild_items(p, chunk);
+    if (st) return st;
+    return build_owner_items(p, chunk);
 }
 
 int pfb_plan_tables(const pfb_plan *p, int axis, int32_t *index, float *value, void *stream) {
@@ -396,11 +399,11 @@ int pfb_traj_grad(pfb_plan *p, const pfb_apply_t *opt, const void *grid, const v
                             fft_layout != 0, static_cast<cudaStream_t>(stream), opt->flags & PFB_FLAG_ACCUMULATE);
 }
 
-int pfb_gram_create(int ndim, const int *shape, const int *os_shape, int ncoeff, int lowrank, const void *kernel,
-                    int device, void *stream, pfb_gram **out) {
+int pfb_gram_create(int ndim, const int *shape, const int *os_shape, int ncoeff, int lowrank, int nseg,
+                    const void *kernel, int device, void *stream, pfb_gram **out) {
     if (!out) return fail(PFB_ERR_INVALID, "out is NULL");
     *out = nullptr;
-    if (ndim < 1 || ndim > 3 || !shape || !os_shape || !kernel || ncoeff < 1)
+    if (ndim < 1 || ndim > 3 || !shape || !os_shape || !kernel || ncoeff < 1 || nseg < 1)
         return fail(PFB_ERR_INVALID, "bad argument");
     if (lowrank && ncoeff > 8) return fail(PFB_ERR_UNSUPPORTED, "subspace size K > 8");
     DeviceGuard dg(device);
@@ -420,7 +423,9 @@ int pfb_gram_create(int ndim, const int *shape, const int *os_shape, int ncoeff,
     }
     g->K = ncoeff;
     g->lowrank = lowrank != 0;
-    size_t tbytes = (size_t)g->gvol * sizeof(float2) * (g->lowrank ? (size_t)ncoeff * ncoeff : (size_t)ncoeff);
+    g->nseg = nseg;
+    size_t tbytes = (size_t)nseg * g->gvol * sizeof(float2) *
+                    (g->lowrank ? (size_t)ncoeff * ncoeff : (size_t)ncoeff);
     cudaError_t e = cudaMalloc(&g->d_T, tbytes);
     if (e != cudaSuccess) {
         delete g;
@@ -452,7 +457,7 @@ int pfb_gram_destroy(pfb_gram *g) {
 int pfb_gram_workspace_size(pfb_gram *g, int64_t batch, size_t *bytes) {
     if (!g || !bytes || batch < 1) return fail(PFB_ERR_INVALID, "bad argument");
     DeviceGuard dg(g->device);
-    int64_t P = batch * g->K;
+    int64_t P = (int64_t)g->nseg * batch * g->K;
     cufftHandle h;
     size_t wb = 0;
     int st = get_fft_plan(g->fft_mu, g->fft_plans, g->fft_work, g->ndim, g->nos, P, &h, &wb);
@@ -461,14 +466,17 @@ int pfb_gram_workspace_size(pfb_gram *g, int64_t batch, size_t *bytes) {
     return PFB_OK;
 }
 
-int pfb_gram_apply(pfb_gram *g, const void *image, void *out, int64_t batch, void *workspace,
-                   size_t workspace_bytes, void *stream) {
+int pfb_gram_apply(pfb_gram *g, const void *image, void *out, int64_t batch, const void *b0_space,
+                   void *workspace, size_t workspace_bytes, void *stream) {
     if (!g || !image || !out || !workspace) return fail(PFB_ERR_INVALID, "NULL argument");
     if (batch < 0) return fail(PFB_ERR_INVALID, "batch < 0");
+    if (g->nseg > 1 && !b0_space) return fail(PFB_ERR_INVALID, "a Gram with B0 segments needs b0_space");
     if (batch == 0) return PFB_OK;
     DeviceGuard dg(g->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int64_t P = batch * g->K;
+    const int L = g->nseg;
+    const int64_t bk = batch * g->K;  // image planes
+    const int64_t P = L * bk;         // grid planes (segment-major)
     cufftHandle h;
     size_t wb = 0;
     int st = get_fft_plan(g->fft_mu, g->fft_plans, g->fft_work, g->ndim, g->nos, P, &h, &wb);
@@ -477,12 +485,18 @@ int pfb_gram_apply(pfb_gram *g, const void *image, void *out, int64_t batch, voi
     if (workspace_bytes < gbytes + wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
     float2 *grid = static_cast<float2 *>(workspace);
     void *work = static_cast<char *>(workspace) + gbytes;
-    if ((st = launch_embed(g->ndim, g->n, g->nos, static_cast<const float2 *>(image), grid, P, s))) return st;
+    const float2 *Cl = static_cast<const float2 *>(b0_space);
+    if ((st = launch_embed(g->ndim, g->n, g->nos, static_cast<const float2 *>(image), grid, bk, Cl, L, s)))
+        return st;
     if ((st = run_fft(h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
-    if ((st = launch_mix(g->gvol, g->K, g->lowrank, batch, g->d_T, grid, s))) return st;
+    const size_t tplane = (size_t)g->gvol * (g->lowrank ? (size_t)g->K * g->K : (size_t)g->K);
+    for (int l = 0; l < L; ++l)  // segment l's kernel on segment l's planes
+        if ((st = launch_mix(g->gvol, g->K, g->lowrank, batch, g->d_T + l * tplane, grid + l * bk * g->gvol, s)))
+            return st;
     if ((st = run_fft(h, wb, grid, +1, work, workspace_bytes - gbytes, s))) return st;
     // forward and inverse FFT scalings multiply to 1/G whatever `norm` is
-    return launch_extract(g->ndim, g->n, g->nos, grid, static_cast<float2 *>(out), P, (float)(1.0 / (double)g->gvol), s);
+    return launch_extract(g->ndim, g->n, g->nos, grid, static_cast<float2 *>(out), bk,
+                          (float)(1.0 / (double)g->gvol), Cl, L, s);
 }
 
 }  // extern "C"

@@ -106,6 +106,9 @@ struct EmbedParams {
     const float2 *src;
     float2 *dst;
     float factor;
+    const float2 *Cl;  // (L, nvol) B0 spatial coefficients or null
+    int L;             // segments (grid planes = L * bk)
+    int64_t bk;        // image planes per segment
 };
 
 __global__ void embed_kernel(const EmbedParams P) {
@@ -120,8 +123,13 @@ __global__ void embed_kernel(const EmbedParams P) {
         int q2 = (int)(rest / P.nos[1]);
         int r0 = q0 - P.off[0], r1 = q1 - P.off[1], r2 = q2 - P.off[2];
         float2 v = make_float2(0.f, 0.f);
-        if (r0 >= 0 && r0 < P.n[0] && r1 >= 0 && r1 < P.n[1] && r2 >= 0 && r2 < P.n[2])
-            v = P.src[plane * P.nvol + ((int64_t)r2 * P.n[1] + r1) * P.n[0] + r0];
+        if (r0 >= 0 && r0 < P.n[0] && r1 >= 0 && r1 < P.n[1] && r2 >= 0 && r2 < P.n[2]) {
+            // grid plane (l, image plane); the segment multiplies by C_l
+            const int64_t l = plane / P.bk, ip = plane - l * P.bk;
+            const int64_t rl = ((int64_t)r2 * P.n[1] + r1) * P.n[0] + r0;
+            v = P.src[ip * P.nvol + rl];
+            if (P.Cl) v = cmul(v, P.Cl[l * P.nvol + rl]);
+        }
         P.dst[e] = v;
     }
 }
@@ -137,7 +145,14 @@ __global__ void extract_kernel(const EmbedParams P) {
         int r1 = (int)(rest % P.n[1]);
         int r2 = (int)(rest / P.n[1]);
         int64_t pos = ((int64_t)(r2 + P.off[2]) * P.nos[1] + (r1 + P.off[1])) * P.nos[0] + (r0 + P.off[0]);
-        float2 v = P.src[plane * P.gvol + pos];
+        // sum over segments of conj(C_l) times segment l's plane
+        float2 v = make_float2(0.f, 0.f);
+        for (int l = 0; l < P.L; ++l) {
+            float2 g = P.src[((int64_t)l * P.bk + plane) * P.gvol + pos];
+            if (P.Cl) g = cmulc(g, P.Cl[(int64_t)l * P.nvol + rl]);
+            v.x += g.x;
+            v.y += g.y;
+        }
         P.dst[e] = make_float2(v.x * P.factor, v.y * P.factor);
     }
 }
@@ -252,9 +267,13 @@ static void fill_embed(int ndim, const int *n, const int *nos, EmbedParams &P) {
 }
 
 int launch_embed(int ndim, const int *n, const int *nos, const float2 *img, float2 *grid,
-                 int64_t nplanes, cudaStream_t s) {
+                 int64_t nplanes, const float2 *Cl, int L, cudaStream_t s) {
     EmbedParams P{};
     fill_embed(ndim, n, nos, P);
+    P.Cl = Cl;
+    P.L = L;
+    P.bk = nplanes;
+    nplanes *= L;
     P.nplanes = nplanes;
     P.src = img;
     P.dst = grid;
@@ -267,9 +286,12 @@ int launch_embed(int ndim, const int *n, const int *nos, const float2 *img, floa
 }
 
 int launch_extract(int ndim, const int *n, const int *nos, const float2 *grid, float2 *img,
-                   int64_t nplanes, float factor, cudaStream_t s) {
+                   int64_t nplanes, float factor, const float2 *Cl, int L, cudaStream_t s) {
     EmbedParams P{};
     fill_embed(ndim, n, nos, P);
+    P.Cl = Cl;
+    P.L = L;
+    P.bk = nplanes;
     P.nplanes = nplanes;
     P.src = grid;
     P.dst = img;

@@ -43,7 +43,7 @@ def test_status_mapping_without_gpu():
     assert b"ndim" in L.pfb_last_error()
     with pytest.raises(ValueError):
         _lib.check(st)
-    st = L.pfb_gram_create(2, None, None, 4, 1, None, 0, None, ctypes.byref(out))
+    st = L.pfb_gram_create(2, None, None, 4, 1, 1, None, 0, None, ctypes.byref(out))
     assert st == _lib.PFB_ERR_INVALID
     # NULL handles are rejected, destroy(NULL) is a no-op
     assert L.pfb_plan_destroy(None) == 0

@@ -92,6 +92,57 @@ def test_gram_autograd_self_adjoint():
     assert rel(x.grad, ref.detach().cpu().numpy()) < 1e-5
 
 
+def _b0_map(N):
+    yy, xx = np.mgrid[:N, :N] / N - 0.5
+    return 100 * np.exp(-((xx - 0.1) ** 2 + yy ** 2) / 0.05) - 50
+
+
+@pytest.mark.parametrize("subspace", [False, True])
+def test_gram_field_map_vs_oracle(subspace):
+    """Time-segmented Gram: L kernels, sum_l conj(C_l) G_l(C_l x), same as the oracle."""
+    P = pf()
+    rng = np.random.default_rng(4)
+    N, ns = 24, 64
+    dt = 5e-3 / ns
+    b0 = _b0_map(N)
+    if subspace:
+        F, K = 6, 3
+        coord = spiral_frames(F, 3, ns, N)
+        basis = np.linalg.qr(crandn(rng, F, K))[0].astype(np.complex64)
+        x = crandn(rng, 2, K, N, N)
+    else:
+        coord, basis = radial(16, ns, N), None
+        x = crandn(rng, 2, N, N)
+    og = orc.plan_spgram(coord, (N, N), basis=basis, zmap=b0, L=6, nbins=40, dt=dt)
+    gg = P.plan_spgram(torch.as_tensor(coord), (N, N), basis=None if basis is None else torch.as_tensor(basis),
+                       zmap=torch.as_tensor(b0), L=6, nbins=40, dt=dt, device="cuda:0")
+    assert gg.nseg == 6 and gg.value.shape == og.value.shape
+    assert rel(gg.value, og.value) < 1e-5
+    assert rel(gg.zmap_s_kernel, og.zmap_s_kernel) < 1e-6
+    assert rel(P.sparse_gram(torch.as_tensor(x).cuda(), gg), orc.sparse_gram(x, og)) < 1e-5
+
+
+def test_gram_field_map_vs_exact_model():
+    """normalize=None: the segmented Gram approximates E^H E of the exact
+    off-resonance model E = exp(-i 2 pi (k r + t b0(r))) (segmentation error only)."""
+    P = pf()
+    rng = np.random.default_rng(7)
+    N, nv, ns = 24, 16, 64
+    coord = radial(nv, ns, N)
+    b0 = _b0_map(N)
+    dt = 5e-3 / ns
+    gm = P.plan_spgram(torch.as_tensor(coord), (N, N), zmap=torch.as_tensor(b0), L=8, nbins=40, dt=dt,
+                       device="cuda:0", normalize=None)
+    x = crandn(rng, N, N)
+    g = P.sparse_gram(torch.as_tensor(x).cuda(), gm)
+    r = orc.pixel_grid((N, N))
+    cm = coord.reshape(-1, 2).astype(np.float64)
+    tm = np.tile(dt * np.arange(ns), nv)
+    E = np.exp(-2j * np.pi * (cm / N) @ r.T) * np.exp(-2j * np.pi * tm[:, None] * b0.ravel()[None, :])
+    ref = (E.conj().T @ (E @ x.ravel().astype(np.complex128))).reshape(N, N)
+    assert rel(g, ref) < 2e-2
+
+
 # ---------------------------------------------------------------------------------
 # autograd
 # ---------------------------------------------------------------------------------

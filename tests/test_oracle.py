@@ -155,3 +155,25 @@ def test_oracle_b0_segmentation_vs_exact():
     E = np.exp(-2j * np.pi * (cm / N) @ r.T) * np.exp(-2j * np.pi * tm[:, None] * b0.ravel()[None, :])
     y_ref = (E @ x.ravel().astype(np.complex128)).reshape(nv, ns)
     assert orc.rel_l2(y, y_ref) < 2e-3
+
+
+def test_oracle_gram_with_field_map_vs_exact():
+    """Toeplitz Gram with B0 segments approximates A^H W A of the exact
+    off-resonance model (time segmentation error only)."""
+    rng = np.random.default_rng(7)
+    N, nv, ns = 24, 16, 64
+    coord = _radial(nv, ns, N)
+    yy, xx = np.mgrid[:N, :N] / N - 0.5
+    b0 = 100 * np.exp(-((xx - 0.1) ** 2 + yy ** 2) / 0.05) - 50
+    dt = 5e-3 / ns
+    t = dt * np.arange(ns)
+    gm = orc.plan_spgram(coord, (N, N), normalize=None, zmap=b0, L=8, nbins=40, dt=dt)
+    assert gm.value.shape[0] == 8 and gm.zmap_s_kernel.shape == (8, N, N)
+    x = (rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))).astype(np.complex64)
+    g = orc.sparse_gram(x, gm)
+    r = orc.pixel_grid((N, N))
+    cm = coord.reshape(-1, 2).astype(np.float64)
+    tm = np.tile(t, nv)
+    E = np.exp(-2j * np.pi * (cm / N) @ r.T) * np.exp(-2j * np.pi * tm[:, None] * b0.ravel()[None, :])
+    ref = (E.conj().T @ (E @ x.ravel().astype(np.complex128))).reshape(N, N)
+    assert orc.rel_l2(g, ref) < 2e-2
