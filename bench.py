@@ -92,9 +92,10 @@ def coil_maps_3d(torch, N, ncoils, device):
 WORKLOADS = {
     "cfg2": dict(desc="3D golden-means radial NUFFT fwd+adj", N=200, nspokes=20000, nread=400, coils=32,
                  width=4, oversamp=1.25, nell=20),
-    # mid-size variant for profiler captures (grid 8 x 160^3 complex64 = 262 MB > L2)
+    # mid-size variant for profiler captures, same 32 channels per sample
+    # (grid 32 x 160^3 complex64 = 1.05 GB > L2, about 3.5 GB on the device)
     "cfg2-mid": dict(desc="3D golden-means radial NUFFT fwd+adj (mid)", N=128, nspokes=8000, nread=256,
-                     coils=8, width=4, oversamp=1.25, nell=20),
+                     coils=32, width=4, oversamp=1.25, nell=20),
     # reduced variant for quick checks (same construction)
     "cfg2-small": dict(desc="3D golden-means radial NUFFT fwd+adj (reduced)", N=64, nspokes=2000, nread=128,
                        coils=8, width=4, oversamp=1.25, nell=20),

@@ -75,79 +75,100 @@ struct PadPL {
     int accumulate;
 };
 
+// Both kernels walk rows of the grid / image: a warp takes a segment of up to
+// kRowSeg points of one row (no per-element divisions), lanes take consecutive
+// points, so loads and stores are coalesced along x.
+constexpr int kRowSeg = 256;
+
 // grid plane (grp, ch), FFT-layout position p -> image pixel r = (p + N//2) mod n_os, valid if r < N
 __global__ void __launch_bounds__(256) pad_pl_kernel(const PadPL P) {
-    const int64_t gvol = P.g.gvol;
-    const int64_t total = (int64_t)P.ch.ngrp * P.ch.nch * gvol;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nx = P.g.nos[0], nseg = (nx + kRowSeg - 1) / kRowSeg;
+    const int nrows = P.g.nos[1] * P.g.nos[2];
+    const int64_t units = (int64_t)nrows * nseg;
+    const int64_t u = (int64_t)blockIdx.x * 8 + warp;
+    if (u >= units) return;
+    const int row = (int)(u / nseg), seg = (int)(u - (int64_t)row * nseg);
+    const int p1 = row % P.g.nos[1], p2 = row / P.g.nos[1];
+    int r1 = p1 + P.g.n[1] / 2; r1 = r1 >= P.g.nos[1] ? r1 - P.g.nos[1] : r1;
+    int r2 = p2 + P.g.n[2] / 2; r2 = r2 >= P.g.nos[2] ? r2 - P.g.nos[2] : r2;
+    const bool inside = r1 < P.g.n[1] && r2 < P.g.n[2];
+    float arow = P.factor;
+    if (inside) {
+        if (P.apod1) arow *= P.apod1[r1];
+        if (P.apod2) arow *= P.apod2[r2];
+    }
+    const int x0 = seg * kRowSeg, x1 = min(nx, x0 + kRowSeg);
     const int Kc = P.ch.K ? P.ch.K : 1, B = P.ch.B;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        const int64_t plane = e / gvol;
-        const int64_t pos = e - plane * gvol;
-        const int grp = (int)(plane / P.ch.nch), ch = (int)(plane - (int64_t)grp * P.ch.nch);
-        const int p0 = (int)(pos % P.g.nos[0]);
-        const int64_t rest = pos / P.g.nos[0];
-        const int p1 = (int)(rest % P.g.nos[1]);
-        const int p2 = (int)(rest / P.g.nos[1]);
-        int r0 = p0 + P.g.n[0] / 2; r0 = r0 >= P.g.nos[0] ? r0 - P.g.nos[0] : r0;
-        int r1 = p1 + P.g.n[1] / 2; r1 = r1 >= P.g.nos[1] ? r1 - P.g.nos[1] : r1;
-        int r2 = p2 + P.g.n[2] / 2; r2 = r2 >= P.g.nos[2] ? r2 - P.g.nos[2] : r2;
-        float2 out = make_float2(0.f, 0.f);
-        if (r0 < P.g.n[0] && r1 < P.g.n[1] && r2 < P.g.n[2]) {
-            const int k = ch % Kc, lb = ch / Kc, b = lb % B, l = lb / B;
-            const int c = P.ch.K ? k : grp;
-            const int64_t rl = ((int64_t)r2 * P.g.n[1] + r1) * P.g.n[0] + r0;
-            float2 v = P.src[((int64_t)b * P.C + c) * P.g.nvol + rl];
-            float a = P.factor;
-            if (P.apod0) a *= P.apod0[r0];
-            if (P.apod1) a *= P.apod1[r1];
-            if (P.apod2) a *= P.apod2[r2];
-            if (P.Cl) v = cmul(v, P.Cl[(int64_t)l * P.g.nvol + rl]);
-            out = make_float2(v.x * a, v.y * a);
+    const int64_t rbase = ((int64_t)r2 * P.g.n[1] + r1) * P.g.n[0];
+    const int nplanes = P.ch.ngrp * P.ch.nch;
+    for (int plane = blockIdx.y; plane < nplanes; plane += gridDim.y) {
+        const int grp = plane / P.ch.nch, ch = plane - grp * P.ch.nch;
+        const int k = ch % Kc, lb = ch / Kc, b = lb % B, l = lb / B;
+        const int c = P.ch.K ? k : grp;
+        const float2 *src = P.src + ((int64_t)b * P.C + c) * P.g.nvol + rbase;
+        const float2 *cl = P.Cl ? P.Cl + (int64_t)l * P.g.nvol + rbase : nullptr;
+        float2 *dst = P.dst + (int64_t)plane * P.g.gvol + (int64_t)row * nx;
+        for (int p0 = x0 + lane; p0 < x1; p0 += 32) {
+            int r0 = p0 + P.g.n[0] / 2;
+            r0 = r0 >= nx ? r0 - nx : r0;
+            float2 out = make_float2(0.f, 0.f);
+            if (inside && r0 < P.g.n[0]) {
+                float2 v = src[r0];
+                if (cl) v = cmul(v, cl[r0]);
+                const float a = P.apod0 ? arow * P.apod0[r0] : arow;
+                out = make_float2(v.x * a, v.y * a);
+            }
+            dst[p0] = out;
         }
-        P.dst[e] = out;
     }
 }
 
 // image (b, c, r) = factor * apod(r) * sum_l conj(C_l(r)) * grid[plane(l, b, c)][(r - N//2) mod n_os]
 __global__ void __launch_bounds__(256) crop_pl_kernel(const PadPL P) {
-    const int64_t nvol = P.g.nvol;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n0 = P.g.n[0], nseg = (n0 + kRowSeg - 1) / kRowSeg;
+    const int nrows = P.g.n[1] * P.g.n[2];
+    const int64_t units = (int64_t)nrows * nseg;
+    const int64_t u = (int64_t)blockIdx.x * 8 + warp;
+    if (u >= units) return;
+    const int row = (int)(u / nseg), seg = (int)(u - (int64_t)row * nseg);
+    const int r1 = row % P.g.n[1], r2 = row / P.g.n[1];
+    int p1 = r1 - P.g.n[1] / 2; p1 = p1 < 0 ? p1 + P.g.nos[1] : p1;
+    int p2 = r2 - P.g.n[2] / 2; p2 = p2 < 0 ? p2 + P.g.nos[2] : p2;
+    float arow = P.factor;
+    if (P.apod1) arow *= P.apod1[r1];
+    if (P.apod2) arow *= P.apod2[r2];
+    const int x0 = seg * kRowSeg, x1 = min(n0, x0 + kRowSeg);
     const int B = P.ch.B, L = P.ch.L, Kc = P.ch.K ? P.ch.K : 1;
-    const int64_t total = (int64_t)B * P.C * nvol;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        const int64_t bc = e / nvol;
-        const int64_t rl = e - bc * nvol;
-        const int b = (int)(bc / P.C), c = (int)(bc - (int64_t)b * P.C);
-        const int r0 = (int)(rl % P.g.n[0]);
-        const int64_t rest = rl / P.g.n[0];
-        const int r1 = (int)(rest % P.g.n[1]);
-        const int r2 = (int)(rest / P.g.n[1]);
-        int p0 = r0 - P.g.n[0] / 2; p0 = p0 < 0 ? p0 + P.g.nos[0] : p0;
-        int p1 = r1 - P.g.n[1] / 2; p1 = p1 < 0 ? p1 + P.g.nos[1] : p1;
-        int p2 = r2 - P.g.n[2] / 2; p2 = p2 < 0 ? p2 + P.g.nos[2] : p2;
-        const int64_t pos = ((int64_t)p2 * P.g.nos[1] + p1) * P.g.nos[0] + p0;
+    const int64_t gbase = ((int64_t)p2 * P.g.nos[1] + p1) * P.g.nos[0];
+    const int64_t rbase = (int64_t)row * n0;
+    const int nbc = B * P.C;
+    for (int bc = blockIdx.y; bc < nbc; bc += gridDim.y) {
+        const int b = bc / P.C, c = bc - b * P.C;
         const int grp = P.ch.K ? 0 : c;
-        float2 acc = make_float2(0.f, 0.f);
-        for (int l = 0; l < L; ++l) {
-            const int ch = P.ch.K ? (l * B + b) * Kc + c : l * B + b;
-            float2 v = P.src[((int64_t)grp * P.ch.nch + ch) * P.g.gvol + pos];
-            if (P.Cl) v = cmulc(v, P.Cl[(int64_t)l * nvol + rl]);
-            acc.x += v.x;
-            acc.y += v.y;
+        float2 *dst = P.dst + (int64_t)bc * P.g.nvol + rbase;
+        for (int r0 = x0 + lane; r0 < x1; r0 += 32) {
+            int p0 = r0 - n0 / 2;
+            p0 = p0 < 0 ? p0 + P.g.nos[0] : p0;
+            float2 acc = make_float2(0.f, 0.f);
+            for (int l = 0; l < L; ++l) {
+                const int ch = P.ch.K ? (l * B + b) * Kc + c : l * B + b;
+                float2 v = P.src[((int64_t)grp * P.ch.nch + ch) * P.g.gvol + gbase + p0];
+                if (P.Cl) v = cmulc(v, P.Cl[(int64_t)l * P.g.nvol + rbase + r0]);
+                acc.x += v.x;
+                acc.y += v.y;
+            }
+            const float a = P.apod0 ? arow * P.apod0[r0] : arow;
+            acc.x *= a;
+            acc.y *= a;
+            if (P.accumulate) {
+                const float2 o = dst[r0];
+                acc.x += o.x;
+                acc.y += o.y;
+            }
+            dst[r0] = acc;
         }
-        float a = P.factor;
-        if (P.apod0) a *= P.apod0[r0];
-        if (P.apod1) a *= P.apod1[r1];
-        if (P.apod2) a *= P.apod2[r2];
-        acc.x *= a;
-        acc.y *= a;
-        if (P.accumulate) {
-            float2 o = P.dst[e];
-            acc.x += o.x;
-            acc.y += o.y;
-        }
-        P.dst[e] = acc;
     }
 }
 
@@ -174,6 +195,46 @@ __global__ void __launch_bounds__(256) transpose_kernel(const float2 *__restrict
         int c = c0 + cl;
         int64_t p = p0 + pl;
         if (c < nch && p < gvol) Dd[p * nch + c] = sm[cl * (tp + 1) + pl];
+    }
+}
+
+// Wide form for 32-channel chunks: a tile of 64 points x 32 channels; a warp
+// reads 64 consecutive points of one channel (512 B, as float4 when the planes
+// are 16-byte aligned) and writes the 32 channels of one point (256 B).
+__global__ void __launch_bounds__(256) transpose32_kernel(const float2 *__restrict__ src, float2 *__restrict__ dst,
+                                                          int64_t gvol, int nch, int vec) {
+    __shared__ float2 sm[32][64 + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = blockIdx.z;
+    const int64_t p0 = (int64_t)blockIdx.x * 64;
+    const int c0 = blockIdx.y * 32;
+    const float2 *S = src + (int64_t)grp * nch * gvol;
+    float2 *Dd = dst + (int64_t)grp * nch * gvol;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int cl = warp + 8 * q, c = c0 + cl;
+        if (c >= nch) continue;
+        const int64_t p = p0 + 2 * lane;
+        const float2 *row = S + (int64_t)c * gvol;
+        float2 a = make_float2(0.f, 0.f), b = a;
+        if (vec && p + 1 < gvol) {
+            const float4 v = __ldg(reinterpret_cast<const float4 *>(row + p));
+            a = make_float2(v.x, v.y);
+            b = make_float2(v.z, v.w);
+        } else {
+            if (p < gvol) a = row[p];
+            if (p + 1 < gvol) b = row[p + 1];
+        }
+        sm[cl][2 * lane] = a;
+        sm[cl][2 * lane + 1] = b;
+    }
+    __syncthreads();
+    const int c = c0 + lane;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int pl = warp + 8 * q;
+        const int64_t p = p0 + pl;
+        if (c < nch && p < gvol) Dd[p * nch + c] = sm[lane][pl];
     }
 }
 
@@ -347,10 +408,12 @@ __device__ __forceinline__ void warp_taps(const InterpIL &P, int64_t j, float *s
 template <int D>
 __host__ __device__ constexpr int ipow(int b) { return D == 1 ? b : (D == 2 ? b * b : b * b * b); }
 
-// Per-sample tap list in the warp's shared memory: element offset (point * nch)
-// and weight of every tap of the WM^D box; taps beyond the kernel widths get
-// weight 0 and offset 0 (an in-bounds address).  Lanes build 32 taps at a time.
-template <int D, int WM>
+// Per-sample tap list in the warp's shared memory: the tap's offset and weight
+// for every tap of the WM^D box; taps beyond the kernel widths get weight 0 and
+// offset 0 (an in-bounds address).  The offset is the element offset point * nch
+// when that fits in 32 bits (WIDE = false), else the point index.  Lanes build
+// 32 taps at a time.
+template <int D, int WM, bool WIDE>
 __device__ __forceinline__ void build_tap_list(const InterpIL &P, const float *sw, const int *sp, int nch,
                                                int *s_off, float *s_wt, int lane) {
     constexpr int NT = ipow<D>(WM);
@@ -362,14 +425,15 @@ __device__ __forceinline__ void build_tap_list(const InterpIL &P, const float *s
         int off = 0;
         if (ok) {
             w = sw[ix] * (D > 1 ? sw[WM + iy] : 1.f) * (D > 2 ? sw[2 * WM + iz] : 1.f);
-            off = (sp[ix] + (D > 1 ? sp[WM + iy] * nx : 0) + (D > 2 ? sp[2 * WM + iz] * nxy : 0)) * nch;
+            off = sp[ix] + (D > 1 ? sp[WM + iy] * nx : 0) + (D > 2 ? sp[2 * WM + iz] * nxy : 0);
+            if (!WIDE) off *= nch;
         }
         s_off[t] = off;
         s_wt[t] = w;
     }
 }
 
-template <int D, int WM>
+template <int D, int WM, bool WIDE>
 __global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const InterpIL P) {
     constexpr int NT = ipow<D>(WM);
     __shared__ float s_w[kTileWarps][3 * WM];
@@ -387,17 +451,17 @@ __global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const Interp
     for (int64_t j = jbeg + warp; j < jend; j += kTileWarps) {
         warp_taps<D, WM, false>(P, j, s_w[warp], s_p[warp], nullptr, lane);
         __syncwarp();
-        build_tap_list<D, WM>(P, s_w[warp], s_p[warp], nch, s_off[warp], s_wt[warp], lane);
-        __syncwarp();
         const int grp = P.ch.K ? 0 : P.sframe[j];
         const float2 *G = P.grid + (int64_t)grp * P.g.gvol * nch;
+        build_tap_list<D, WM, WIDE>(P, s_w[warp], s_p[warp], nch, s_off[warp], s_wt[warp], lane);
+        __syncwarp();
         for (int c0 = 0; c0 < nch; c0 += cw) {
             const int c = c0 + cl;
             const float2 *Gc = G + (c < nch ? c : nch - 1);  // in-bounds address; result discarded
             float2 acc = make_float2(0.f, 0.f);
 #pragma unroll 8
             for (int t = tg; t < NT; t += tg_n) {
-                const float2 v = __ldg(Gc + s_off[warp][t]);
+                const float2 v = WIDE ? __ldg(Gc + (int64_t)s_off[warp][t] * nch) : __ldg(Gc + s_off[warp][t]);
                 acc = cfma(s_wt[warp][t], v, acc);
             }
             // reduce over tap groups (lanes that share the channel)
@@ -662,6 +726,46 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
                 lo[a] = d;
             }
         }
+        if (tg_n == 1) {
+            // lanes are 32 channels: walk the box of this sample's taps that lies
+            // inside the tile, axis by axis (warp-uniform bounds, unrolled taps)
+            int i0[3], i1[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                i0[a] = 0;
+                i1[a] = 1;
+                if (a < D) {
+                    i0[a] = wrap[a] ? 0 : max(0, -lo[a]);
+                    i1[a] = wrap[a] ? P.g.w[a] : min(P.g.w[a], text[a] - lo[a]);
+                }
+            }
+            float wx[WM];
+#pragma unroll
+            for (int i = 0; i < WM; ++i) wx[i] = s_w[warp][i];
+            float *a0 = acc + cl;
+            for (int iz = i0[2]; iz < i1[2]; ++iz) {
+                int z = lo[2] + iz;
+                if (D > 2 && wrap[2] && z >= wrap[2]) z -= wrap[2];
+                const float wz = D > 2 ? s_w[warp][2 * WM + iz] : 1.f;
+                for (int iy = i0[1]; iy < i1[1]; ++iy) {
+                    int y = lo[1] + iy;
+                    if (D > 1 && wrap[1] && y >= wrap[1]) y -= wrap[1];
+                    const float wzy = wz * (D > 1 ? s_w[warp][WM + iy] : 1.f);
+                    const float vx = wzy * val.x, vy = wzy * val.y;
+                    float *row = a0 + (z * T1 + y) * T0 * pitch;
+#pragma unroll
+                    for (int ix = 0; ix < WM; ++ix) {
+                        if (ix < i0[0] || ix >= i1[0]) continue;
+                        int x = lo[0] + ix;
+                        if (wrap[0] && x >= wrap[0]) x -= wrap[0];
+                        atomicAdd(row + x * pitch, wx[ix] * vx);
+                        atomicAdd(row + x * pitch + cw, wx[ix] * vy);
+                    }
+                }
+            }
+            __syncwarp();
+            continue;
+        }
         // compact list of this sample's taps that fall inside the tile:
         // (shared-memory row index * pitch, weight)
         int n_in = 0;
@@ -711,6 +815,238 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
             if (it.atomic) atomicAdd(G + pos, vv);
             else G[pos] = vv;
         }
+    }
+}
+
+// Register-tile spread for 3D tiles of up to 8 x 8 x 8 points and 32 channels per
+// CTA (tile points are packed 8 per axis whatever the tile extent).  Each of the
+// 16 warps owns a 4 x 4 x 2 block of the tile and keeps its 32 points x (its
+// lane's channel) in registers, so no two warps ever write the same point and
+// no atomics are needed.  Samples go through shared memory in batches: their
+// raw rows (channel values, kernel weights, first taps) arrive by cp.async one
+// batch ahead; then lanes (axis, t) turn them into tile-relative weight vectors
+// w_x[0..8), w_y, w_z (zero outside the support and outside the tile) with a
+// 24-bit mask of the non-zero entries, by which each warp picks (ballot) the
+// samples that touch its block.  The tile leaves through shared memory,
+// coalesced along x.
+constexpr int kRegBatch = 128;                // samples per staged batch
+constexpr int kRegTile = 8;                   // packed tile extent per axis
+constexpr int kRegPts = kRegTile * kRegTile * kRegTile;
+// one staging buffer: raw values [B][32] f2, raw weights [B][24] f, raw first
+// taps [B][4] i, neighbour bits [B] i, tile weights [B][24] f, masks [B] u
+constexpr size_t kRegOffW = (size_t)kRegBatch * 32 * sizeof(float2);
+constexpr size_t kRegOffX = kRegOffW + (size_t)kRegBatch * 24 * sizeof(float);
+constexpr size_t kRegOffD = kRegOffX + (size_t)kRegBatch * 4 * sizeof(int);
+constexpr size_t kRegOffTW = kRegOffD + (size_t)kRegBatch * sizeof(int);
+constexpr size_t kRegOffM = kRegOffTW + (size_t)kRegBatch * 24 * sizeof(float);
+constexpr size_t kRegBuf = kRegOffM + (size_t)kRegBatch * sizeof(unsigned);
+constexpr size_t kRegSmemOut = (size_t)kRegPts * 33 * sizeof(float2);
+constexpr size_t kRegSmem = kRegPts * sizeof(int) + (kRegSmemOut > 2 * kRegBuf ? kRegSmemOut : 2 * kRegBuf);
+static_assert(kRegBuf % 16 == 0 && kRegOffTW % 16 == 0, "16-byte aligned staging arrays");
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+// 8-byte copy; valid = false writes zeros (nothing is read)
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <int WM>
+__global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const SpreadIL P) {
+    static_assert(kSpreadWarps == 16, "16 warps own the 2 x 2 x 4 blocks of the tile");
+    constexpr int D = 3, DW = D * WM;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    int *s_pos = reinterpret_cast<int *>(smraw);
+    unsigned char *ub = smraw + kRegPts * sizeof(int);
+    float2 *s_out = reinterpret_cast<float2 *>(ub);  // [512][33], after the last batch
+    constexpr int NR = 27;
+    __shared__ int s_pre[NR + 1];
+    __shared__ int s_beg[NR];
+    __shared__ int s_dlt[NR];
+    const OwnerItem it = P.items[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nch = P.ch.nch;
+    const int c0 = blockIdx.y * 32, c = c0 + lane;
+    int org[3], text[3], wrap[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int tc = tile_coord(it.tile, a, P.g);
+        org[a] = tc * P.g.tile[a];
+        text[a] = min(P.g.tile[a], P.g.nos[a] - org[a]);
+        wrap[a] = P.g.nbins[a] == 1 ? text[a] : 0;
+    }
+    for (int pt = threadIdx.x; pt < kRegPts; pt += blockDim.x) {
+        const int t0 = pt & 7, t1 = (pt >> 3) & 7, t2 = pt >> 6;
+        int pos = -1;
+        if (t0 < text[0] && t1 < text[1] && t2 < text[2]) {
+            pos = pmod(org[0] + t0 - P.g.sh[0], P.g.nos[0]) +
+                  pmod(org[1] + t1 - P.g.sh[1], P.g.nos[1]) * P.g.nos[0] +
+                  pmod(org[2] + t2 - P.g.sh[2], P.g.nos[2]) * P.g.nos[0] * P.g.nos[1];
+        }
+        s_pos[pt] = pos;
+    }
+    if (threadIdx.x == 0) {
+        int run = 0, nrng = 0;
+        for (int dlt = 0; dlt < 8; ++dlt) {
+            int bin = 0, stride = 1;
+            bool ok = true;
+            for (int a = 0; a < D; ++a) {
+                const int da = (dlt >> a) & 1, nb = P.g.nbins[a];
+                if (da && nb == 1) ok = false;
+                int tc = tile_coord(it.tile, a, P.g) - da;
+                tc = tc < 0 ? tc + nb : tc;
+                bin += tc * stride;
+                stride *= nb;
+            }
+            if (!ok) continue;
+            for (int code = 0; code < 8; ++code) {
+                if ((code & dlt) != dlt) continue;
+                int s0, s1;
+                bin_range(P, bin, code, it.frame < 0 ? 0 : it.frame, &s0, &s1);
+                s_pre[nrng] = run;
+                s_beg[nrng] = s0;
+                s_dlt[nrng] = dlt;
+                run += s1 - s0;
+                ++nrng;
+            }
+        }
+        for (int q = nrng; q <= NR; ++q) s_pre[q] = run;
+    }
+    __syncthreads();
+    const int nvis = it.v1 - it.v0;
+    const int nbat = (nvis + kRegBatch - 1) / kRegBatch;
+    auto batch_size = [&](int bb) { return (nvis - bb + nbat - 1) / nbat; };
+    // issue the copies of batch bb into buffer buf (warps take samples warp, warp + 16, ...)
+    auto issue = [&](int bb, int buf) {
+        unsigned char *B = ub + buf * kRegBuf;
+        float2 *rv = reinterpret_cast<float2 *>(B);
+        float *rw = reinterpret_cast<float *>(B + kRegOffW);
+        int *rx = reinterpret_cast<int *>(B + kRegOffX);
+        int *rd = reinterpret_cast<int *>(B + kRegOffD);
+        const int nb = batch_size(bb);
+        for (int q = warp; q < nb; q += kSpreadWarps) {
+            // batch bb takes visits bb, bb + nbat, bb + 2 nbat, ...: every batch
+            // mixes the neighbour ranges, so all warps find work in it
+            const int v = it.v0 + bb + q * nbat;
+            // range: the last one whose prefix is <= v (empty ranges share the
+            // prefix of the next one and are skipped)
+            const unsigned le = __ballot_sync(0xffffffffu, lane < NR && s_pre[lane] <= v);
+            const int r = 31 - __clz(le);
+            const int64_t j = (int64_t)s_beg[r] + (v - s_pre[r]);
+            cp_async8(rv + q * 32 + lane, P.vals + j * nch + (c < nch ? c : 0), c < nch);
+            if (lane < DW) cp_async4(rw + q * 24 + lane, P.wtap + j * DW + lane);
+            if (lane < D) cp_async4(rx + q * 4 + lane, P.xtap + j * D + lane);
+            if (lane == 0) rd[q] = s_dlt[r];
+        }
+    };
+    // this warp's block and its bits in the sample masks
+    const int bx0 = (warp & 1) * 4, by0 = ((warp >> 1) & 1) * 4, bz0 = (warp >> 2) * 2;
+    const unsigned bmx = 0xFu << bx0, bmy = 0xFu << (8 + by0), bmz = 0x3u << (16 + bz0);
+    // lane (a, t): tile coordinate t on axis a (lanes 0..23)
+    const int la = lane >> 3, lt = lane & 7;
+    const int orga = la == 0 ? org[0] : (la == 1 ? org[1] : org[2]);
+    const int texta = la == 0 ? text[0] : (la == 1 ? text[1] : text[2]);
+    const int wrapa = la == 0 ? wrap[0] : (la == 1 ? wrap[1] : wrap[2]);
+    const int nosa = la == 0 ? P.g.nos[0] : (la == 1 ? P.g.nos[1] : P.g.nos[2]);
+    const int wa = la == 0 ? P.g.w[0] : (la == 1 ? P.g.w[1] : P.g.w[2]);
+    float ax[32], ay[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+        ax[q] = 0.f;
+        ay[q] = 0.f;
+    }
+    if (nbat > 0) issue(0, 0);
+    cp_async_commit();
+    for (int b = 0; b < nbat; ++b) {
+        const int cur = b & 1;
+        cp_async_wait_all();
+        __syncthreads();  // batch b landed; every warp is done with batch b - 1
+        if (b + 1 < nbat) issue(b + 1, cur ^ 1);
+        cp_async_commit();
+        unsigned char *B = ub + cur * kRegBuf;
+        const float2 *rv = reinterpret_cast<const float2 *>(B);
+        const float *rw = reinterpret_cast<const float *>(B + kRegOffW);
+        const int *rx = reinterpret_cast<const int *>(B + kRegOffX);
+        const int *rd = reinterpret_cast<const int *>(B + kRegOffD);
+        float *tw = reinterpret_cast<float *>(B + kRegOffTW);
+        unsigned *tm = reinterpret_cast<unsigned *>(B + kRegOffM);
+        const int nb = batch_size(b);
+        for (int q = warp; q < nb; q += kSpreadWarps) {
+            float wv = 0.f;
+            if (lane < 24) {
+                int d = rx[q * 4 + la] - orga;
+                if (((rd[q] >> la) & 1) && d >= 0) d -= nosa;
+                int i = lt - d;
+                if (wrapa && i < 0) i += wrapa;
+                if (lt < texta && i >= 0 && i < wa) wv = rw[q * 24 + la * WM + i];
+                tw[q * 24 + lane] = wv;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, wv != 0.f);
+            if (lane == 0) tm[q] = m;
+        }
+        __syncthreads();  // tile weights and masks of batch b ready
+        for (int q0 = 0; q0 < nb; q0 += 32) {
+            bool hit = false;
+            if (q0 + lane < nb) {
+                const unsigned m = tm[q0 + lane];
+                hit = (m & bmx) && (m & bmy) && (m & bmz);
+            }
+            unsigned hm = __ballot_sync(0xffffffffu, hit);
+            while (hm) {
+                const int q = q0 + __ffs(hm) - 1;
+                hm &= hm - 1;
+                const unsigned m = tm[q];
+                const unsigned ym = (m >> (8 + by0)) & 0xFu, zm = (m >> (16 + bz0)) & 0x3u;
+                const float2 v = rv[q * 32 + lane];
+                const float4 wx = *reinterpret_cast<const float4 *>(tw + q * 24 + bx0);
+                const float4 wy = *reinterpret_cast<const float4 *>(tw + q * 24 + 8 + by0);
+                const float2 wz = *reinterpret_cast<const float2 *>(tw + q * 24 + 16 + bz0);
+                const float wxa[4] = {wx.x, wx.y, wx.z, wx.w};
+                const float wya[4] = {wy.x, wy.y, wy.z, wy.w};
+#pragma unroll
+                for (int pz = 0; pz < 2; ++pz) {
+                    if (!((zm >> pz) & 1u)) continue;
+                    const float wzz = pz ? wz.y : wz.x;
+#pragma unroll
+                    for (int py = 0; py < 4; ++py) {
+                        if ((ym >> py) & 1u) {
+                            const float wyz = wzz * wya[py];
+                            const float vx = wyz * v.x, vy = wyz * v.y;
+#pragma unroll
+                            for (int px = 0; px < 4; ++px) {
+                                const int q2 = px + 4 * (py + 4 * pz);
+                                ax[q2] = fmaf(wxa[px], vx, ax[q2]);
+                                ay[q2] = fmaf(wxa[px], vy, ay[q2]);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();  // staging no longer read: reuse it for the output tile
+#pragma unroll
+    for (int q = 0; q < 32; ++q) s_out[(warp * 32 + q) * 33 + lane] = make_float2(ax[q], ay[q]);
+    __syncthreads();
+    const int grp = P.ch.K ? 0 : (it.frame < 0 ? 0 : it.frame);
+    for (int e = threadIdx.x; e < 32 * kRegPts; e += blockDim.x) {
+        const int cl = e / kRegPts, pt = e - cl * kRegPts;
+        const int ch = c0 + cl;
+        if (ch >= nch) break;
+        const int pos = s_pos[pt];
+        if (pos < 0) continue;
+        const int x = pt & 7, y = (pt >> 3) & 7, z = pt >> 6;
+        const int w = (x >> 2) | ((y >> 2) << 1) | ((z >> 1) << 2);
+        const int q = (x & 3) | ((y & 3) << 2) | ((z & 1) << 4);
+        const float2 vv = s_out[(w * 32 + q) * 33 + cl];
+        float2 *G = P.grid + ((int64_t)grp * nch + ch) * P.g.gvol;
+        if (it.atomic) atomicAdd(G + pos, vv);
+        else G[pos] = vv;
     }
 }
 
@@ -772,7 +1108,9 @@ int layout_ws(pfb_plan *p, const Chan &c, WsLayout *L, cufftHandle *h, size_t *w
 
 template <int D, int WM>
 int launch_interp_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
-    interp_il_kernel<D, WM><<<blocks, kTileWarps * 32, 0, s>>>(P);
+    // element offsets point * nch in 32 bits when the grid allows it
+    if (P.g.gvol * (int64_t)P.ch.nch < (1LL << 31)) interp_il_kernel<D, WM, false><<<blocks, kTileWarps * 32, 0, s>>>(P);
+    else interp_il_kernel<D, WM, true><<<blocks, kTileWarps * 32, 0, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
 }
@@ -780,6 +1118,16 @@ int launch_interp_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
 template <int D, int WM>
 int launch_traj_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
     traj_il_kernel<D, WM><<<blocks, kTileWarps * 32, 0, s>>>(P);
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
+template <int WM>
+int launch_spread_reg3_t(const SpreadIL &P, int nitems, int nchunks, cudaStream_t s) {
+    auto k = spread_reg3_kernel<WM>;
+    PFB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRegSmem));
+    dim3 grid(nitems, nchunks);
+    k<<<grid, kSpreadWarps * 32, kRegSmem, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
 }
@@ -930,11 +1278,15 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             if (stage == PFB_STAGE_PAD) {
                 Q.src = static_cast<const float2 *>(src);
                 Q.dst = gridp;
-                pad_pl_kernel<<<flat_blocks(P * p->g.gvol), 256, 0, s>>>(Q);
+                const int64_t units = (int64_t)p->g.nos[1] * p->g.nos[2] * ((p->g.nos[0] + kRowSeg - 1) / kRowSeg);
+                dim3 grid((unsigned)((units + 7) / 8), (unsigned)std::min<int64_t>(P, 65535));
+                pad_pl_kernel<<<grid, 256, 0, s>>>(Q);
             } else {
                 Q.src = gridp;
                 Q.dst = static_cast<float2 *>(dst);
-                crop_pl_kernel<<<flat_blocks((int64_t)c.B * d.ncoeff * p->g.nvol), 256, 0, s>>>(Q);
+                const int64_t units = (int64_t)p->g.n[1] * p->g.n[2] * ((p->g.n[0] + kRowSeg - 1) / kRowSeg);
+                dim3 grid((unsigned)((units + 7) / 8), (unsigned)std::min<int64_t>((int64_t)c.B * d.ncoeff, 65535));
+                crop_pl_kernel<<<grid, 256, 0, s>>>(Q);
             }
             PFB_CHECK_LAUNCH();
             return PFB_OK;
@@ -944,9 +1296,14 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             return run_fft(h, wb, gridp, stage == PFB_STAGE_FFT ? -1 : +1, work, L.work, s);
         case PFB_STAGE_TRANSPOSE: {
             const int tc = std::min(32, pow2ceil(c.nch));
-            const int tp = 1024 / tc;
-            dim3 g3((unsigned)((p->g.gvol + tp - 1) / tp), (unsigned)((c.nch + tc - 1) / tc), (unsigned)c.ngrp);
-            transpose_kernel<<<g3, 256, 0, s>>>(gridp, gridi, p->g.gvol, c.nch, tc);
+            if (tc == 32) {
+                dim3 g3((unsigned)((p->g.gvol + 63) / 64), (unsigned)((c.nch + 31) / 32), (unsigned)c.ngrp);
+                transpose32_kernel<<<g3, 256, 0, s>>>(gridp, gridi, p->g.gvol, c.nch, p->g.gvol % 2 == 0);
+            } else {
+                const int tp = 1024 / tc;
+                dim3 g3((unsigned)((p->g.gvol + tp - 1) / tp), (unsigned)((c.nch + tc - 1) / tc), (unsigned)c.ngrp);
+                transpose_kernel<<<g3, 256, 0, s>>>(gridp, gridi, p->g.gvol, c.nch, tc);
+            }
             PFB_CHECK_LAUNCH();
             return PFB_OK;
         }
@@ -1039,6 +1396,12 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             S.ch = c;
             S.cw = spread_cw(p, c);
             S.per_frame = basis ? 0 : 1;
+            if (p->g.ndim == 3 && p->g.tile[0] <= kRegTile && p->g.tile[1] <= kRegTile &&
+                p->g.tile[2] <= kRegTile && c.nch > 16) {
+                // register-tile form: 32 channels per CTA, no shared atomics
+                const int nchunks = (c.nch + 31) / 32;
+                return w4 ? launch_spread_reg3_t<4>(S, nitems, nchunks, s) : launch_spread_reg3_t<8>(S, nitems, nchunks, s);
+            }
             const size_t smem = spread_smem(p, S.cw);
             const int nchunks = (c.nch + S.cw - 1) / S.cw;
 #define PFB_S4(DD) launch_spread_il_t<DD, 4>(S, nitems, nchunks, smem, s)

@@ -153,7 +153,8 @@ def _pipeline_both(plan, x, y, basis=None, zs=None, zt=None, L=1):
     assert rel(res["fast"][1].cpu(), res["planar"][1].cpu().numpy()) < 1e-5
 
 
-@pytest.mark.parametrize("case", ["2d_coils", "2d_frames", "3d", "basis", "b0", "3d_w6_odd", "2d_single_tile"])
+@pytest.mark.parametrize("case", ["2d_coils", "2d_frames", "3d", "basis", "b0", "3d_w6_odd", "2d_single_tile",
+                                  "2d_single_tile_32ch", "3d_w6_32ch", "1d_32ch"])
 def test_interleaved_pipeline_matches_planar(case):
     rng = np.random.default_rng(21)
     crn = lambda *s: torch.as_tensor((rng.standard_normal(s) + 1j * rng.standard_normal(s)).astype(np.complex64)).cuda()  # noqa: E731
@@ -179,6 +180,23 @@ def test_interleaved_pipeline_matches_planar(case):
                                 np.full((1, 1, 4, 2), -6.0), np.full((1, 1, 4, 2), 5.9)], axis=2).astype(np.float32)
         plan = _plan(coord, N, (2.0, 2.0), (4, 4))
         _pipeline_both(plan, crn(3, 1, *N), crn(3, 68))
+    elif case == "2d_single_tile_32ch":
+        # 32 channels per warp with taps wrapping inside a single tile
+        N = (12, 12)
+        coord = np.concatenate([((rng.random((1, 1, 60, 2)) - 0.5) * 12),
+                                np.full((1, 1, 4, 2), -6.0), np.full((1, 1, 4, 2), 5.9)], axis=2).astype(np.float32)
+        plan = _plan(coord, N, (2.0, 2.0), (4, 4))
+        _pipeline_both(plan, crn(40, 1, *N), crn(40, 68))
+    elif case == "3d_w6_32ch":
+        N = (17, 21, 19)
+        coord = ((rng.random((1, 20, 50, 3)) - 0.5) * np.array([19, 21, 17])).astype(np.float32)
+        plan = _plan(coord, N, (2.0, 1.5, 2.0), (6, 5, 7))
+        _pipeline_both(plan, crn(32, 1, *N), crn(32, 20 * 50))
+    elif case == "1d_32ch":
+        N = (300,)
+        coord = ((rng.random((1, 4, 100, 1)) - 0.5) * 300).astype(np.float32)
+        plan = _plan(coord, N, (1.25,), (4,))
+        _pipeline_both(plan, crn(32, 1, *N), crn(32, 400))
     elif case == "3d_w6_odd":
         N = (17, 21, 19)
         coord = ((rng.random((1, 20, 50, 3)) - 0.5) * np.array([19, 21, 17])).astype(np.float32)

@@ -106,6 +106,20 @@ def test_all_samples_in_one_tile_and_chunking():
     assert gplan.interpolator.max_bin >= 1000  # 4000 samples in one tile, split over <= 4 edge codes
 
 
+def test_crowded_3d_tiles_with_many_channels():
+    """3D, more than 16 channels (register-tile spread): a hot spot of 6000
+    samples split into several work items combined with atomics, items of
+    several staged batches, and tiles at the periodic edge."""
+    rng = np.random.default_rng(15)
+    N = 24
+    hot = ((rng.random((6000, 3)) - 0.5) * 2.0).astype(np.float32)
+    edge = ((rng.random((500, 3)) - 0.5) * N).astype(np.float32)
+    edge[:100] = -N / 2  # first taps wrap across the periodic boundary
+    coord = np.concatenate([hot, edge])[None]
+    check_pair(coord, (N, N, N), crandn(rng, 20, N, N, N), crandn(rng, 20, 1, 6500), width=4, oversamp=1.25)
+    check_pair(coord, (N, N, N), crandn(rng, 33, N, N, N), crandn(rng, 33, 1, 6500), width=6, oversamp=2.0)
+
+
 def test_multiframe_and_weights():
     rng = np.random.default_rng(6)
     N, F = 40, 3
