@@ -231,6 +231,12 @@ int pfb_nufft_traj_grad(pfb_plan *plan, const pfb_apply_t *opt, const void *imag
  *   INTERP: interleaved grid -> per-channel sample results;  OUT: results -> dst k-space
  *   VALS:   src k-space -> per-channel sample values;  SPREAD: values -> grid
  *   CROP:   grid -> dst image (cropped, deapodised, times `factor`)
+ * For 2D and 3D grids whose axes are at most 512 long with factors 2, 3, 5, 7
+ * the transform is the fused pruned FFT: PAD, FFT and TRANSPOSE are then its
+ * three forward passes (image -> z pass -> y pass -> x pass writing the
+ * interleaved grid; 2D: y pass, nothing, x pass) and IFFT / CROP its adjoint
+ * passes (x and y passes / last pass writing the image); the chain of stages
+ * computes the same result either way.
  * Stages of the forward path replace _do_nufft's steps
  * (src/pyfourier/_nufft/_nufft.py:235-246), those of the adjoint _do_nufft_adj's
  * (:271-282). */

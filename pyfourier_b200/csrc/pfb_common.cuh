@@ -87,6 +87,29 @@ struct ApplyDesc {
     int norm;               // 0: none, 1: ortho
 };
 
+// One axis of the fused FFT: a mixed-radix Stockham factorisation of n and
+// the offsets of each stage's twiddles exp(-2 pi i j q / (ns * radix)),
+// j < ns, 1 <= q < radix, in a device table.
+constexpr int kFftMaxStages = 16;
+struct FftAxis {
+    int n = 0, nst = 0;
+    int radix[kFftMaxStages] = {};
+    int ns[kFftMaxStages] = {};
+    int twoff[kFftMaxStages] = {};
+    unsigned magic[kFftMaxStages] = {};  // floor(i / ns) = umulhi(i, magic) for i < 2^16 (ns > 1)
+    const float2 *tw = nullptr;
+};
+
+// Channels of an apply on the oversampled grids: nch channels per group
+// (segment l, batch b, coefficient k with k fastest), ngrp groups (frames, or
+// one group with a basis).
+struct Chan {
+    int nch;       // channels per group
+    int ngrp;      // groups
+    int B, L, K;   // batch, segments, coefficients (K = 0 without basis)
+    int F;
+};
+
 }  // namespace pfb
 
 // Opaque plan handle (declared in pfb200.h).
@@ -125,8 +148,10 @@ struct pfb_plan {
     pfb::OwnerItem *d_own_all = nullptr, *d_zero_all = nullptr;
     int n_own_all = 0, n_zero_all = 0;
     int own_chunk = 0;
-    std::map<int, cufftHandle> fft_plans_il;   // keyed by channels per group
-    std::map<int, size_t> fft_work_il;
+    // fused pruned FFT of the channel-interleaved pipeline (tables made on first use)
+    int fft_fused = -1;          // -1 not decided, 0 not applicable, 1 ready
+    pfb::FftAxis fft_ax[pfb::kMaxDim];
+    float2 *d_fft_tw = nullptr;  // twiddles of all axes and stages
 };
 
 namespace pfb {
@@ -189,6 +214,19 @@ __device__ __forceinline__ float kb_eval_deriv(float u, float beta, float *dval)
     *dval = dda * dadu;
     return val;
 }
+
+// Asynchronous global -> shared copies (cp.async, completed by cp_async_wait_all)
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+// 8-byte copy; valid = false writes zeros (nothing is read)
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // a mod n in [0, n); the common cases (|a| within one period) avoid the 64-bit division
 __host__ __device__ __forceinline__ int pmod(long long a, int n) {
@@ -303,5 +341,15 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
                float factor, bool accumulate, cudaStream_t s);
 int build_owner_items(pfb_plan *p, int chunk);
 void free_owner_items(pfb_plan *p);
+
+// fused pruned FFT (pfb_fft.cu): 1 when it applies to the plan (tables ready)
+int fft_fused_ready(pfb_plan *p);
+void fft_fused_free(pfb_plan *p);
+// forward passes: 0 image -> first intermediate, 1 middle (3D only), 2 -> interleaved grid
+int fft_fused_fwd(pfb_plan *p, int pass, const Chan &c, int C, const float2 *img, const float *const *apod,
+                  const float2 *Cl, float factor, float2 *gridp, float2 *gridi, cudaStream_t s);
+// adjoint passes: 0 planar grid -> intermediate(s), 1 -> image (crop, deapodisation, sum over segments)
+int fft_fused_adj(pfb_plan *p, int pass, const Chan &c, int C, float2 *img, const float *const *apod,
+                  const float2 *Cl, float factor, bool accumulate, float2 *gridp, float2 *gridi, cudaStream_t s);
 
 }  // namespace pfb

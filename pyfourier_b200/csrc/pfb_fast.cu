@@ -40,13 +40,6 @@ constexpr int kTileWarps = 8;        // warps per CTA of the sample kernels
 constexpr int kOutRows = 32;         // samples per CTA in the transposing kernels
 constexpr int kSpreadWarps = 16;     // warps per CTA of the spread
 
-struct Chan {
-    int nch;       // channels per group
-    int ngrp;      // groups
-    int B, L, K;   // batch, segments, coefficients (K = 0 without basis)
-    int F;
-};
-
 Chan make_chan(const pfb_plan *p, const ApplyDesc &d) {
     Chan c;
     c.B = (int)d.batch;
@@ -844,17 +837,7 @@ constexpr size_t kRegSmemOut = (size_t)kRegPts * 33 * sizeof(float2);
 constexpr size_t kRegSmem = kRegPts * sizeof(int) + (kRegSmemOut > 2 * kRegBuf ? kRegSmemOut : 2 * kRegBuf);
 static_assert(kRegBuf % 16 == 0 && kRegOffTW % 16 == 0, "16-byte aligned staging arrays");
 
-__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
-}
-// 8-byte copy; valid = false writes zeros (nothing is read)
-__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 
 template <int WM>
 __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const SpreadIL P) {
@@ -1094,8 +1077,14 @@ int wm_of(const Geom &g) { return std::max(g.w[0], std::max(g.w[1], g.w[2])) <= 
 
 int layout_ws(pfb_plan *p, const Chan &c, WsLayout *L, cufftHandle *h, size_t *wb) {
     const int64_t P = (int64_t)c.ngrp * c.nch;
-    int st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, h, wb);
-    if (st) return st;
+    if (fft_fused_ready(p)) {
+        // the fused transform needs no library plan or work area
+        *h = 0;
+        *wb = 0;
+    } else {
+        int st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, h, wb);
+        if (st) return st;
+    }
     L->gridp = up256((size_t)P * p->g.gvol * sizeof(float2));
     L->gridi = L->gridp;
     L->samp = up256((size_t)p->mtot * c.nch * sizeof(float2));
@@ -1262,6 +1251,28 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
     const bool basis = d.basis != nullptr;
     const bool w4 = wmax_of(p->g) <= 4;
     const int64_t P = (int64_t)c.ngrp * c.nch;
+    const bool fused = fft_fused_ready(p) == 1;
+    const float *apod[3] = {p->d_apod[0], p->d_apod[1], p->d_apod[2]};
+    if (fused) {
+        // PAD, FFT and TRANSPOSE are the three forward passes of the fused
+        // transform; IFFT is its first adjoint pass(es) and CROP the last
+        switch (stage) {
+            case PFB_STAGE_PAD:
+                return fft_fused_fwd(p, 0, c, d.ncoeff, static_cast<const float2 *>(src), apod, d.b0_space, factor,
+                                     gridp, gridi, s);
+            case PFB_STAGE_FFT:
+                return fft_fused_fwd(p, 1, c, d.ncoeff, nullptr, apod, d.b0_space, 1.f, gridp, gridi, s);
+            case PFB_STAGE_TRANSPOSE:
+                return fft_fused_fwd(p, 2, c, d.ncoeff, nullptr, apod, d.b0_space, 1.f, gridp, gridi, s);
+            case PFB_STAGE_IFFT:
+                return fft_fused_adj(p, 0, c, d.ncoeff, nullptr, apod, d.b0_space, 1.f, false, gridp, gridi, s);
+            case PFB_STAGE_CROP:
+                return fft_fused_adj(p, 1, c, d.ncoeff, static_cast<float2 *>(dst), apod, d.b0_space, factor,
+                                     accumulate, gridp, gridi, s);
+            default:
+                break;
+        }
+    }
     switch (stage) {
         case PFB_STAGE_PAD:
         case PFB_STAGE_CROP: {
@@ -1576,9 +1587,7 @@ void free_owner_items(pfb_plan *p) {
     cudaFree(p->d_own_all);
     cudaFree(p->d_zero_all);
     p->d_own_frame = p->d_zero_frame = p->d_own_all = p->d_zero_all = nullptr;
-    std::lock_guard<std::mutex> lk(p->fft_mu);
-    for (auto &kv : p->fft_plans_il) cufftDestroy(kv.second);
-    p->fft_plans_il.clear();
+    fft_fused_free(p);
 }
 
 }  // namespace pfb

@@ -1,0 +1,711 @@
+// Fused, pruned FFT of the channel-interleaved NUFFT pipeline (2D and 3D).
+//
+// The reference's glue around the library FFT (src/pyfourier/_subroutines/_fft.py:72-79
+// via _nufft/_nufft.py:218-287) is pad -> centred FFT -> (interpolate) and
+// (spread) -> centred inverse FFT -> crop, with deapodisation (_apod.py:16-46) and
+// the B0 spatial factors applied on the image side.  Here the multi-dimensional
+// transform is run axis by axis as batched 1D transforms in shared memory, and
+// the passes are pruned and fused with their neighbours:
+//
+//   forward 3D: image --(z pass: deapodise, C_l, zero-pad, FFT)--> T1[plane][kz][y][x]
+//               --(y pass)--> T2[plane][kz][ky][x] --(x pass)--> interleaved grid
+//   adjoint 3D: planar grid --(x pass: IFFT, crop x)--> T1[plane][kz][ky][x]
+//               --(y pass: crop y)--> T2[plane][kz][y][x]
+//               --(z pass: crop z, sum_l conj(C_l), deapodise)--> image
+//
+// (2D drops the z pass.)  Rows and columns that are all zero are never read or
+// written, so a forward transform of an N^3 image onto an n^3 grid moves about
+// N^3 + 2 n N^2 + 2 n^2 N + n^3 elements per plane instead of the 2 n^3 per pass
+// of an unpruned transform, and the pad, crop and channel transpose cost nothing
+// extra.
+//
+// Each 1D transform is a mixed-radix Stockham autosort FFT (radices 8, 5, 4, 3, 7, 2;
+// Govindaraju et al., "High performance discrete Fourier transforms on graphics
+// processors", SC 2008): stage s with radix r and ns = product of the earlier radices
+// reads x_q = src[i + q n / r], multiplies by exp(-2 pi i j q / (ns r)) (j = i mod
+// ns), takes the r-point DFT and writes dst[(i - j) r + j + k ns].  A CTA holds 16
+// vectors (columns of shared memory, one lane each in a half-warp); 16 streams of
+// butterflies run over them.  The inverse transform conjugates on load and store.
+// Twiddles are computed in double precision on the host.
+
+#include <cmath>
+#include <vector>
+
+#include "pfb_common.cuh"
+
+namespace pfb {
+namespace {
+
+constexpr int kCols = 16;                 // vectors per CTA
+constexpr int kPitch = kCols + 2;         // shared row pitch (float2): 16-byte aligned rows
+constexpr int kThreads = 256;
+constexpr int kStreams = kThreads / kCols;        // load / store: 16 lanes per row
+constexpr int kPairStreams = kThreads / (kCols / 2);  // butterflies: a thread takes 2 columns
+constexpr int kMaxN = 512;                // longest axis handled here (else the library FFT)
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// -i * a
+__device__ __forceinline__ float2 cmi(float2 a) { return make_float2(a.y, -a.x); }
+__device__ __forceinline__ float2 caxpy(float s, float2 a, float2 y) {
+    return make_float2(fmaf(s, a.x, y.x), fmaf(s, a.y, y.y));
+}
+
+// forward r-point DFTs, b_k = sum_q a_q exp(-2 pi i q k / r), in place
+template <int R>
+__device__ __forceinline__ void dft(float2 *a);
+
+template <>
+__device__ __forceinline__ void dft<2>(float2 *a) {
+    const float2 t = a[1];
+    a[1] = csub(a[0], t);
+    a[0] = cadd(a[0], t);
+}
+
+template <>
+__device__ __forceinline__ void dft<4>(float2 *a) {
+    const float2 t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
+    const float2 t2 = cadd(a[1], a[3]), t3 = cmi(csub(a[1], a[3]));
+    a[0] = cadd(t0, t2);
+    a[2] = csub(t0, t2);
+    a[1] = cadd(t1, t3);
+    a[3] = csub(t1, t3);
+}
+
+template <>
+__device__ __forceinline__ void dft<8>(float2 *a) {
+    float2 e[4] = {a[0], a[2], a[4], a[6]}, o[4] = {a[1], a[3], a[5], a[7]};
+    dft<4>(e);
+    dft<4>(o);
+    const float h = 0.70710678118654757f;  // sqrt(1/2)
+    // o_k * exp(-2 pi i k / 8)
+    const float2 o1 = make_float2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+    const float2 o2 = cmi(o[2]);
+    const float2 o3 = make_float2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+    a[0] = cadd(e[0], o[0]);
+    a[4] = csub(e[0], o[0]);
+    a[1] = cadd(e[1], o1);
+    a[5] = csub(e[1], o1);
+    a[2] = cadd(e[2], o2);
+    a[6] = csub(e[2], o2);
+    a[3] = cadd(e[3], o3);
+    a[7] = csub(e[3], o3);
+}
+
+template <>
+__device__ __forceinline__ void dft<3>(float2 *a) {
+    const float s = 0.86602540378443871f;  // sin(2 pi / 3)
+    const float2 t = cadd(a[1], a[2]), d = csub(a[1], a[2]);
+    const float2 m = caxpy(-0.5f, t, a[0]);
+    const float2 u = make_float2(s * d.y, -s * d.x);  // -i s d
+    a[0] = cadd(a[0], t);
+    a[1] = cadd(m, u);
+    a[2] = csub(m, u);
+}
+
+template <>
+__device__ __forceinline__ void dft<5>(float2 *a) {
+    // cos and sin of 2 pi / 5 and 4 pi / 5
+    const float c1 = 0.30901699437494745f, c2 = -0.80901699437494734f;
+    const float s1 = 0.95105651629515353f, s2 = 0.58778525229247325f;
+    const float2 t1 = cadd(a[1], a[4]), t2 = cadd(a[2], a[3]);
+    const float2 t3 = csub(a[1], a[4]), t4 = csub(a[2], a[3]);
+    const float2 p1 = caxpy(c2, t2, caxpy(c1, t1, a[0]));
+    const float2 p2 = caxpy(c1, t2, caxpy(c2, t1, a[0]));
+    const float2 q1 = caxpy(s2, t4, make_float2(s1 * t3.x, s1 * t3.y));
+    const float2 q2 = caxpy(-s1, t4, make_float2(s2 * t3.x, s2 * t3.y));
+    a[0] = cadd(a[0], cadd(t1, t2));
+    a[1] = cadd(p1, cmi(q1));
+    a[4] = csub(p1, cmi(q1));
+    a[2] = cadd(p2, cmi(q2));
+    a[3] = csub(p2, cmi(q2));
+}
+
+template <>
+__device__ __forceinline__ void dft<7>(float2 *a) {
+    // cos and sin of 2 pi k / 7
+    const float C[7] = {1.f, 0.62348980185873359f, -0.22252093395631434f, -0.90096886790241903f,
+                        -0.90096886790241915f, -0.22252093395631459f, 0.62348980185873337f};
+    const float S[7] = {0.f, 0.7818314824680298f, 0.97492791218182362f, 0.43388373911755823f,
+                        -0.43388373911755801f, -0.97492791218182362f, -0.78183148246802991f};
+    float2 t[4], d[4];
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        t[k] = cadd(a[k], a[7 - k]);
+        d[k] = csub(a[k], a[7 - k]);
+    }
+    const float2 a0 = a[0];
+    a[0] = cadd(a0, cadd(t[1], cadd(t[2], t[3])));
+#pragma unroll
+    for (int m = 1; m <= 3; ++m) {
+        float2 p = a0, q = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 1; k <= 3; ++k) {
+            p = caxpy(C[(k * m) % 7], t[k], p);
+            q = caxpy(S[(k * m) % 7], d[k], q);
+        }
+        a[m] = cadd(p, cmi(q));
+        a[7 - m] = csub(p, cmi(q));
+    }
+}
+
+template <>
+__device__ __forceinline__ void dft<10>(float2 *a) {
+    float2 e[5] = {a[0], a[2], a[4], a[6], a[8]}, o[5] = {a[1], a[3], a[5], a[7], a[9]};
+    dft<5>(e);
+    dft<5>(o);
+    // exp(-2 pi i k / 10), k = 1..4
+    const float c1 = 0.80901699437494745f, s1 = 0.58778525229247314f;
+    const float c2 = 0.30901699437494745f, s2 = 0.95105651629515353f;
+    const float2 w[5] = {make_float2(1.f, 0.f), make_float2(c1, -s1), make_float2(c2, -s2), make_float2(-c2, -s2),
+                         make_float2(-c1, -s1)};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        const float2 t = k ? cmul(o[k], w[k]) : o[0];
+        a[k] = cadd(e[k], t);
+        a[k + 5] = csub(e[k], t);
+    }
+}
+
+// One Stockham stage over the CTA's 16 columns; a thread takes two adjacent
+// columns (one float4) of each of its butterflies.
+template <int R>
+__device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2 *__restrict__ dst, int m, int ns,
+                                          unsigned magic, const float2 *__restrict__ tw, int stream, int cp) {
+    for (int i = stream; i < m; i += kPairStreams) {
+        const int j = ns == 1 ? 0 : i - (int)__umulhi((unsigned)i, magic) * ns;
+        float2 a[R], b[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const float4 v = *reinterpret_cast<const float4 *>(src + (i + q * m) * kPitch + 2 * cp);
+            a[q] = make_float2(v.x, v.y);
+            b[q] = make_float2(v.z, v.w);
+        }
+        if (j != 0) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                const float2 w = __ldg(tw + j * (R - 1) + (q - 1));
+                a[q] = cmul(a[q], w);
+                b[q] = cmul(b[q], w);
+            }
+        }
+        dft<R>(a);
+        dft<R>(b);
+        const int base = (i - j) * R + j;
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+            *reinterpret_cast<float4 *>(dst + (base + k * ns) * kPitch + 2 * cp) = make_float4(a[k].x, a[k].y, b[k].x, b[k].y);
+    }
+}
+
+// forward FFT of the 16 columns held in A (B is scratch); returns the buffer
+// holding the result.  Ends with the CTA synchronised.
+__device__ __forceinline__ const float2 *fft_run(float2 *A, float2 *B, const FftAxis &fa) {
+    float2 *src = A, *dst = B;
+    const int cp = threadIdx.x & (kCols / 2 - 1), stream = threadIdx.x / (kCols / 2);
+    for (int s = 0; s < fa.nst; ++s) {
+        const int r = fa.radix[s], ns = fa.ns[s], m = fa.n / r;
+        const unsigned mg = fa.magic[s];
+        const float2 *tw = fa.tw + fa.twoff[s];
+        switch (r) {
+            case 2: fft_stage<2>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 3: fft_stage<3>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 4: fft_stage<4>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 5: fft_stage<5>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 7: fft_stage<7>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 10: fft_stage<10>(src, dst, m, ns, mg, tw, stream, cp); break;
+            default: fft_stage<8>(src, dst, m, ns, mg, tw, stream, cp); break;
+        }
+        __syncthreads();
+        float2 *t = src;
+        src = dst;
+        dst = t;
+    }
+    return src;
+}
+
+// Transform along an outer axis (y or z) of 16 adjacent x positions.
+//   mode 0: buffer -> buffer; 1: image -> buffer (forward first pass: deapodisation,
+//   C_l, factor); 2: buffer -> image (adjoint last pass: sum over segments of
+//   conj(C_l) times the transform, deapodisation, factor, optional accumulate).
+// Forward passes read lin = N elements placed at FFT positions (i - N/2) mod n
+// and write all n; inverse passes read all n and write lout = N, element o from
+// FFT position (o - N/2) mod n.  Strides are in elements; for the image side they
+// are the image strides.
+struct ColPass {
+    FftAxis fa;
+    int inv, mode;
+    int lin, lout, nax;
+    int X, nmid, nplanes;
+    int64_t in_plane, in_mid, in_ax;
+    int64_t out_plane, out_mid, out_ax;
+    const float2 *src;
+    float2 *dst;
+    Chan ch;
+    int C;
+    int64_t nvol;
+    const float *apod_ax, *apod_mid, *apod_x;
+    const float2 *Cl;
+    float factor;
+    int accumulate;
+};
+
+__global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
+    extern __shared__ float2 fsm[];
+    const int n = P.fa.n;
+    float2 *A = fsm, *Bf = fsm + n * kPitch, *Acc = fsm + 2 * n * kPitch;
+    const int nxc = (P.X + kCols - 1) / kCols;
+    int blk = blockIdx.x;
+    const int xc = blk % nxc;
+    blk /= nxc;
+    const int mid = blk % P.nmid;
+    const int plane = blk / P.nmid;
+    const int col = threadIdx.x & (kCols - 1), stream = threadIdx.x >> 4;
+    const int x = xc * kCols + col;
+    const bool xin = x < P.X;
+    const int xs = xin ? x : P.X - 1;  // in-bounds address for columns past the edge
+    const int hn = P.nax / 2;
+    const int Kc = P.ch.K ? P.ch.K : 1;
+    const int nl = P.mode == 2 ? P.ch.L : 1;
+    for (int l = 0; l < nl; ++l) {
+        int64_t in_base;
+        const float2 *cl = nullptr;
+        if (P.mode == 1) {  // grid plane (grp, ch) <- image plane (b, c), segment ll
+            const int grp = plane / P.ch.nch, chn = plane - grp * P.ch.nch;
+            const int k = chn % Kc, lb = chn / Kc, b = lb % P.ch.B, ll = lb / P.ch.B;
+            const int c = P.ch.K ? k : grp;
+            in_base = ((int64_t)b * P.C + c) * P.nvol + mid * P.in_mid;
+            if (P.Cl) cl = P.Cl + (int64_t)ll * P.nvol + mid * P.in_mid;
+        } else if (P.mode == 2) {  // image plane (b, c) <- grid plane of segment l
+            const int b = plane / P.C, c = plane - b * P.C;
+            const int grp = P.ch.K ? 0 : c;
+            const int chn = P.ch.K ? (l * P.ch.B + b) * Kc + c : l * P.ch.B + b;
+            in_base = ((int64_t)grp * P.ch.nch + chn) * P.in_plane + mid * P.in_mid;
+        } else {
+            in_base = (int64_t)plane * P.in_plane + mid * P.in_mid;
+        }
+        // all copies of the column in flight at once (C_l into the scratch buffer);
+        // positions without input are zero-filled
+        for (int p = stream; p < n; p += kStreams) {
+            int i = p;
+            if (!P.inv) {
+                i = p + hn;
+                if (i >= n) i -= n;
+            }
+            const bool valid = i < P.lin;
+            const int64_t off = (int64_t)(valid ? i : 0) * P.in_ax + xs;
+            cp_async8(A + p * kPitch + col, P.src + in_base + off, valid);
+            if (cl) cp_async8(Bf + p * kPitch + col, cl + off, valid);
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        if (P.mode == 1 || P.inv) {
+            // each thread finishes the elements it copied
+            float amid = P.factor;
+            if (P.mode == 1 && P.apod_mid) amid *= P.apod_mid[mid];
+            if (P.mode == 1 && P.apod_x) amid *= P.apod_x[xs];
+            for (int p = stream; p < n; p += kStreams) {
+                int i = p;
+                if (!P.inv) {
+                    i = p + hn;
+                    if (i >= n) i -= n;
+                }
+                if (i >= P.lin) continue;
+                float2 v = A[p * kPitch + col];
+                if (P.mode == 1) {
+                    if (cl) v = cmul(v, Bf[p * kPitch + col]);
+                    const float a = P.apod_ax ? amid * P.apod_ax[i] : amid;
+                    v = make_float2(v.x * a, v.y * a);
+                }
+                if (P.inv) v.y = -v.y;
+                A[p * kPitch + col] = v;
+            }
+        }
+        __syncthreads();
+        const float2 *R = fft_run(A, Bf, P.fa);
+        if (P.mode == 2) {
+            float amid = P.factor;
+            if (P.apod_mid) amid *= P.apod_mid[mid];
+            if (P.apod_x) amid *= P.apod_x[xs];
+            const int64_t out_base = (int64_t)plane * P.nvol + mid * P.out_mid;
+            for (int o = stream; o < P.lout; o += kStreams) {
+                int pp = o - hn;
+                if (pp < 0) pp += n;
+                float2 v = R[pp * kPitch + col];
+                v.y = -v.y;
+                if (P.Cl) v = cmulc(v, P.Cl[(int64_t)l * P.nvol + (int64_t)o * P.out_ax + mid * P.out_mid + xs]);
+                if (l > 0) v = cadd(v, Acc[o * kPitch + col]);
+                if (l + 1 < nl) {
+                    Acc[o * kPitch + col] = v;
+                } else if (xin) {
+                    // last segment: deapodise, scale and write the image
+                    const float a = P.apod_ax ? amid * P.apod_ax[o] : amid;
+                    v = make_float2(v.x * a, v.y * a);
+                    float2 *d = P.dst + out_base + (int64_t)o * P.out_ax + x;
+                    if (P.accumulate) v = cadd(v, *d);
+                    *d = v;
+                }
+            }
+            if (l + 1 < nl) __syncthreads();  // the next segment reloads A
+        } else {
+            const int64_t out_base = (int64_t)plane * P.out_plane + mid * P.out_mid;
+            for (int o = stream; o < P.lout; o += kStreams) {
+                int pp = o;
+                if (P.inv) {
+                    pp = o - hn;
+                    if (pp < 0) pp += n;
+                }
+                float2 v = R[pp * kPitch + col];
+                if (P.inv) v.y = -v.y;
+                if (xin) P.dst[out_base + (int64_t)o * P.out_ax + x] = v;
+            }
+        }
+    }
+}
+
+// Transform along x.  Forward: rows of T (N0 long, [plane][kz][ky][x]) -> the
+// interleaved grid [grp][point][ch]; the 16 vectors of a CTA are consecutive
+// (grp, kz, ky, ch) with ch fastest, so a half-warp stores 16 channels of one
+// point.  Inverse: rows of the planar grid ([plane][kz][ky][kx], n0 long) -> rows
+// of T cropped to N0.
+struct RowPass {
+    FftAxis fa;
+    int N0;
+    int64_t nvec;
+    int nch, nos1, nos2;
+    int64_t gvol;
+    const float2 *src;
+    float2 *dst;
+};
+
+__global__ void __launch_bounds__(kThreads) row_fwd_kernel(const RowPass P) {
+    extern __shared__ float2 fsm[];
+    const int n = P.fa.n;
+    float2 *A = fsm, *Bf = fsm + n * kPitch;
+    const int64_t u0 = (int64_t)blockIdx.x * kCols;
+    const int hn = P.N0 / 2;
+    {
+        const int v = threadIdx.x >> 4, lx = threadIdx.x & 15;
+        const int64_t u = u0 + v;
+        const bool ok = u < P.nvec;
+        int64_t src_off = 0;
+        if (ok) {
+            const int chn = (int)(u % P.nch);
+            int64_t r = u / P.nch;
+            const int ky = (int)(r % P.nos1);
+            r /= P.nos1;
+            const int kz = (int)(r % P.nos2);
+            const int64_t grp = r / P.nos2;
+            src_off = (((grp * P.nch + chn) * P.nos2 + kz) * P.nos1 + ky) * P.N0;
+        }
+        for (int p = lx; p < n; p += 16) {
+            int x = p + hn;
+            if (x >= n) x -= n;
+            const bool valid = ok && x < P.N0;
+            cp_async8(A + p * kPitch + v, P.src + src_off + (valid ? x : 0), valid);
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+    }
+    __syncthreads();
+    const float2 *R = fft_run(A, Bf, P.fa);
+    {
+        const int v = threadIdx.x & 15;
+        const int64_t u = u0 + v;
+        if (u < P.nvec) {
+            const int chn = (int)(u % P.nch);
+            int64_t r = u / P.nch;
+            const int ky = (int)(r % P.nos1);
+            r /= P.nos1;
+            const int kz = (int)(r % P.nos2);
+            const int64_t grp = r / P.nos2;
+            const int64_t base = (grp * P.gvol + ((int64_t)kz * P.nos1 + ky) * n) * P.nch + chn;
+            for (int kx = threadIdx.x >> 4; kx < n; kx += kStreams) P.dst[base + (int64_t)kx * P.nch] = R[kx * kPitch + v];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) row_inv_kernel(const RowPass P) {
+    extern __shared__ float2 fsm[];
+    const int n = P.fa.n;
+    float2 *A = fsm, *Bf = fsm + n * kPitch;
+    const int64_t u0 = (int64_t)blockIdx.x * kCols;
+    const int hn = P.N0 / 2;
+    const int v = threadIdx.x >> 4, lx = threadIdx.x & 15;
+    const int64_t u = u0 + v;
+    const bool ok = u < P.nvec;
+    const int64_t ub = ok ? u : 0;
+    for (int p = lx; p < n; p += 16) cp_async8(A + p * kPitch + v, P.src + ub * n + p, ok);
+    cp_async_commit();
+    cp_async_wait_all();
+    for (int p = lx; p < n; p += 16) A[p * kPitch + v].y = -A[p * kPitch + v].y;  // conjugate (inverse)
+    __syncthreads();
+    const float2 *R = fft_run(A, Bf, P.fa);
+    if (ok) {
+        for (int x = lx; x < P.N0; x += 16) {
+            int pp = x - hn;
+            if (pp < 0) pp += n;
+            float2 val = R[pp * kPitch + v];
+            val.y = -val.y;
+            P.dst[u * P.N0 + x] = val;
+        }
+    }
+}
+
+constexpr double kPi = 3.14159265358979323846;
+
+// radices in the order the stages use them
+bool make_axis(int n, FftAxis *fa, std::vector<float2> &tw) {
+    if (n < 1 || n > kMaxN) return false;
+    *fa = FftAxis{};
+    fa->n = n;
+    int m = n, ns = 1;
+    const int order[7] = {8, 10, 5, 4, 3, 7, 2};
+    for (int r : order) {
+        while (m % r == 0) {
+            if (fa->nst >= kFftMaxStages) return false;
+            const int s = fa->nst++;
+            fa->radix[s] = r;
+            fa->ns[s] = ns;
+            fa->twoff[s] = (int)tw.size();
+            fa->magic[s] = ns > 1 ? (unsigned)(0xFFFFFFFFull / (unsigned long long)ns + 1ull) : 0u;
+            for (int j = 0; j < ns; ++j)
+                for (int q = 1; q < r; ++q) {
+                    const double ang = -2.0 * kPi * (double)j * (double)q / ((double)ns * (double)r);
+                    tw.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
+                }
+            ns *= r;
+            m /= r;
+        }
+    }
+    return m == 1;
+}
+
+// the accumulator over segments only when there are several
+size_t col_smem(int n, int mode, int nseg) {
+    return (size_t)(mode == 2 && nseg > 1 ? 3 : 2) * n * kPitch * sizeof(float2);
+}
+size_t row_smem(int n) { return (size_t)2 * n * kPitch * sizeof(float2); }
+
+int launch_col(const ColPass &P, cudaStream_t s) {
+    const int64_t blocks = (int64_t)P.nplanes * P.nmid * ((P.X + kCols - 1) / kCols);
+    if (blocks == 0) return PFB_OK;
+    if (blocks >= (1LL << 31)) return fail(PFB_ERR_UNSUPPORTED, "too many vectors for the fused FFT");
+    const size_t smem = col_smem(P.fa.n, P.mode, P.ch.L);
+    PFB_CUDA_TRY(cudaFuncSetAttribute(col_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    col_pass_kernel<<<(unsigned)blocks, kThreads, smem, s>>>(P);
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
+int launch_row(const RowPass &P, bool inv, cudaStream_t s) {
+    const int64_t blocks = (P.nvec + kCols - 1) / kCols;
+    if (blocks == 0) return PFB_OK;
+    if (blocks >= (1LL << 31)) return fail(PFB_ERR_UNSUPPORTED, "too many vectors for the fused FFT");
+    const size_t smem = row_smem(P.fa.n);
+    auto k = inv ? row_inv_kernel : row_fwd_kernel;
+    PFB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<(unsigned)blocks, kThreads, smem, s>>>(P);
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
+}  // namespace
+
+int fft_fused_ready(pfb_plan *p) {
+    std::lock_guard<std::mutex> lk(p->fft_mu);
+    if (p->fft_fused >= 0) return p->fft_fused;
+    p->fft_fused = 0;
+    const int D = p->g.ndim;
+    if (D < 2) return 0;
+    std::vector<float2> tw;
+    for (int a = 0; a < D; ++a)
+        if (!make_axis(p->g.nos[a], &p->fft_ax[a], tw)) return 0;
+    if (tw.empty()) tw.push_back(make_float2(1.f, 0.f));
+    if (cudaMalloc(&p->d_fft_tw, tw.size() * sizeof(float2)) != cudaSuccess) {
+        p->d_fft_tw = nullptr;
+        return 0;
+    }
+    if (cudaMemcpy(p->d_fft_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(p->d_fft_tw);
+        p->d_fft_tw = nullptr;
+        return 0;
+    }
+    for (int a = 0; a < D; ++a) p->fft_ax[a].tw = p->d_fft_tw;
+    p->fft_fused = 1;
+    return 1;
+}
+
+void fft_fused_free(pfb_plan *p) {
+    std::lock_guard<std::mutex> lk(p->fft_mu);
+    cudaFree(p->d_fft_tw);
+    p->d_fft_tw = nullptr;
+    p->fft_fused = -1;
+}
+
+int fft_fused_fwd(pfb_plan *p, int pass, const Chan &c, int C, const float2 *img, const float *const *apod,
+                  const float2 *Cl, float factor, float2 *gridp, float2 *gridi, cudaStream_t s) {
+    const Geom &g = p->g;
+    const int D = g.ndim;
+    const int P = c.ngrp * c.nch;
+    const int64_t N0 = g.n[0], N1 = g.n[1], n1 = g.nos[1], n2 = g.nos[2];
+    if (pass == 0) {  // image -> first intermediate: z pass (3D) into gridi, or y pass (2D) into gridp
+        ColPass Q{};
+        Q.inv = 0;
+        Q.mode = 1;
+        Q.X = (int)N0;
+        Q.nplanes = P;
+        Q.src = img;
+        Q.ch = c;
+        Q.C = C;
+        Q.nvol = g.nvol;
+        Q.Cl = Cl;
+        Q.factor = factor;
+        Q.apod_x = apod[0];
+        if (D == 3) {
+            Q.fa = p->fft_ax[2];
+            Q.lin = Q.nax = g.n[2];
+            Q.lout = (int)n2;
+            Q.nmid = (int)N1;
+            Q.in_mid = N0;
+            Q.in_ax = N1 * N0;
+            Q.out_plane = n2 * N1 * N0;
+            Q.out_mid = N0;
+            Q.out_ax = N1 * N0;
+            Q.apod_ax = apod[2];
+            Q.apod_mid = apod[1];
+            Q.dst = gridi;
+        } else {
+            Q.fa = p->fft_ax[1];
+            Q.lin = Q.nax = (int)N1;
+            Q.lout = (int)n1;
+            Q.nmid = 1;
+            Q.in_mid = 0;
+            Q.in_ax = N0;
+            Q.out_plane = n1 * N0;
+            Q.out_mid = 0;
+            Q.out_ax = N0;
+            Q.apod_ax = apod[1];
+            Q.apod_mid = nullptr;
+            Q.dst = gridp;
+        }
+        return launch_col(Q, s);
+    }
+    if (pass == 1) {  // 3D: y pass, gridi -> gridp
+        if (D != 3) return PFB_OK;
+        ColPass Q{};
+        Q.fa = p->fft_ax[1];
+        Q.inv = 0;
+        Q.mode = 0;
+        Q.lin = Q.nax = (int)N1;
+        Q.lout = (int)n1;
+        Q.X = (int)N0;
+        Q.nmid = (int)n2;
+        Q.nplanes = P;
+        Q.in_plane = n2 * N1 * N0;
+        Q.in_mid = N1 * N0;
+        Q.in_ax = N0;
+        Q.out_plane = n2 * n1 * N0;
+        Q.out_mid = n1 * N0;
+        Q.out_ax = N0;
+        Q.src = gridi;
+        Q.dst = gridp;
+        return launch_col(Q, s);
+    }
+    // x pass: gridp rows -> interleaved grid
+    RowPass R{};
+    R.fa = p->fft_ax[0];
+    R.N0 = (int)N0;
+    R.nch = c.nch;
+    R.nos1 = (int)n1;
+    R.nos2 = D == 3 ? (int)n2 : 1;
+    R.nvec = (int64_t)c.ngrp * R.nos2 * R.nos1 * c.nch;
+    R.gvol = g.gvol;
+    R.src = gridp;
+    R.dst = gridi;
+    return launch_row(R, false, s);
+}
+
+int fft_fused_adj(pfb_plan *p, int pass, const Chan &c, int C, float2 *img, const float *const *apod,
+                  const float2 *Cl, float factor, bool accumulate, float2 *gridp, float2 *gridi, cudaStream_t s) {
+    const Geom &g = p->g;
+    const int D = g.ndim;
+    const int P = c.ngrp * c.nch;
+    const int64_t N0 = g.n[0], N1 = g.n[1], n1 = g.nos[1], n2 = g.nos[2];
+    if (pass == 0) {
+        // x pass: planar grid rows -> gridi, cropped to N0
+        RowPass R{};
+        R.fa = p->fft_ax[0];
+        R.N0 = (int)N0;
+        R.nos1 = (int)n1;
+        R.nos2 = D == 3 ? (int)n2 : 1;
+        R.nvec = (int64_t)P * R.nos2 * R.nos1;
+        R.src = gridp;
+        R.dst = gridi;
+        int st = launch_row(R, true, s);
+        if (st || D != 3) return st;
+        // 3D: y pass, gridi -> gridp, cropped to N1
+        ColPass Q{};
+        Q.fa = p->fft_ax[1];
+        Q.inv = 1;
+        Q.mode = 0;
+        Q.lin = (int)n1;
+        Q.lout = Q.nax = (int)N1;
+        Q.X = (int)N0;
+        Q.nmid = (int)n2;
+        Q.nplanes = P;
+        Q.in_plane = n2 * n1 * N0;
+        Q.in_mid = n1 * N0;
+        Q.in_ax = N0;
+        Q.out_plane = n2 * N1 * N0;
+        Q.out_mid = N1 * N0;
+        Q.out_ax = N0;
+        Q.src = gridi;
+        Q.dst = gridp;
+        return launch_col(Q, s);
+    }
+    // last pass -> image: z pass (3D, from gridp) or y pass (2D, from gridi)
+    ColPass Q{};
+    Q.inv = 1;
+    Q.mode = 2;
+    Q.X = (int)N0;
+    Q.nplanes = c.B * C;
+    Q.ch = c;
+    Q.C = C;
+    Q.nvol = g.nvol;
+    Q.Cl = Cl;
+    Q.factor = factor;
+    Q.accumulate = accumulate ? 1 : 0;
+    Q.apod_x = apod[0];
+    Q.dst = img;
+    if (D == 3) {
+        Q.fa = p->fft_ax[2];
+        Q.lin = (int)n2;
+        Q.lout = Q.nax = g.n[2];
+        Q.nmid = (int)N1;
+        Q.in_plane = n2 * N1 * N0;
+        Q.in_mid = N0;
+        Q.in_ax = N1 * N0;
+        Q.out_mid = N0;
+        Q.out_ax = N1 * N0;
+        Q.apod_ax = apod[2];
+        Q.apod_mid = apod[1];
+        Q.src = gridp;
+    } else {
+        Q.fa = p->fft_ax[1];
+        Q.lin = (int)n1;
+        Q.lout = Q.nax = (int)N1;
+        Q.nmid = 1;
+        Q.in_plane = n1 * N0;
+        Q.in_mid = 0;
+        Q.in_ax = N0;
+        Q.out_mid = 0;
+        Q.out_ax = N0;
+        Q.apod_ax = apod[1];
+        Q.apod_mid = nullptr;
+        Q.src = gridi;
+    }
+    return launch_col(Q, s);
+}
+
+}  // namespace pfb
