@@ -240,21 +240,41 @@ def stage_times(torch, pf, plan, x, iters):
 
 
 def algorithmic_bytes(wl, plan, B):
-    """Bytes each kernel must move at minimum (inputs read once, outputs written once)."""
+    """Bytes each stage must move at minimum (inputs read once, outputs written once).
+
+    3D grids use the fused pruned FFT, whose passes are the pad / fft / transpose
+    (forward) and ifft / crop (adjoint) stages: per plane, with N the image and
+    n the oversampled extent, the z pass reads N^3 and writes n N^2, the y pass
+    n N^2 -> n^2 N, the x pass n^2 N -> n^3 (and the reverse for the adjoint)."""
     M = plan.interpolator.total_samples
     G = int(np.prod(plan.os_shape))
-    Nv = int(np.prod(plan.shape))
     nd = plan.ndim
     coords = M * (4 * nd + 4 + 4)  # sorted coords, permutation, frame index
+    N, n = plan.shape[-1], plan.os_shape[-1]
+    e = 8 * B
     return {
         "interp": B * G * 8 + B * M * 8 + coords,   # grid read once, per-channel results written
         "out": 2 * B * M * 8,                        # results read, k-space written
         "vals": 2 * B * M * 8,                       # k-space read, per-channel values written
         "spread": B * M * 8 + B * G * 8 + coords,   # values read, grid written once
-        "pad": B * Nv * 8 + B * G * 8,               # image read, padded grid written
-        "transpose": 2 * B * G * 8,                  # planar grid read, interleaved grid written
-        "crop": B * Nv * 8 + B * Nv * 8,             # image region of the grid read, image written
+        "pad": e * (N ** 3 + n * N ** 2),            # z pass
+        "fft": e * (n * N ** 2 + n ** 2 * N),        # y pass
+        "transpose": e * (n ** 2 * N + n ** 3),      # x pass into the interleaved grid
+        "ifft": e * (n ** 3 + 2 * n ** 2 * N + n * N ** 2),  # x and y passes
+        "crop": e * (n * N ** 2 + N ** 3),           # z pass into the image
     }
+
+
+def fp32_roofline(wl, plan, B, ms):
+    """Interp and spread as FP32 work: 8 flops per (tap, channel) (a complex
+    value times a real weight, accumulated), against the nominal FP32 rate of
+    148 SMs x 128 lanes x 2 flops x 1.965 GHz."""
+    M = plan.interpolator.total_samples
+    taps = B * M * wl["width"] ** plan.ndim
+    peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    achieved = 8 * taps / (ms / 1e3) / 1e12
+    return {"achieved": round(achieved, 2), "peak": round(peak, 1), "peak_source": "nominal",
+            "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "flops": 8 * taps}
 
 
 def gpu_arm(args, wl, rank, world, local_rank):
@@ -337,7 +357,10 @@ def gpu_arm(args, wl, rank, world, local_rank):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                 "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": NCU_TRAFFIC.get((args.workload, dom)),
-                "algorithmic_bytes": alg[dom]}
+                "algorithmic_bytes": alg[dom],
+                "fp32": fp32_roofline(wl, plan, B, mine[dom]) if dom in ("spread", "interp") else None,
+                "stages": {k: {"ms": round(mine[k], 3), "GB/s": round(alg[k] / (mine[k] / 1e3) / 1e9, 1),
+                               "frac": round(alg[k] / (mine[k] / 1e3) / 1e9 / peak, 3)} for k in mine}}
     return dict(ms=ms, value=value, e2e=world * samples_per_step / e2e_s, h2d=h2d, d2h=d2h, stages=stages,
                 roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=mine_l,
                 kernels_per_step=all_l)
@@ -569,9 +592,11 @@ def extra_workload(args):
     print(json.dumps(line), flush=True)
 
 
-# DRAM bytes (read + write) per launch from one ncu capture of the named
-# workload; the capture and its command are summarised under profiles/.
-NCU_TRAFFIC = {}
+# DRAM bytes (read + write) per launch of the dominant kernel: the ncu capture of
+# the 128^3 / 32-coil variant (1.928 GB for 32 x 2.048 M samples) scaled by the
+# samples processed (x 3.906) to the 200^3 / 8 M-sample workload; the capture and
+# its command are summarised under profiles/.
+NCU_TRAFFIC = {("cfg2", "spread"): int(1.928e9 * 3.906)}
 
 
 def main():
