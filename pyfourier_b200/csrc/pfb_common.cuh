@@ -124,6 +124,7 @@ struct pfb_plan {
     int64_t *d_frame_off = nullptr;   // device copy
     float *d_cos[pfb::kMaxDim] = {nullptr, nullptr, nullptr};  // bin-sorted oversampled coords
     int *d_perm = nullptr;       // sorted position -> global sample index
+    int *d_iperm = nullptr;      // global sample index -> sorted position
     int *d_sframe = nullptr;     // sorted position -> frame
     int *d_bin_start = nullptr;  // (nbins_total * ncode * F + 1) offsets into the sorted order
     int nbins_total = 0;

@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(256) transpose32_kernel(const float2 *__restri
 // sample-side transposes
 // ------------------------------------------------------------------------------------
 struct SampIL {
-    const int *perm, *sframe;
+    const int *iperm, *sframe;
     const int64_t *frame_off;
     int64_t mtot;
     int readout;
@@ -249,75 +249,76 @@ struct SampIL {
     int accumulate;
 };
 
-// vals[j][ch] = y[b][perm[j]] * w[g] * conj(B_l(t)) * conj(basis[f, k])
+// Both transposes walk the samples in their original order, kOutRows per CTA,
+// so the k-space side is read / written coalesced and the sorted side moves
+// whole rows of nch channels (iperm: original -> sorted position).
+
+// vals[iperm[g]][ch] = y[b][g] * w[g] * conj(B_l(t)) * conj(basis[f, k])
 __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
     extern __shared__ float2 sm[];  // [32][B]
-    const int64_t j0 = (int64_t)blockIdx.x * kOutRows;
+    const int64_t g0 = (int64_t)blockIdx.x * kOutRows;
     const int B = P.ch.B;
     for (int e = threadIdx.x; e < kOutRows * B; e += blockDim.x) {
-        int b = e / kOutRows, jj = e - b * kOutRows;
-        int64_t j = j0 + jj;
+        const int b = e / kOutRows, gg = e - b * kOutRows;
+        const int64_t g = g0 + gg;
         float2 v = make_float2(0.f, 0.f);
-        if (j < P.mtot) {
-            int g = P.perm[j];
+        if (g < P.mtot) {
             v = P.src[(int64_t)b * P.mtot + g];
             if (P.weight) {
-                float w = P.weight[g];
+                const float w = P.weight[g];
                 v.x *= w;
                 v.y *= w;
             }
         }
-        sm[jj * B + b] = v;
+        sm[gg * B + b] = v;
     }
     __syncthreads();
     const int nch = P.ch.nch, Kc = P.ch.K ? P.ch.K : 1;
     for (int e = threadIdx.x; e < kOutRows * nch; e += blockDim.x) {
-        int jj = e / nch, c = e - jj * nch;
-        int64_t j = j0 + jj;
-        if (j >= P.mtot) continue;
-        int k = c % Kc, lb = c / Kc, b = lb % B, l = lb / B;
-        float2 v = sm[jj * B + b];
-        if (P.factors) {
-            if (P.tB || P.ch.K) {
-                int g = P.perm[j], f = P.sframe[j];
-                if (P.tB) {
-                    int t = (int)((g - P.frame_off[f]) % P.readout);
-                    v = cmulc(v, P.tB[(int64_t)l * P.readout + t]);
-                }
-                if (P.ch.K) v = cmulc(v, P.basis[(int64_t)f * P.ch.K + k]);
+        const int gg = e / nch, c = e - gg * nch;
+        const int64_t g = g0 + gg;
+        if (g >= P.mtot) continue;
+        const int64_t j = P.iperm[g];
+        const int k = c % Kc, lb = c / Kc, b = lb % B, l = lb / B;
+        float2 v = sm[gg * B + b];
+        if (P.factors && (P.tB || P.ch.K)) {
+            const int f = P.sframe[j];
+            if (P.tB) {
+                const int t = (int)((g - P.frame_off[f]) % P.readout);
+                v = cmulc(v, P.tB[(int64_t)l * P.readout + t]);
             }
+            if (P.ch.K) v = cmulc(v, P.basis[(int64_t)f * P.ch.K + k]);
         }
         P.dst[j * nch + c] = v;
     }
 }
 
-// y[b][perm[j]] (+)= w[g] * sum_{l,k} B_l(t) basis[f, k] res[j][(l, b, k)]
+// y[b][g] (+)= w[g] * sum_{l,k} B_l(t) basis[f, k] res[iperm[g]][(l, b, k)]
 __global__ void __launch_bounds__(256) out_il_kernel(const SampIL P) {
     extern __shared__ float2 sm[];  // [32][nch]
-    const int64_t j0 = (int64_t)blockIdx.x * kOutRows;
+    const int64_t g0 = (int64_t)blockIdx.x * kOutRows;
     const int nch = P.ch.nch;
     for (int e = threadIdx.x; e < kOutRows * nch; e += blockDim.x) {
-        int jj = e / nch, c = e - jj * nch;
-        int64_t j = j0 + jj;
-        sm[e] = j < P.mtot ? P.src[j * nch + c] : make_float2(0.f, 0.f);
+        const int gg = e / nch, c = e - gg * nch;
+        const int64_t g = g0 + gg;
+        sm[e] = g < P.mtot ? P.src[(int64_t)P.iperm[g] * nch + c] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     const int B = P.ch.B, L = P.ch.L, Kc = P.ch.K ? P.ch.K : 1;
     for (int e = threadIdx.x; e < kOutRows * B; e += blockDim.x) {
-        int b = e / kOutRows, jj = e - b * kOutRows;
-        int64_t j = j0 + jj;
-        if (j >= P.mtot) continue;
-        int g = P.perm[j];
+        const int b = e / kOutRows, gg = e - b * kOutRows;
+        const int64_t g = g0 + gg;
+        if (g >= P.mtot) continue;
         float2 acc = make_float2(0.f, 0.f);
         if (L == 1 && !P.ch.K) {
-            acc = sm[jj * nch + b];
+            acc = sm[gg * nch + b];
         } else {
-            int f = P.sframe[j];
-            int t = P.tB ? (int)((g - P.frame_off[f]) % P.readout) : 0;
+            const int f = P.sframe[P.iperm[g]];
+            const int t = P.tB ? (int)((g - P.frame_off[f]) % P.readout) : 0;
             for (int l = 0; l < L; ++l) {
                 float2 accl = make_float2(0.f, 0.f);
                 for (int k = 0; k < Kc; ++k) {
-                    float2 v = sm[jj * nch + (l * B + b) * Kc + k];
+                    float2 v = sm[gg * nch + (l * B + b) * Kc + k];
                     if (P.ch.K) v = cmul(v, P.basis[(int64_t)f * P.ch.K + k]);
                     accl.x += v.x;
                     accl.y += v.y;
@@ -328,13 +329,13 @@ __global__ void __launch_bounds__(256) out_il_kernel(const SampIL P) {
             }
         }
         if (P.weight) {
-            float w = P.weight[g];
+            const float w = P.weight[g];
             acc.x *= w;
             acc.y *= w;
         }
         float2 *dst = P.dst + (int64_t)b * P.mtot + g;
         if (P.accumulate) {
-            float2 o = *dst;
+            const float2 o = *dst;
             acc.x += o.x;
             acc.y += o.y;
         }
@@ -1335,7 +1336,7 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
         case PFB_STAGE_VALS: {
             if (p->mtot == 0) return PFB_OK;
             SampIL O{};
-            O.perm = p->d_perm;
+            O.iperm = p->d_iperm;
             O.sframe = p->d_sframe;
             O.frame_off = p->d_frame_off;
             O.mtot = p->mtot;
@@ -1466,7 +1467,7 @@ int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const flo
     cb.K = 0;
     cb.nch = c.B;
     SampIL V{};
-    V.perm = p->d_perm;
+    V.iperm = p->d_iperm;
     V.sframe = p->d_sframe;
     V.frame_off = p->d_frame_off;
     V.mtot = p->mtot;

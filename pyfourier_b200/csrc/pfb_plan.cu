@@ -72,10 +72,11 @@ __global__ void scale_and_key_kernel(ScaleParams P, const float *__restrict__ co
 __global__ void gather_sorted_kernel(int ndim, int64_t mtot, int nframes, const float *__restrict__ cos_in,
                                      const int *__restrict__ perm, const int *__restrict__ keys_sorted,
                                      float *__restrict__ c0, float *__restrict__ c1, float *__restrict__ c2,
-                                     int *__restrict__ sframe) {
+                                     int *__restrict__ sframe, int *__restrict__ iperm) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= mtot) return;
     int g = perm[j];
+    iperm[g] = (int)j;
     c0[j] = cos_in[g];
     if (ndim > 1) c1[j] = cos_in[mtot + g];
     if (ndim > 2) c2[j] = cos_in[2 * mtot + g];
@@ -165,6 +166,8 @@ void free_plan_buffers(pfb_plan *p) {
         p->d_cos[a] = p->d_apod[a] = nullptr;
     }
     cudaFree(p->d_perm);
+    cudaFree(p->d_iperm);
+    p->d_iperm = nullptr;
     cudaFree(p->d_sframe);
     cudaFree(p->d_bin_start);
     cudaFree(p->d_items_frame);
@@ -331,6 +334,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
                                cudaMemcpyHostToDevice, stream));
     for (int a = 0; a < ndim; ++a) PFB_TRY_ST(dev_alloc(&p->d_cos[a], mtot));
     PFB_TRY_ST(dev_alloc(&p->d_perm, mtot));
+    PFB_TRY_ST(dev_alloc(&p->d_iperm, mtot));
     PFB_TRY_ST(dev_alloc(&p->d_sframe, mtot));
     PFB_TRY_ST(dev_alloc(&p->d_bin_start, nkeys + 1));
     PFB_TRY_ST(dev_alloc(&d_cos_tmp, (size_t)ndim * mtot));
@@ -366,7 +370,8 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
         PFB_TRY_CU(cub::DeviceRadixSort::SortPairs(d_temp, temp_bytes, d_keys, d_keys_sorted, d_vals,
                                                    p->d_perm, (int)mtot, 0, end_bit, stream));
         gather_sorted_kernel<<<blocks, T, 0, stream>>>(ndim, mtot, nframes, d_cos_tmp, p->d_perm, d_keys_sorted,
-                                                       p->d_cos[0], p->d_cos[1], p->d_cos[2], p->d_sframe);
+                                                       p->d_cos[0], p->d_cos[1], p->d_cos[2], p->d_sframe,
+                                                       p->d_iperm);
         PFB_TRY_CU(cudaGetLastError());
     }
     bin_start_kernel<<<(nkeys + 1 + T - 1) / T, T, 0, stream>>>(d_keys_sorted, mtot, nkeys, p->d_bin_start);
