@@ -125,6 +125,8 @@ struct pfb_plan {
     float *d_cos[pfb::kMaxDim] = {nullptr, nullptr, nullptr};  // bin-sorted oversampled coords
     int *d_perm = nullptr;       // sorted position -> global sample index
     int *d_iperm = nullptr;      // global sample index -> sorted position
+    float *d_wtap = nullptr;     // per sorted sample: D x WM kernel weights (WM = 4 for W <= 4, else 8)
+    int *d_xtap = nullptr;       // per sorted sample: D first taps x0 mod n_os
     int *d_sframe = nullptr;     // sorted position -> frame
     int *d_bin_start = nullptr;  // (nbins_total * ncode * F + 1) offsets into the sorted order
     int nbins_total = 0;
@@ -341,6 +343,8 @@ int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const flo
 int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void *dst, void *ws, size_t wsb,
                float factor, bool accumulate, cudaStream_t s);
 int build_owner_items(pfb_plan *p, int chunk);
+// per-sample kernel weights and first taps of the sorted samples (plan time)
+int build_plan_taps(pfb_plan *p, cudaStream_t s);
 void free_owner_items(pfb_plan *p);
 
 // fused pruned FFT (pfb_fft.cu): 1 when it applies to the plan (tables ready)

@@ -366,6 +366,8 @@ struct InterpIL {
     float chain[kMaxDim];
     float *grad;          // (M, ndim) in original sample order
     int accumulate;
+    const float *wtap;    // plan taps: [M][D * WM] weights, [M][D] first taps mod n_os
+    const int *xtap;
 };
 
 // Per-sample tap weights and FFT-layout positions, computed by lanes (axis, i)
@@ -396,6 +398,17 @@ __device__ __forceinline__ void warp_taps(const InterpIL &P, int64_t j, float *s
         sw[a * WM + i] = wv;
         sp[a * WM + i] = q;
         if (DERIV) sd[a * WM + i] = dv;
+    }
+}
+
+// The same from the plan's per-sample taps: weights as stored, positions from
+// the first tap x0 mod n_os.
+template <int D, int WM>
+__device__ __forceinline__ void warp_taps_plan(const InterpIL &P, int64_t j, float *sw, int *sp, int lane) {
+    if (lane < D * WM) {
+        const int a = lane / WM, i = lane - a * WM;
+        sw[lane] = P.wtap[j * (D * WM) + lane];
+        sp[lane] = pmod((long long)P.xtap[j * D + a] + i - P.g.sh[a], P.g.nos[a]);
     }
 }
 
@@ -443,7 +456,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const Interp
     const int64_t per = (P.mtot + gridDim.x - 1) / gridDim.x;
     const int64_t jbeg = (int64_t)blockIdx.x * per, jend = min(P.mtot, jbeg + per);
     for (int64_t j = jbeg + warp; j < jend; j += kTileWarps) {
-        warp_taps<D, WM, false>(P, j, s_w[warp], s_p[warp], nullptr, lane);
+        warp_taps_plan<D, WM>(P, j, s_w[warp], s_p[warp], lane);
         __syncwarp();
         const int grp = P.ch.K ? 0 : P.sframe[j];
         const float2 *G = P.grid + (int64_t)grp * P.g.gvol * nch;
@@ -1090,7 +1103,7 @@ int layout_ws(pfb_plan *p, const Chan &c, WsLayout *L, cufftHandle *h, size_t *w
     L->gridi = L->gridp;
     L->samp = up256((size_t)p->mtot * c.nch * sizeof(float2));
     const int D = p->g.ndim, WM = wm_of(p->g);
-    L->taps = up256((size_t)p->mtot * D * WM * sizeof(float)) + up256((size_t)p->mtot * D * sizeof(int));
+    L->taps = 0;  // the per-sample taps live in the plan
     L->work = up256(*wb);
     L->total = L->gridp + L->gridi + L->samp + L->taps + L->work;
     return PFB_OK;
@@ -1154,6 +1167,8 @@ void fill_interp(const pfb_plan *p, const Chan &c, InterpIL &P) {
     P.cw = std::min(32, pow2ceil(c.nch));
     P.frame_off = p->d_frame_off;
     P.readout = p->readout;
+    P.wtap = p->d_wtap;
+    P.xtap = p->d_xtap;
     for (int a = 0; a < kMaxDim; ++a) P.chain[a] = (float)p->g.nos[a] / (float)p->g.n[a];
 }
 
@@ -1245,9 +1260,8 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
     float2 *gridp = static_cast<float2 *>(ws);
     float2 *gridi = reinterpret_cast<float2 *>(static_cast<char *>(ws) + L.gridp);
     float2 *samp = reinterpret_cast<float2 *>(static_cast<char *>(ws) + L.gridp + L.gridi);
-    float *wtap = reinterpret_cast<float *>(static_cast<char *>(ws) + L.gridp + L.gridi + L.samp);
-    int *xtap = reinterpret_cast<int *>(reinterpret_cast<char *>(wtap) +
-                                        up256((size_t)p->mtot * p->g.ndim * wm_of(p->g) * sizeof(float)));
+    const float *wtap = p->d_wtap;
+    const int *xtap = p->d_xtap;
     void *work = static_cast<char *>(ws) + L.gridp + L.gridi + L.samp + L.taps;
     const bool basis = d.basis != nullptr;
     const bool w4 = wmax_of(p->g) <= 4;
@@ -1380,18 +1394,6 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
                 PFB_CHECK_LAUNCH();
             }
             if (nitems == 0) return PFB_OK;
-            if (p->mtot > 0) {
-                const int tb = flat_blocks(p->mtot);
-                switch (p->g.ndim * 10 + wm_of(p->g)) {
-                    case 14: taps_prep_kernel<1, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
-                    case 18: taps_prep_kernel<1, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
-                    case 24: taps_prep_kernel<2, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
-                    case 28: taps_prep_kernel<2, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
-                    case 34: taps_prep_kernel<3, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
-                    default: taps_prep_kernel<3, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, wtap, xtap); break;
-                }
-                PFB_CHECK_LAUNCH();
-            }
             SpreadIL S{};
             S.g = p->g;
             S.cos0 = p->d_cos[0];
@@ -1582,7 +1584,36 @@ int build_owner_items(pfb_plan *p, int chunk) {
     return PFB_OK;
 }
 
+int build_plan_taps(pfb_plan *p, cudaStream_t s) {
+    cudaFree(p->d_wtap);
+    cudaFree(p->d_xtap);
+    p->d_wtap = nullptr;
+    p->d_xtap = nullptr;
+    const int D = p->g.ndim, WM = wm_of(p->g);
+    const size_t n = (size_t)std::max<int64_t>(p->mtot, 1);
+    PFB_CUDA_TRY(cudaMalloc(&p->d_wtap, n * D * WM * sizeof(float)));
+    PFB_CUDA_TRY(cudaMalloc(&p->d_xtap, n * D * sizeof(int)));
+    if (p->mtot == 0) return PFB_OK;
+    const int tb = flat_blocks(p->mtot);
+    float *w = p->d_wtap;
+    int *x = p->d_xtap;
+    switch (D * 10 + WM) {
+        case 14: taps_prep_kernel<1, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
+        case 18: taps_prep_kernel<1, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
+        case 24: taps_prep_kernel<2, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
+        case 28: taps_prep_kernel<2, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
+        case 34: taps_prep_kernel<3, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
+        default: taps_prep_kernel<3, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
+    }
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
 void free_owner_items(pfb_plan *p) {
+    cudaFree(p->d_wtap);
+    cudaFree(p->d_xtap);
+    p->d_wtap = nullptr;
+    p->d_xtap = nullptr;
     cudaFree(p->d_own_frame);
     cudaFree(p->d_zero_frame);
     cudaFree(p->d_own_all);

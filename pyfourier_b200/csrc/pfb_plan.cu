@@ -411,6 +411,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
     int chunk = ndim == 3 ? 256 : 512;
     PFB_TRY_ST(rebuild_items(p, chunk));
     PFB_TRY_ST(build_owner_items(p, ndim == 3 ? 2048 : 4096));
+    PFB_TRY_ST(build_plan_taps(p, stream));
     // twiddle tables of the fused transform now, so that no apply allocates
     // (applies may be captured into CUDA graphs)
     fft_fused_ready(p);
