@@ -250,6 +250,10 @@ struct ColPass {
     int accumulate;
 };
 
+// VEC: a thread moves two adjacent columns (16 bytes) in the copy, finish and
+// store loops; the host selects it when every base and stride is even in
+// elements (16-byte aligned pairs) and X is even.
+template <bool VEC>
 __global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
     extern __shared__ float2 fsm[];
     const int n = P.fa.n;
@@ -260,13 +264,24 @@ __global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
     blk /= nxc;
     const int mid = blk % P.nmid;
     const int plane = blk / P.nmid;
-    const int col = threadIdx.x & (kCols - 1), stream = threadIdx.x >> 4;
+    // element loops: NC columns per thread starting at column col, NS streams over positions
+    constexpr int NC = VEC ? 2 : 1;
+    constexpr int NS = kThreads * NC / kCols;
+    const int col = (threadIdx.x % (kCols / NC)) * NC, stream = threadIdx.x / (kCols / NC);
     const int x = xc * kCols + col;
-    const bool xin = x < P.X;
-    const int xs = xin ? x : P.X - 1;  // in-bounds address for columns past the edge
+    const bool xin = x < P.X;  // VEC: X is even, so both columns of the pair are in or out
+    const int xs = xin ? x : P.X - NC;  // in-bounds address for columns past the edge
     const int hn = P.nax / 2;
     const int Kc = P.ch.K ? P.ch.K : 1;
     const int nl = P.mode == 2 ? P.ch.L : 1;
+    // per-column factors of the image side (deapodisation across the mid and x axes)
+    float amid[NC];
+#pragma unroll
+    for (int k = 0; k < NC; ++k) {
+        amid[k] = P.factor;
+        if (P.mode != 0 && P.apod_mid) amid[k] *= P.apod_mid[mid];
+        if (P.mode != 0 && P.apod_x) amid[k] *= P.apod_x[xs + k];
+    }
     for (int l = 0; l < nl; ++l) {
         int64_t in_base;
         const float2 *cl = nullptr;
@@ -284,9 +299,9 @@ __global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
         } else {
             in_base = (int64_t)plane * P.in_plane + mid * P.in_mid;
         }
-        // all copies of the column in flight at once (C_l into the scratch buffer);
-        // positions without input are zero-filled
-        for (int p = stream; p < n; p += kStreams) {
+        // all copies of the column block in flight at once (C_l into the scratch
+        // buffer); positions without input are zero-filled
+        for (int p = stream; p < n; p += NS) {
             int i = p;
             if (!P.inv) {
                 i = p + hn;
@@ -294,70 +309,103 @@ __global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
             }
             const bool valid = i < P.lin;
             const int64_t off = (int64_t)(valid ? i : 0) * P.in_ax + xs;
-            cp_async8(A + p * kPitch + col, P.src + in_base + off, valid);
-            if (cl) cp_async8(Bf + p * kPitch + col, cl + off, valid);
+            if (VEC) {
+                cp_async16(A + p * kPitch + col, P.src + in_base + off, valid);
+                if (cl) cp_async16(Bf + p * kPitch + col, cl + off, valid);
+            } else {
+                cp_async8(A + p * kPitch + col, P.src + in_base + off, valid);
+                if (cl) cp_async8(Bf + p * kPitch + col, cl + off, valid);
+            }
         }
         cp_async_commit();
         cp_async_wait_all();
         if (P.mode == 1 || P.inv) {
             // each thread finishes the elements it copied
-            float amid = P.factor;
-            if (P.mode == 1 && P.apod_mid) amid *= P.apod_mid[mid];
-            if (P.mode == 1 && P.apod_x) amid *= P.apod_x[xs];
-            for (int p = stream; p < n; p += kStreams) {
+            for (int p = stream; p < n; p += NS) {
                 int i = p;
                 if (!P.inv) {
                     i = p + hn;
                     if (i >= n) i -= n;
                 }
                 if (i >= P.lin) continue;
-                float2 v = A[p * kPitch + col];
-                if (P.mode == 1) {
-                    if (cl) v = cmul(v, Bf[p * kPitch + col]);
-                    const float a = P.apod_ax ? amid * P.apod_ax[i] : amid;
-                    v = make_float2(v.x * a, v.y * a);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    float2 v = A[p * kPitch + col + k];
+                    if (P.mode == 1) {
+                        if (cl) v = cmul(v, Bf[p * kPitch + col + k]);
+                        const float a = P.apod_ax ? amid[k] * P.apod_ax[i] : amid[k];
+                        v = make_float2(v.x * a, v.y * a);
+                    }
+                    if (P.inv) v.y = -v.y;
+                    A[p * kPitch + col + k] = v;
                 }
-                if (P.inv) v.y = -v.y;
-                A[p * kPitch + col] = v;
             }
         }
         __syncthreads();
         const float2 *R = fft_run(A, Bf, P.fa);
         if (P.mode == 2) {
-            float amid = P.factor;
-            if (P.apod_mid) amid *= P.apod_mid[mid];
-            if (P.apod_x) amid *= P.apod_x[xs];
             const int64_t out_base = (int64_t)plane * P.nvol + mid * P.out_mid;
-            for (int o = stream; o < P.lout; o += kStreams) {
+            for (int o = stream; o < P.lout; o += NS) {
                 int pp = o - hn;
                 if (pp < 0) pp += n;
-                float2 v = R[pp * kPitch + col];
-                v.y = -v.y;
-                if (P.Cl) v = cmulc(v, P.Cl[(int64_t)l * P.nvol + (int64_t)o * P.out_ax + mid * P.out_mid + xs]);
-                if (l > 0) v = cadd(v, Acc[o * kPitch + col]);
+                const int64_t oo = (int64_t)o * P.out_ax + mid * P.out_mid;
+                float2 v[NC];
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    v[k] = R[pp * kPitch + col + k];
+                    v[k].y = -v[k].y;
+                    if (P.Cl) v[k] = cmulc(v[k], P.Cl[(int64_t)l * P.nvol + oo + xs + k]);
+                    if (l > 0) v[k] = cadd(v[k], Acc[o * kPitch + col + k]);
+                }
                 if (l + 1 < nl) {
-                    Acc[o * kPitch + col] = v;
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) Acc[o * kPitch + col + k] = v[k];
                 } else if (xin) {
                     // last segment: deapodise, scale and write the image
-                    const float a = P.apod_ax ? amid * P.apod_ax[o] : amid;
-                    v = make_float2(v.x * a, v.y * a);
+#pragma unroll
+                    for (int k = 0; k < NC; ++k) {
+                        const float a = P.apod_ax ? amid[k] * P.apod_ax[o] : amid[k];
+                        v[k] = make_float2(v[k].x * a, v[k].y * a);
+                    }
                     float2 *d = P.dst + out_base + (int64_t)o * P.out_ax + x;
-                    if (P.accumulate) v = cadd(v, *d);
-                    *d = v;
+                    if (VEC) {
+                        float4 r = make_float4(v[0].x, v[0].y, v[NC - 1].x, v[NC - 1].y);
+                        if (P.accumulate) {
+                            const float4 old = *reinterpret_cast<const float4 *>(d);
+                            r.x += old.x;
+                            r.y += old.y;
+                            r.z += old.z;
+                            r.w += old.w;
+                        }
+                        *reinterpret_cast<float4 *>(d) = r;
+                    } else {
+                        if (P.accumulate) v[0] = cadd(v[0], *d);
+                        *d = v[0];
+                    }
                 }
             }
             if (l + 1 < nl) __syncthreads();  // the next segment reloads A
         } else {
             const int64_t out_base = (int64_t)plane * P.out_plane + mid * P.out_mid;
-            for (int o = stream; o < P.lout; o += kStreams) {
+            for (int o = stream; o < P.lout; o += NS) {
                 int pp = o;
                 if (P.inv) {
                     pp = o - hn;
                     if (pp < 0) pp += n;
                 }
-                float2 v = R[pp * kPitch + col];
-                if (P.inv) v.y = -v.y;
-                if (xin) P.dst[out_base + (int64_t)o * P.out_ax + x] = v;
+                float2 *d = P.dst + out_base + (int64_t)o * P.out_ax + x;
+                if (VEC) {
+                    float4 r = *reinterpret_cast<const float4 *>(R + pp * kPitch + col);
+                    if (P.inv) {
+                        r.y = -r.y;
+                        r.w = -r.w;
+                    }
+                    if (xin) *reinterpret_cast<float4 *>(d) = r;
+                } else {
+                    float2 v = R[pp * kPitch + col];
+                    if (P.inv) v.y = -v.y;
+                    if (xin) *d = v;
+                }
             }
         }
     }
@@ -492,8 +540,16 @@ int launch_col(const ColPass &P, cudaStream_t s) {
     if (blocks == 0) return PFB_OK;
     if (blocks >= (1LL << 31)) return fail(PFB_ERR_UNSUPPORTED, "too many vectors for the fused FFT");
     const size_t smem = col_smem(P.fa.n, P.mode, P.ch.L);
-    PFB_CUDA_TRY(cudaFuncSetAttribute(col_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    col_pass_kernel<<<(unsigned)blocks, kThreads, smem, s>>>(P);
+    // two-column moves when every base and stride keeps the pairs 16-byte aligned
+    auto a16 = [](const void *q) { return ((uintptr_t)q & 15u) == 0; };
+    const bool img_in = P.mode == 1, img_out = P.mode == 2;
+    bool vec = P.X % 2 == 0 && a16(P.src) && a16(P.dst) && (!P.Cl || a16(P.Cl)) && P.in_mid % 2 == 0 &&
+               P.in_ax % 2 == 0 && P.out_mid % 2 == 0 && P.out_ax % 2 == 0;
+    vec = vec && (img_in || img_out ? P.nvol % 2 == 0 : true);
+    vec = vec && (img_in ? true : P.in_plane % 2 == 0) && (img_out ? true : P.out_plane % 2 == 0);
+    auto k = vec ? col_pass_kernel<true> : col_pass_kernel<false>;
+    PFB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<(unsigned)blocks, kThreads, smem, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
 }
