@@ -457,7 +457,24 @@ __global__ void __launch_bounds__(kThreads) row_fwd_kernel(const RowPass P) {
     }
     __syncthreads();
     const float2 *R = fft_run(A, Bf, P.fa);
-    {
+    if (P.nch % 2 == 0) {
+        // even channel count: vectors u, u + 1 (u even) are channels ch, ch + 1 of the
+        // same point, stored together as one float4
+        const int v = (threadIdx.x & 7) * 2;
+        const int64_t u = u0 + v;
+        if (u < P.nvec) {
+            const int chn = (int)(u % P.nch);
+            int64_t r = u / P.nch;
+            const int ky = (int)(r % P.nos1);
+            r /= P.nos1;
+            const int kz = (int)(r % P.nos2);
+            const int64_t grp = r / P.nos2;
+            const int64_t base = (grp * P.gvol + ((int64_t)kz * P.nos1 + ky) * n) * P.nch + chn;
+            for (int kx = threadIdx.x >> 3; kx < n; kx += 2 * kStreams)
+                *reinterpret_cast<float4 *>(P.dst + base + (int64_t)kx * P.nch) =
+                    *reinterpret_cast<const float4 *>(R + kx * kPitch + v);
+        }
+    } else {
         const int v = threadIdx.x & 15;
         const int64_t u = u0 + v;
         if (u < P.nvec) {
