@@ -447,7 +447,7 @@ def time_device(torch, fn, steps, warmup):
 
 
 def extra_workload(args):
-    """2D radial (cfg1), Toeplitz Gram (cfg3), B0 plain vs batched (cfg4), autograd (cfg5)."""
+    """2D radial (cfg1), Toeplitz Gram (cfg3), B0 plain vs batched (cfg4), autograd (cfg5), Pipe-Menon DCF (dcf)."""
     import torch
 
     import pyfourier_b200 as pf
@@ -558,6 +558,29 @@ def extra_workload(args):
                             "batched_over_plain": ms_plain / ms_graph,
                             "batched_stages_ms": {k: round(v, 4) for k, v in stages.items()}},
                     cpu_baseline=None)
+    elif args.workload == "dcf":
+        # Pipe-Menon density compensation with the reference's defaults (W 6, osf 1.5, 30 iterations)
+        N, nsp, nrd, niter = 128, 8000, 256, 30
+        coord = golden_means_radial_3d(nsp, nrd, N)
+        ct = torch.as_tensor(coord, device=dev)
+        step = lambda: pf.pipe_menon_dcf(ct, (N, N, N), niter=niter)  # noqa: E731
+        clocks.start()
+        ms = time_device(torch, step, args.steps, args.warmup)
+        clk = clocks.stop()
+        M = nsp * nrd
+        # CPU: the oracle's restatement, one iteration (bounded sample), scaled to iterations/s
+        t0 = time.perf_counter()
+        orc.pipe_menon_dcf(coord, (N, N, N), niter=1)
+        cpu_s = time.perf_counter() - t0
+        line.update(metric="Pipe-Menon DCF iterations/s (3D golden-means radial, 128^3, W 6, osf 1.5)",
+                    value=niter / (ms / 1e3), unit="iterations/s", ms_per_step=ms,
+                    config={"workload": "pipe_menon_dcf, 30 iterations of w / |A A^H w| per step",
+                            "image": [N, N, N], "spokes": nsp, "readout": nrd, "samples": M, "iterations": niter,
+                            "width": 6, "oversamp": 1.5, "grid": [192, 192, 192],
+                            "sample_iterations_per_s": niter * M / (ms / 1e3)},
+                    cpu_baseline={"value": 1.0 / cpu_s, "unit": "iterations/s", "cores": orc.lib().orc_num_threads(),
+                                  "kind": "port", "sample": "one iteration of the oracle's pipe_menon_dcf "
+                                                            "(plan build included)"})
     elif args.workload == "cfg5":
         N, B, nimg = 256, 8, 32
         coord = vd_spiral(16, 4096, N)
@@ -605,13 +628,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg1", "cfg3", "cfg4", "cfg5"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg1", "cfg3", "cfg4", "cfg5", "dcf"])
     ap.add_argument("--cpu-coils", type=int, default=2, help="coils in the bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-launch-trace", action="store_true",
                     help="skip the CUDA activity trace that counts launches (for runs under ncu)")
     args = ap.parse_args()
-    if args.workload in ("cfg1", "cfg3", "cfg4", "cfg5"):
+    if args.workload in ("cfg1", "cfg3", "cfg4", "cfg5", "dcf"):
         extra_workload(args)
         return
     wl = WORKLOADS[args.workload]

@@ -252,6 +252,20 @@ int pfb_nufft_traj_grad(pfb_plan *plan, const pfb_apply_t *opt, const void *imag
 int pfb_nufft_stage(pfb_plan *plan, const pfb_apply_t *opt, int stage, const void *src, void *dst,
                     float factor, void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- density compensation (src/pyfourier/_dcomp) ------------------------------ */
+
+/* Pipe-Menon density compensation, replacing pipe_menon_dcf
+ * (src/pyfourier/_dcomp/pipemenon.py:9-96, _GHG :99-115): niter times
+ *     w <- w / |A A^H w|
+ * with A the plan's NUFFT (norm "ortho"), one channel over all the plan's
+ * frames.  weights: device float32 (total samples) in the original sample
+ * order, updated in place; the caller sets the start (ones in the reference).
+ * The iterations run back to back on `stream` without host synchronisation.
+ * Workspace: pfb_dcf_workspace_size bytes. */
+int pfb_dcf_workspace_size(pfb_plan *plan, size_t *bytes);
+int pfb_pipe_menon_dcf(pfb_plan *plan, float *weights, int niter, void *workspace, size_t workspace_bytes,
+                       void *stream);
+
 /* ---- Toeplitz Gram (src/pyfourier/_sparsegram) ------------------------------------ */
 
 /* Create a Gram operator from its Toeplitz kernel on the 2x grid.

@@ -613,6 +613,22 @@ def _sparse_gram1(image, gram, norm=None):
 
 
 # --------------------------------------------------------------------------------------
+# Pipe-Menon density compensation
+# --------------------------------------------------------------------------------------
+def pipe_menon_dcf(coord, shape, niter=30, width=6, oversamp=1.5):
+    """src/pyfourier/_dcomp/pipemenon.py:9-96: w = ones(coord.shape[:-1]); the plan
+    with (width, oversamp); niter times w = w / |nufft(nufft_adj(w, ortho), ortho)|
+    (_GHG, :99-115).  float32 like the reference's weights."""
+    coord = np.asarray(coord, np.float32)
+    w = np.ones(coord.shape[:-1], np.float32)
+    plan = plan_nufft(coord, shape, width=width, oversamp=oversamp)
+    for _ in range(niter):
+        ghg = nufft_fwd(nufft_adj(w.astype(np.complex64), plan, norm="ortho"), plan, norm="ortho")
+        w = (w / np.abs(ghg)).astype(np.float32)
+    return w
+
+
+# --------------------------------------------------------------------------------------
 # FP64 references
 # --------------------------------------------------------------------------------------
 def pixel_grid(shape_zyx):

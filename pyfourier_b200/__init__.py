@@ -2,7 +2,8 @@
 
 Drop-in entry points (same names, arguments and shape conventions as
 pyfourier): ``nufft``, ``nufft_adj``, ``plan_nufft`` / ``NUFFTPlan``,
-``plan_spgram`` / ``sparse_gram`` / ``GramMatrix``.  Everything computes in
+``plan_spgram`` / ``sparse_gram`` / ``GramMatrix``, ``pipe_menon_dcf`` (also
+as ``pipemenon.pipe_menon_dcf``).  Everything computes in
 ``libpfb200.so`` through its C ABI (include/pfb200.h); there is no CPU
 fallback and importing an operator without the library raises.
 """
@@ -10,13 +11,16 @@ fallback and importing an operator without the library raises.
 from . import _lib
 from ._autotune import autotune
 from ._b0 import mri_exp_approx
+from ._dcf import pipe_menon_dcf
 from ._gram import GramMatrix, plan_spgram, sparse_gram
 from ._nufft import nufft, nufft_adj
 from ._plan import Interpolator, NUFFTPlan, plan_nufft
+from . import pipemenon  # noqa: E402  (module path of the reference: pyfourier.pipemenon)
 
 __version__ = "0.1.0"
 
 __all__ = [
     "nufft", "nufft_adj", "plan_nufft", "NUFFTPlan", "Interpolator",
-    "plan_spgram", "sparse_gram", "GramMatrix", "mri_exp_approx", "autotune",
+    "plan_spgram", "sparse_gram", "GramMatrix", "mri_exp_approx", "autotune", "pipe_menon_dcf",
+    "pipemenon",
 ]

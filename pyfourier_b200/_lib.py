@@ -27,7 +27,7 @@ STAGES = {"pad": 0, "fft": 1, "interp": 2, "out": 3, "vals": 4, "spread": 5, "if
 
 # Every symbol exported by the C ABI (kept in sync with include/pfb200.h).
 EXPORTS = (
-    "pfb_last_error", "pfb_version", "pfb_plan_create", "pfb_plan_destroy", "pfb_plan_info",
+    "pfb_last_error", "pfb_version", "pfb_plan_create", "pfb_plan_destroy", "pfb_plan_info", "pfb_dcf_workspace_size", "pfb_pipe_menon_dcf",
     "pfb_plan_set_tuning", "pfb_plan_set_chunk", "pfb_plan_tables", "pfb_workspace_size",
     "pfb_nufft_fwd", "pfb_nufft_adj", "pfb_spread", "pfb_interp", "pfb_deapod_pad",
     "pfb_crop_deapod", "pfb_grid_fft", "pfb_traj_grad", "pfb_gram_create", "pfb_gram_destroy",
@@ -96,6 +96,8 @@ def load(path=LIB_PATH):
                                   i32, vp, P(vp)]),
         "pfb_plan_destroy": (i32, [vp]),
         "pfb_plan_info": (i32, [vp, P(PlanInfoT)]),
+        "pfb_dcf_workspace_size": (i32, [vp, P(ctypes.c_size_t)]),
+        "pfb_pipe_menon_dcf": (i32, [vp, vp, i32, vp, ctypes.c_size_t, vp]),
         "pfb_plan_set_tuning": (i32, [vp, i32, i32, i32]),
         "pfb_plan_set_chunk": (i32, [vp, i32]),
         "pfb_plan_tables": (i32, [vp, i32, vp, vp, vp]),

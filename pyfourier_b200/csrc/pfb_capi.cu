@@ -234,9 +234,6 @@ int pfb_nufft_fwd(pfb_plan *p, const pfb_apply_t *opt, const void *image, void *
     if (d.batch == 0) return PFB_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int64_t P = planes_of(d);
-    cufftHandle h;
-    size_t wb = 0;
-    if ((st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, &h, &wb))) return st;
     // forward: unnormalised FFT ("ortho": 1/sqrt(G)), and 1/scale of _cart2noncart:110
     double fac = 1.0 / p->scale;
     if (d.norm == PFB_NORM_ORTHO) fac /= std::sqrt((double)p->g.gvol);
@@ -245,6 +242,9 @@ int pfb_nufft_fwd(pfb_plan *p, const pfb_apply_t *opt, const void *image, void *
     if (fast_supported(p, d, nullptr) && fast_workspace(p, d, &fast_bytes) == PFB_OK && workspace_bytes >= fast_bytes)
         return fast_fwd(p, d, static_cast<const float2 *>(image), static_cast<float2 *>(kspace), workspace,
                         workspace_bytes, (float)fac, opt->flags & PFB_FLAG_ACCUMULATE, s);
+    cufftHandle h;
+    size_t wb = 0;
+    if ((st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, &h, &wb))) return st;
     size_t gbytes = align_up((size_t)P * p->g.gvol * sizeof(float2));
     if (workspace_bytes < gbytes + wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
     float2 *grid = static_cast<float2 *>(workspace);
@@ -264,9 +264,6 @@ int pfb_nufft_adj(pfb_plan *p, const pfb_apply_t *opt, const void *kspace, void 
     if (d.batch == 0) return PFB_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int64_t P = planes_of(d);
-    cufftHandle h;
-    size_t wb = 0;
-    if ((st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, &h, &wb))) return st;
     // adjoint: inverse FFT scaled 1/G (None) or 1/sqrt(G) (ortho), and 1/scale of _noncart2cart:119
     double fac = 1.0 / p->scale;
     fac /= (d.norm == PFB_NORM_ORTHO) ? std::sqrt((double)p->g.gvol) : (double)p->g.gvol;
@@ -274,6 +271,9 @@ int pfb_nufft_adj(pfb_plan *p, const pfb_apply_t *opt, const void *kspace, void 
     if (fast_supported(p, d, nullptr) && fast_workspace(p, d, &fast_bytes) == PFB_OK && workspace_bytes >= fast_bytes)
         return fast_adj(p, d, static_cast<const float2 *>(kspace), static_cast<float2 *>(image), workspace,
                         workspace_bytes, (float)fac, opt->flags & PFB_FLAG_ACCUMULATE, s);
+    cufftHandle h;
+    size_t wb = 0;
+    if ((st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, P, &h, &wb))) return st;
     size_t gbytes = align_up((size_t)P * p->g.gvol * sizeof(float2));
     if (workspace_bytes < gbytes + wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
     float2 *grid = static_cast<float2 *>(workspace);

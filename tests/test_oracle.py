@@ -177,3 +177,17 @@ def test_oracle_gram_with_field_map_vs_exact():
     E = np.exp(-2j * np.pi * (cm / N) @ r.T) * np.exp(-2j * np.pi * tm[:, None] * b0.ravel()[None, :])
     ref = (E.conj().T @ (E @ x.ravel().astype(np.complex128))).reshape(N, N)
     assert orc.rel_l2(g, ref) < 2e-2
+
+
+def test_oracle_pipe_menon_weights_grow_with_radius():
+    """Pipe-Menon on a radial trajectory: the weights follow the 1/density of the
+    spokes, growing with |k| (averaged over spokes, outer ring vs inner ring)."""
+    N, ns = 32, 64
+    coord = _radial(48, ns, N)
+    w = orc.pipe_menon_dcf(coord, (N, N), niter=15)
+    assert w.shape == coord.shape[:-1] and w.dtype == np.float32
+    assert np.all(np.isfinite(w)) and np.all(w > 0)
+    kr = np.abs(np.arange(ns) - ns // 2)
+    inner = w[:, (kr >= 2) & (kr < 8)].mean()
+    outer = w[:, (kr >= 20) & (kr < 28)].mean()
+    assert outer > 2.0 * inner
