@@ -613,6 +613,61 @@ def _sparse_gram1(image, gram, norm=None):
 
 
 # --------------------------------------------------------------------------------------
+# Sparse (Cartesian-subsampled) FFT
+# --------------------------------------------------------------------------------------
+def _sparse_index(indexes, shape):
+    """(frames, npts, ndim) integer grid indexes in (z, y, x) order (centred input,
+    any entry negative, shifted by N // 2, the intent of _traj.py:36-53), and dshape."""
+    idx = np.rint(np.asarray(indexes, np.float64)).astype(np.int64)
+    nd = idx.shape[-1]
+    if (idx < 0).any():
+        idx = idx + np.asarray([s // 2 for s in shape[::-1]])
+    ds = list(idx.shape[:-1])
+    while len(ds) < 3:
+        ds = [1] + ds
+    return idx.reshape(ds[0], -1, nd)[..., ::-1], tuple(ds[1:])
+
+
+def sparse_fftn(image, indexes, shape, basis=None, norm=None):
+    """src/pyfourier/_sparsefft/_sparsefft.py:98-108 + _mask/_dense2sparse: centred FFT,
+    then y[b, f, p] = X[b, f][idx] (or sum_k basis[f, k] X[b, k][idx])."""
+    nd = len(shape)
+    idx, ds = _sparse_index(indexes, shape)
+    F = idx.shape[0]
+    X = fft_c(np.asarray(image, np.complex64), nd, norm)
+    C = X.shape[-nd - 1] if (basis is not None or F > 1) else 1
+    X = X.reshape(-1, C, *shape)
+    out = np.zeros((X.shape[0], F, idx.shape[1]), np.complex64)
+    for f in range(F):
+        sel = tuple(idx[f, :, a] for a in range(nd))
+        if basis is None:
+            out[:, f] = X[:, f if C > 1 else 0][(slice(None),) + sel]
+        else:
+            out[:, f] = np.einsum("k,bkp->bp", np.asarray(basis)[f], X[(slice(None), slice(None)) + sel])
+    return out
+
+
+def sparse_ifftn(kspace, indexes, shape, basis=None, norm=None):
+    """src/pyfourier/_sparsefft/_sparsefft.py:111-121 + _mask/_sparse2dense: scatter-add
+    (duplicates add; basis conj-transposed), then the centred inverse FFT."""
+    nd = len(shape)
+    idx, ds = _sparse_index(indexes, shape)
+    F = idx.shape[0]
+    y = np.asarray(kspace, np.complex64).reshape(-1, F, idx.shape[1])
+    C = np.asarray(basis).shape[1] if basis is not None else F
+    grid = np.zeros((y.shape[0], C, *shape), np.complex64)
+    for f in range(F):
+        sel = tuple(idx[f, :, a] for a in range(nd))
+        for b in range(y.shape[0]):
+            if basis is None:
+                np.add.at(grid[b, f], sel, y[b, f])
+            else:
+                for k in range(C):
+                    np.add.at(grid[b, k], sel, np.conj(np.asarray(basis)[f, k]) * y[b, f])
+    return ifft_c(grid, nd, norm)
+
+
+# --------------------------------------------------------------------------------------
 # Pipe-Menon density compensation
 # --------------------------------------------------------------------------------------
 def pipe_menon_dcf(coord, shape, niter=30, width=6, oversamp=1.5):

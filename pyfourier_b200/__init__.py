@@ -2,7 +2,8 @@
 
 Drop-in entry points (same names, arguments and shape conventions as
 pyfourier): ``nufft``, ``nufft_adj``, ``plan_nufft`` / ``NUFFTPlan``,
-``plan_spgram`` / ``sparse_gram`` / ``GramMatrix``, ``pipe_menon_dcf`` (also
+``plan_spgram`` / ``sparse_gram`` / ``GramMatrix``, ``plan_spfft`` /
+``sparse_fftn`` / ``sparse_ifftn``, ``pipe_menon_dcf`` (also
 as ``pipemenon.pipe_menon_dcf``).  Everything computes in
 ``libpfb200.so`` through its C ABI (include/pfb200.h); there is no CPU
 fallback and importing an operator without the library raises.
@@ -15,6 +16,7 @@ from ._dcf import pipe_menon_dcf
 from ._gram import GramMatrix, plan_spgram, sparse_gram
 from ._nufft import nufft, nufft_adj
 from ._plan import Interpolator, NUFFTPlan, plan_nufft
+from ._sparsefft import FFTPlan, plan_spfft, sparse_fftn, sparse_ifftn
 from . import pipemenon  # noqa: E402  (module path of the reference: pyfourier.pipemenon)
 
 __version__ = "0.1.0"
@@ -22,5 +24,5 @@ __version__ = "0.1.0"
 __all__ = [
     "nufft", "nufft_adj", "plan_nufft", "NUFFTPlan", "Interpolator",
     "plan_spgram", "sparse_gram", "GramMatrix", "mri_exp_approx", "autotune", "pipe_menon_dcf",
-    "pipemenon",
+    "pipemenon", "plan_spfft", "sparse_fftn", "sparse_ifftn", "FFTPlan",
 ]

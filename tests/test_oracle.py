@@ -191,3 +191,29 @@ def test_oracle_pipe_menon_weights_grow_with_radius():
     inner = w[:, (kr >= 2) & (kr < 8)].mean()
     outer = w[:, (kr >= 20) & (kr < 28)].mean()
     assert outer > 2.0 * inner
+
+
+def test_oracle_sparse_fft_is_the_width_one_nufft():
+    """The sparse FFT restatement (centred FFT + gather / scatter-add + centred IFFT)
+    equals the NUFFT restatement on integer coordinates (width 1, no oversampling),
+    with frames, duplicates and a subspace basis."""
+    rng = np.random.default_rng(11)
+    N = (12, 16)
+    F, K = 3, 2
+    idx = np.stack([rng.integers(0, N[1], (F, 5, 7)), rng.integers(0, N[0], (F, 5, 7))], -1).astype(np.float32)
+    idx[0, 0, :2] = idx[0, 0, 2]  # duplicates add in the adjoint
+    basis = (rng.standard_normal((F, K)) + 1j * rng.standard_normal((F, K))).astype(np.complex64)
+    coord = idx - np.array([N[1] // 2, N[0] // 2], np.float32)
+    plan = orc.plan_nufft(coord, N, width=2, oversamp=1.0)
+    assert plan.width == (1, 1) and plan.os_shape == N
+    for b in (None, basis):
+        C = K if b is not None else F
+        x = (rng.standard_normal((2, C, *N)) + 1j * rng.standard_normal((2, C, *N))).astype(np.complex64)
+        y = (rng.standard_normal((2, F, 5, 7)) + 1j * rng.standard_normal((2, F, 5, 7))).astype(np.complex64)
+        for norm in (None, "ortho"):
+            a = orc.sparse_fftn(x, idx, N, basis=b, norm=norm)
+            r = orc.nufft_fwd(x, plan, basis=b, norm=norm).reshape(a.shape)
+            assert orc.rel_l2(a, r) < 1e-6
+            a = orc.sparse_ifftn(y, idx, N, basis=b, norm=norm)
+            r = orc.nufft_adj(y, plan, basis=b, norm=norm).reshape(a.shape)
+            assert orc.rel_l2(a, r) < 1e-6
