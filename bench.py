@@ -447,7 +447,8 @@ def time_device(torch, fn, steps, warmup):
 
 
 def extra_workload(args):
-    """2D radial (cfg1), Toeplitz Gram (cfg3), B0 plain vs batched (cfg4), autograd (cfg5), Pipe-Menon DCF (dcf)."""
+    """2D radial (cfg1), Toeplitz Gram (cfg3), B0 plain vs batched (cfg4), autograd (cfg5), Pipe-Menon DCF (dcf),
+    sparse FFT (spfft)."""
     import torch
 
     import pyfourier_b200 as pf
@@ -558,6 +559,34 @@ def extra_workload(args):
                             "batched_over_plain": ms_plain / ms_graph,
                             "batched_stages_ms": {k: round(v, 4) for k, v in stages.items()}},
                     cpu_baseline=None)
+    elif args.workload == "spfft":
+        # 3D Cartesian acquisition, 25 % of the (ky, kz) phase encodes, full readouts
+        N, B = 128, 32
+        rng = np.random.default_rng(0)
+        pe = rng.choice(N * N, N * N // 4, replace=False)
+        ky, kz = pe % N, pe // N
+        kx = np.arange(N)
+        idx = np.stack([np.broadcast_to(kx[None, :], (pe.size, N)),
+                        np.broadcast_to(ky[:, None], (pe.size, N)),
+                        np.broadcast_to(kz[:, None], (pe.size, N))], -1).astype(np.float32)
+        plan = pf.plan_spfft(torch.as_tensor(idx, device=dev), (N, N, N))
+        x = (coil_maps_3d(torch, N, B, dev) * phantom_3d(torch, N, 20, dev)[None]).contiguous()
+        step = lambda: pf.sparse_ifftn(pf.sparse_fftn(x, plan=plan), plan=plan)  # noqa: E731
+        clocks.start()
+        ms = time_device(torch, step, args.steps, args.warmup)
+        clk = clocks.stop()
+        M = pe.size * N
+        xc = x[:2].cpu().numpy()
+        orc.sparse_ifftn(orc.sparse_fftn(xc, idx, (N, N, N)), idx, (N, N, N))
+        t0 = time.perf_counter()
+        orc.sparse_ifftn(orc.sparse_fftn(xc, idx, (N, N, N)), idx, (N, N, N))
+        cpu_s = time.perf_counter() - t0
+        line.update(metric="sparse FFT fwd+adj samples/s (3D Cartesian 128^3, 25 % phase encodes, 32 coils)",
+                    value=B * M / (ms / 1e3), unit="samples/s", ms_per_step=ms,
+                    config={"workload": "sparse_fftn + sparse_ifftn over all coils", "image": [N, N, N], "coils": B,
+                            "phase_encodes": int(pe.size), "readout": N, "samples_per_coil": M},
+                    cpu_baseline={"value": 2 * M / cpu_s, "unit": "samples/s", "cores": orc.lib().orc_num_threads(),
+                                  "kind": "port", "sample": "2 of 32 coils, one fwd+adj (NumPy FFT, gather, add.at)"})
     elif args.workload == "dcf":
         # Pipe-Menon density compensation with the reference's defaults (W 6, osf 1.5, 30 iterations)
         N, nsp, nrd, niter = 128, 8000, 256, 30
@@ -628,13 +657,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg1", "cfg3", "cfg4", "cfg5", "dcf"])
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg1", "cfg3", "cfg4", "cfg5", "dcf", "spfft"])
     ap.add_argument("--cpu-coils", type=int, default=2, help="coils in the bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-launch-trace", action="store_true",
                     help="skip the CUDA activity trace that counts launches (for runs under ncu)")
     args = ap.parse_args()
-    if args.workload in ("cfg1", "cfg3", "cfg4", "cfg5", "dcf"):
+    if args.workload in ("cfg1", "cfg3", "cfg4", "cfg5", "dcf", "spfft"):
         extra_workload(args)
         return
     wl = WORKLOADS[args.workload]

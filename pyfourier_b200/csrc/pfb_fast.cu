@@ -1087,7 +1087,11 @@ struct WsLayout {
     size_t gridp, gridi, samp, taps, work, total;
 };
 
-int wm_of(const Geom &g) { return std::max(g.w[0], std::max(g.w[1], g.w[2])) <= 4 ? 4 : 8; }
+// taps per axis the kernels are compiled for: 1 (Cartesian / sparse FFT), 4 or 8
+int wm_of(const Geom &g) {
+    const int w = std::max(g.w[0], std::max(g.w[1], g.w[2]));
+    return w == 1 ? 1 : (w <= 4 ? 4 : 8);
+}
 
 int layout_ws(pfb_plan *p, const Chan &c, WsLayout *L, cufftHandle *h, size_t *wb) {
     const int64_t P = (int64_t)c.ngrp * c.nch;
@@ -1102,7 +1106,6 @@ int layout_ws(pfb_plan *p, const Chan &c, WsLayout *L, cufftHandle *h, size_t *w
     L->gridp = up256((size_t)P * p->g.gvol * sizeof(float2));
     L->gridi = L->gridp;
     L->samp = up256((size_t)p->mtot * c.nch * sizeof(float2));
-    const int D = p->g.ndim, WM = wm_of(p->g);
     L->taps = 0;  // the per-sample taps live in the plan
     L->work = up256(*wb);
     L->total = L->gridp + L->gridi + L->samp + L->taps + L->work;
@@ -1172,7 +1175,6 @@ void fill_interp(const pfb_plan *p, const Chan &c, InterpIL &P) {
     for (int a = 0; a < kMaxDim; ++a) P.chain[a] = (float)p->g.nos[a] / (float)p->g.n[a];
 }
 
-int wmax_of(const Geom &g) { return std::max(g.w[0], std::max(g.w[1], g.w[2])); }
 
 size_t tile_points(const pfb_plan *p) {
     return (size_t)p->g.tile[0] * (p->g.ndim > 1 ? p->g.tile[1] : 1) * (p->g.ndim > 2 ? p->g.tile[2] : 1);
@@ -1198,11 +1200,11 @@ int spread_cw(const pfb_plan *p, const Chan &c) {
     return cw;
 }
 
-#define PFB_DISPATCH_DW(ND, W4, CALL4, CALL8)                 \
-    switch (ND) {                                             \
-        case 1: return (W4) ? CALL4(1) : CALL8(1);            \
-        case 2: return (W4) ? CALL4(2) : CALL8(2);            \
-        default: return (W4) ? CALL4(3) : CALL8(3);           \
+#define PFB_DISPATCH_DW(ND, WMV, CALL1, CALL4, CALL8)                              \
+    switch (ND) {                                                                  \
+        case 1: return (WMV) == 1 ? CALL1(1) : ((WMV) == 4 ? CALL4(1) : CALL8(1)); \
+        case 2: return (WMV) == 1 ? CALL1(2) : ((WMV) == 4 ? CALL4(2) : CALL8(2)); \
+        default: return (WMV) == 1 ? CALL1(3) : ((WMV) == 4 ? CALL4(3) : CALL8(3)); \
     }
 
 }  // namespace
@@ -1264,7 +1266,7 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
     const int *xtap = p->d_xtap;
     void *work = static_cast<char *>(ws) + L.gridp + L.gridi + L.samp + L.taps;
     const bool basis = d.basis != nullptr;
-    const bool w4 = wmax_of(p->g) <= 4;
+    const int wmv = wm_of(p->g);
     const int64_t P = (int64_t)c.ngrp * c.nch;
     const bool fused = fft_fused_ready(p) == 1;
     const float *apod[3] = {p->d_apod[0], p->d_apod[1], p->d_apod[2]};
@@ -1340,9 +1342,11 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             Q.grid = gridi;
             Q.res = samp;
             int blocks = sample_blocks(p->mtot);
+#define PFB_I1(DD) launch_interp_il_t<DD, 1>(Q, blocks, s)
 #define PFB_I4(DD) launch_interp_il_t<DD, 4>(Q, blocks, s)
 #define PFB_I8(DD) launch_interp_il_t<DD, 8>(Q, blocks, s)
-            PFB_DISPATCH_DW(p->g.ndim, w4, PFB_I4, PFB_I8)
+            PFB_DISPATCH_DW(p->g.ndim, wmv, PFB_I1, PFB_I4, PFB_I8)
+#undef PFB_I1
 #undef PFB_I4
 #undef PFB_I8
         }
@@ -1414,13 +1418,17 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
                 p->g.tile[2] <= kRegTile && c.nch > 16) {
                 // register-tile form: 32 channels per CTA, no shared atomics
                 const int nchunks = (c.nch + 31) / 32;
-                return w4 ? launch_spread_reg3_t<4>(S, nitems, nchunks, s) : launch_spread_reg3_t<8>(S, nitems, nchunks, s);
+                return wmv == 1 ? launch_spread_reg3_t<1>(S, nitems, nchunks, s)
+                                : (wmv == 4 ? launch_spread_reg3_t<4>(S, nitems, nchunks, s)
+                                            : launch_spread_reg3_t<8>(S, nitems, nchunks, s));
             }
             const size_t smem = spread_smem(p, S.cw);
             const int nchunks = (c.nch + S.cw - 1) / S.cw;
+#define PFB_S1(DD) launch_spread_il_t<DD, 1>(S, nitems, nchunks, smem, s)
 #define PFB_S4(DD) launch_spread_il_t<DD, 4>(S, nitems, nchunks, smem, s)
 #define PFB_S8(DD) launch_spread_il_t<DD, 8>(S, nitems, nchunks, smem, s)
-            PFB_DISPATCH_DW(p->g.ndim, w4, PFB_S4, PFB_S8)
+            PFB_DISPATCH_DW(p->g.ndim, wmv, PFB_S1, PFB_S4, PFB_S8)
+#undef PFB_S1
 #undef PFB_S4
 #undef PFB_S8
         }
@@ -1491,11 +1499,13 @@ int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const flo
     Q.tB = d.b0_time;
     Q.grad = grad;
     Q.accumulate = accumulate ? 1 : 0;
-    bool w4 = wmax_of(p->g) <= 4;
+    const int wmv = wm_of(p->g);
     int blocks = sample_blocks(p->mtot);
+#define PFB_T1(DD) launch_traj_il_t<DD, 1>(Q, blocks, s)
 #define PFB_T4(DD) launch_traj_il_t<DD, 4>(Q, blocks, s)
 #define PFB_T8(DD) launch_traj_il_t<DD, 8>(Q, blocks, s)
-    PFB_DISPATCH_DW(p->g.ndim, w4, PFB_T4, PFB_T8)
+    PFB_DISPATCH_DW(p->g.ndim, wmv, PFB_T1, PFB_T4, PFB_T8)
+#undef PFB_T1
 #undef PFB_T4
 #undef PFB_T8
 }
@@ -1598,6 +1608,9 @@ int build_plan_taps(pfb_plan *p, cudaStream_t s) {
     float *w = p->d_wtap;
     int *x = p->d_xtap;
     switch (D * 10 + WM) {
+        case 11: taps_prep_kernel<1, 1><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
+        case 21: taps_prep_kernel<2, 1><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
+        case 31: taps_prep_kernel<3, 1><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
         case 14: taps_prep_kernel<1, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
         case 18: taps_prep_kernel<1, 8><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;
         case 24: taps_prep_kernel<2, 4><<<tb, 256, 0, s>>>(p->g, p->d_cos[0], p->d_cos[1], p->d_cos[2], p->mtot, w, x); break;

@@ -7,8 +7,8 @@ trajectories: started from ones + 1e-6 noise, the oracle itself drifts from its
 unperturbed run by O(1) (rel-L2) within about 15 iterations, as the smallest
 weights fall towards zero.  So full runs are compared only over iterations where
 that drift stays far below the tolerance, and the 30-iteration loop is checked
-step by step: every GPU iterate, pushed through one oracle iteration, must give
-the GPU's next iterate.
+step by step: for GPU iterates w_k, w_{k+1}, the magnitude w_k / w_{k+1} the GPU
+divided by must be the oracle's |A A^H w_k|.
 """
 
 import ctypes
@@ -48,9 +48,17 @@ def _gpu_iterate(plan, w, niter):
     return w
 
 
-def _oracle_step(plan, w):
+def _oracle_ghg(plan, w):
+    """|A A^H w| of the reference's map (the well-conditioned, linear part of a step)."""
     ghg = orc.nufft_fwd(orc.nufft_adj(w.astype(np.complex64), plan, norm="ortho"), plan, norm="ortho")
-    return (w / np.abs(ghg)).astype(np.float32)
+    return np.abs(ghg).astype(np.float64)
+
+
+def _step_error(oplan, wk, wnext):
+    """One GPU step w_k -> w_{k+1} against the reference's map: the GPU's implied
+    |A A^H w_k| = w_k / w_{k+1} vs the oracle's (comparing the weights themselves
+    would divide by near-zero |A A^H w| at late, chaotic iterates)."""
+    return rel(wk.astype(np.float64) / wnext.astype(np.float64), _oracle_ghg(oplan, wk))
 
 
 def test_dcf_2d_radial_default_kernel_first_iterations():
@@ -75,9 +83,7 @@ def test_dcf_30_iterations_step_by_step():
         _gpu_iterate(gplan, w, k - done)
         wk = w.cpu().numpy().reshape(coord.shape[:-1])
         nxt = _gpu_iterate(gplan, w.clone(), 1).cpu().numpy().reshape(coord.shape[:-1])
-        # late iterates hold weights near zero whose |A A^H w| is tiny, where one
-        # step amplifies float32 differences; 1e-4 still separates a wrong map
-        assert rel(nxt, _oracle_step(oplan, wk)) < (TOL if k < 20 else TOL_RUN), k
+        assert _step_error(oplan, wk, nxt) < TOL, k
         done = k
 
 
@@ -105,7 +111,7 @@ def test_dcf_multiframe_and_zero_iterations():
     oplan = orc.plan_nufft(coord, (N, N), width=6, oversamp=1.5)
     w3 = _gpu_iterate(gplan, torch.ones(coord.shape[:-1], dtype=torch.float32, device="cuda:0").reshape(-1), 3)
     w4 = _gpu_iterate(gplan, w3.clone(), 1)
-    assert rel(w4.cpu().numpy().reshape(coord.shape[:-1]),
-               _oracle_step(oplan, w3.cpu().numpy().reshape(coord.shape[:-1]))) < TOL_RUN
+    assert _step_error(oplan, w3.cpu().numpy().reshape(coord.shape[:-1]),
+                       w4.cpu().numpy().reshape(coord.shape[:-1])) < TOL
     w0 = pf().pipe_menon_dcf(torch.as_tensor(coord), N, niter=0)
     assert torch.equal(w0, torch.ones_like(w0))
