@@ -266,9 +266,10 @@ int pfb_dcf_workspace_size(pfb_plan *plan, size_t *bytes);
 int pfb_pipe_menon_dcf(pfb_plan *plan, float *weights, int niter, void *workspace, size_t workspace_bytes,
                        void *stream);
 
-/* ---- Toeplitz Gram (src/pyfourier/_sparsegram) ------------------------------------ */
+/* ---- Toeplitz and Cartesian Gram (src/pyfourier/_sparsegram, src/pyfourier/_gram) -- */
 
-/* Create a Gram operator from its Toeplitz kernel on the 2x grid.
+/* Create a Gram operator from its Toeplitz kernel on the 2x grid, or from the
+ * Cartesian sampling mask on the image grid (os_shape == shape: the dense Gram).
  *   ndim, shape (z, y, x): image extent N; os_shape (z, y, x): embedding grid;
  *   ncoeff  K (low rank) or number of kernel planes (elementwise);
  *   lowrank 1: kernel is (prod(os_shape), K, K) with out[v] = T[v] @ in[v];
@@ -276,7 +277,8 @@ int pfb_pipe_menon_dcf(pfb_plan *plan, float *weights, int niter, void *workspac
  *   nseg    B0 time segments L (1 without field map): the kernel then holds
  *           L such kernels, one per segment;
  *   kernel  device complex64, uncentred (ifftshift-ed) layout, copied.
- * Replaces GramMatrix (src/pyfourier/_sparsegram/_plan.py:253-270). */
+ * Replaces GramMatrix (src/pyfourier/_sparsegram/_plan.py:253-270,
+ * src/pyfourier/_gram/_plan.py:160-177). */
 int pfb_gram_create(int ndim, const int *shape, const int *os_shape, int ncoeff, int lowrank,
                     int nseg, const void *kernel, int device, void *stream, pfb_gram **out);
 int pfb_gram_destroy(pfb_gram *gram);
@@ -285,9 +287,12 @@ int pfb_gram_workspace_size(pfb_gram *gram, int64_t batch, size_t *bytes);
 /* Apply: image (batch, ncoeff, *shape) -> out (same).  Zero-pad into the 2x grid,
  * FFT, per-voxel K x K mix (or elementwise product), inverse FFT, crop.  With
  * B0 segments, out = sum_l conj(C_l) G_l(C_l x) with b0_space = C (L, prod(shape)),
- * complex64 (NULL without segments).
+ * complex64 (NULL without segments).  When os_shape == shape and nseg == 1 there is
+ * no embedding: FFT image -> out, mix in out, inverse FFT in out; the workspace
+ * then only holds the cuFFT work area.
  * Replaces _sparsegram / _do_sparsegram / _bdot
- * (src/pyfourier/_sparsegram/_sparsegram.py:11-81, _bmatvec/_bdot.py:16-115). */
+ * (src/pyfourier/_sparsegram/_sparsegram.py:11-81, _bmatvec/_bdot.py:16-115) and
+ * _gram / _do_gram (src/pyfourier/_gram/_gram.py:11-133). */
 int pfb_gram_apply(pfb_gram *gram, const void *image, void *out, int64_t batch, const void *b0_space,
                    void *workspace, size_t workspace_bytes, void *stream);
 

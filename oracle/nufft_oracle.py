@@ -613,6 +613,66 @@ def _sparse_gram1(image, gram, norm=None):
 
 
 # --------------------------------------------------------------------------------------
+# Cartesian (dense) Gram
+# --------------------------------------------------------------------------------------
+def plan_gram(mask, shape, basis=None, zmap=None, T=None, L=6, nbins=(40, 40)):
+    """_gram/_plan.py:19-157 with its intent fixes.
+
+    The kernel is the sampling mask (centred, DC at N // 2) moved to FFT order
+    with ``ifftshift`` (both branches; the shipped code shifts only the low-rank
+    kernel, with ``fftshift``, :133-135).  With a basis (:122-135) the per-voxel
+    matrix is value[v][k2][k1] = sum_t mask_t(v) B[t, k1] conj(B[t, k2]).  A 1D
+    mask (ny,) is (1, ny, 1) and a 2D one has one frame (:90-94); mask planes
+    broadcast to ``shape``.  With a field map (:114-125, :138-145) the spatial
+    coefficients are not folded into the k-space kernel: segment l weights mask
+    point p by B_l(T[p]) (``mri_exp_approx(..., acorr=True)`` over the distinct
+    sampling times) and the apply is sum_l conj(C_l) G_l(C_l x), as for the
+    Toeplitz Gram.
+    """
+    shape = tuple(int(s) for s in shape)
+    assert len(shape) == 2, "dense Gram FFT is 2D (or separable 3D) only (_plan.py:86-88)"
+    m = np.asarray(mask, np.float64)
+    if m.ndim == 1:
+        m = m[None, :, None]
+    elif m.ndim == 2:
+        m = m[None]
+    m = np.broadcast_to(m, (m.shape[0], *shape))
+    nt = m.shape[0]
+    m = np.fft.ifftshift(m, axes=(-2, -1))
+    Cl = None
+    if zmap is not None:
+        t = np.fft.ifftshift(np.broadcast_to(np.asarray(T, np.float32), m.shape), axes=(-2, -1))
+        tu, inv = np.unique(t.astype(np.float64).ravel(), return_inverse=True)
+        Bt, Cl = mri_exp_approx(zmap, tu, L, nbins, acorr=True)
+        wl = Bt[:, inv].reshape(L, *m.shape)
+        Cl = Cl.astype(np.complex64)
+    else:
+        wl = np.ones((1, *m.shape))
+    mw = wl * m[None]  # (L, nt, ny, nx)
+    nvox = int(np.prod(shape))
+    if basis is not None:
+        B = np.asarray(basis, np.complex128)
+        assert B.shape[0] == nt
+        K = B.shape[1]
+        val = np.zeros((mw.shape[0], nvox, K, K), np.complex128)
+        for t_ in range(nt):
+            outer = np.conj(B[t_])[:, None] * B[t_][None, :]  # [k2, k1]
+            val += mw[:, t_].reshape(mw.shape[0], nvox, 1, 1) * outer
+    else:
+        val = mw
+    if zmap is None:
+        val = val[0]
+    return OracleGram(val.astype(np.complex64), shape, 2, basis is not None, Cl)
+
+
+def gram(image, gram_matrix, norm=None):
+    """_gram/_gram.py:11-133: uncentred FFT, per-voxel product with the kernel,
+    uncentred inverse FFT (no embedding: the grid is the image); with a field map
+    sum_l conj(C_l) G_l(C_l x)."""
+    return sparse_gram(image, gram_matrix, norm)
+
+
+# --------------------------------------------------------------------------------------
 # Sparse (Cartesian-subsampled) FFT
 # --------------------------------------------------------------------------------------
 def _sparse_index(indexes, shape):

@@ -78,6 +78,17 @@ int run_fft(cufftHandle h, size_t wbytes, float2 *data, int direction, void *wor
     return PFB_OK;
 }
 
+int run_fft_to(cufftHandle h, size_t wbytes, const float2 *src, float2 *dst, int direction, void *work,
+               size_t work_avail, cudaStream_t s) {
+    if (wbytes > work_avail) return fail(PFB_ERR_WORKSPACE, "workspace too small for the cuFFT work area");
+    PFB_CUFFT_TRY(cufftSetStream(h, s));
+    PFB_CUFFT_TRY(cufftSetWorkArea(h, work));
+    // a C2C transform leaves an out-of-place input unchanged
+    PFB_CUFFT_TRY(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(const_cast<float2 *>(src)),
+                               reinterpret_cast<cufftComplex *>(dst), direction < 0 ? CUFFT_FORWARD : CUFFT_INVERSE));
+    return PFB_OK;
+}
+
 namespace {
 
 int to_desc(const pfb_plan *p, const pfb_apply_t *o, ApplyDesc &d) {
@@ -399,6 +410,20 @@ int pfb_traj_grad(pfb_plan *p, const pfb_apply_t *opt, const void *grid, const v
                             fft_layout != 0, static_cast<cudaStream_t>(stream), opt->flags & PFB_FLAG_ACCUMULATE);
 }
 
+}  // extern "C"
+
+namespace {
+// image grid == FFT grid and no B0 segments: the Gram needs no embedding
+bool gram_is_dense(const pfb_gram *g) {
+    if (g->nseg != 1) return false;
+    for (int a = 0; a < g->ndim; ++a)
+        if (g->n[a] != g->nos[a]) return false;
+    return true;
+}
+}  // namespace
+
+extern "C" {
+
 int pfb_gram_create(int ndim, const int *shape, const int *os_shape, int ncoeff, int lowrank, int nseg,
                     const void *kernel, int device, void *stream, pfb_gram **out) {
     if (!out) return fail(PFB_ERR_INVALID, "out is NULL");
@@ -462,7 +487,9 @@ int pfb_gram_workspace_size(pfb_gram *g, int64_t batch, size_t *bytes) {
     size_t wb = 0;
     int st = get_fft_plan(g->fft_mu, g->fft_plans, g->fft_work, g->ndim, g->nos, P, &h, &wb);
     if (st) return st;
-    *bytes = align_up((size_t)P * g->gvol * sizeof(float2)) + align_up(wb);
+    // a dense Gram transforms in the output array: only the cuFFT work area
+    *bytes = gram_is_dense(g) ? std::max<size_t>(align_up(wb), 256)
+                              : align_up((size_t)P * g->gvol * sizeof(float2)) + align_up(wb);
     return PFB_OK;
 }
 
@@ -481,6 +508,18 @@ int pfb_gram_apply(pfb_gram *g, const void *image, void *out, int64_t batch, con
     size_t wb = 0;
     int st = get_fft_plan(g->fft_mu, g->fft_plans, g->fft_work, g->ndim, g->nos, P, &h, &wb);
     if (st) return st;
+    if (gram_is_dense(g)) {
+        // grid == image, one segment: FFT image -> out, mix in place with the 1/G
+        // of the two transforms folded in, inverse FFT in place (3 passes, no
+        // embed / extract copies)
+        if (workspace_bytes < wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
+        float2 *o = static_cast<float2 *>(out);
+        if ((st = run_fft_to(h, wb, static_cast<const float2 *>(image), o, -1, workspace, workspace_bytes, s)))
+            return st;
+        if ((st = launch_mix(g->gvol, g->K, g->lowrank, batch, g->d_T, o, s, (float)(1.0 / (double)g->gvol))))
+            return st;
+        return run_fft(h, wb, o, +1, workspace, workspace_bytes, s);
+    }
     size_t gbytes = align_up((size_t)P * g->gvol * sizeof(float2));
     if (workspace_bytes < gbytes + wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
     float2 *grid = static_cast<float2 *>(workspace);

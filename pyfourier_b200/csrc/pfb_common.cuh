@@ -319,7 +319,7 @@ int launch_embed(int ndim, const int *n, const int *nos, const float2 *img, floa
 int launch_extract(int ndim, const int *n, const int *nos, const float2 *grid, float2 *img,
                    int64_t nplanes, float factor, const float2 *Cl, int L, cudaStream_t s);
 int launch_mix(int64_t gvol, int K, int lowrank, int64_t batch, const float2 *T, float2 *grid,
-               cudaStream_t s);
+               cudaStream_t s, float scale = 1.f);
 
 // plan.cu
 int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_offsets,
@@ -335,6 +335,9 @@ int get_fft_plan(std::mutex &mu, std::map<int64_t, cufftHandle> &plans, std::map
                  int ndim, const int *nos_xyz, int64_t nplanes, cufftHandle *out, size_t *wbytes);
 int run_fft(cufftHandle h, size_t wbytes, float2 *data, int direction, void *work, size_t work_avail,
             cudaStream_t s);
+// Out-of-place C2C transform src -> dst (src is read only; dst may equal src).
+int run_fft_to(cufftHandle h, size_t wbytes, const float2 *src, float2 *dst, int direction, void *work,
+               size_t work_avail, cudaStream_t s);
 
 // fast.cu (channel-interleaved pipeline)
 int fast_supported(const pfb_plan *p, const ApplyDesc &d, std::string *why);

@@ -157,22 +157,27 @@ __global__ void extract_kernel(const EmbedParams P) {
     }
 }
 
-// Per-voxel K x K mix, out[v] = T[v] @ in[v] (T row-major per voxel), for every
-// batch item; the K-vector of a voxel lives in K planes of the grid.  The
-// evident intent of _bmatvec/_bdot.py:16-115 (the shipped _dot_nb computes
-// in * colsum(T), not the product).
+// Per-voxel K x K mix, out[v] = scale * T[v] @ in[v] (T row-major per voxel),
+// for every batch item; the K-vector of a voxel lives in K planes of the grid.
+// The evident intent of _bmatvec/_bdot.py:16-115 (the shipped _dot_nb computes
+// in * colsum(T), not the product).  blockIdx.y strides over batch items, so
+// small grids still fill the GPU; T (K*K per voxel) is re-read per y-slice and
+// stays in L2.
 template <int KM>
 __global__ void __launch_bounds__(256) mix_kernel(int64_t gvol, int K, int64_t batch,
-                                                  const float2 *__restrict__ T, float2 *__restrict__ grid) {
+                                                  const float2 *__restrict__ T, float2 *__restrict__ grid,
+                                                  float scale) {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < gvol; v += stride) {
         float2 t[KM][KM];
 #pragma unroll
         for (int i = 0; i < KM; ++i)
 #pragma unroll
-            for (int j = 0; j < KM; ++j)
-                t[i][j] = (i < K && j < K) ? __ldg(T + (v * K + i) * K + j) : make_float2(0.f, 0.f);
-        for (int64_t b = 0; b < batch; ++b) {
+            for (int j = 0; j < KM; ++j) {
+                float2 e = (i < K && j < K) ? __ldg(T + (v * K + i) * K + j) : make_float2(0.f, 0.f);
+                t[i][j] = make_float2(e.x * scale, e.y * scale);
+            }
+        for (int64_t b = blockIdx.y; b < batch; b += gridDim.y) {
             float2 x[KM];
 #pragma unroll
             for (int j = 0; j < KM; ++j)
@@ -193,14 +198,15 @@ __global__ void __launch_bounds__(256) mix_kernel(int64_t gvol, int K, int64_t b
     }
 }
 
-// Elementwise Toeplitz multiply (no subspace): plane (b, c) *= T[c] (T has C planes).
+// Elementwise multiply (no subspace): plane (b, c) *= scale * T[c] (T has C planes).
 __global__ void diag_kernel(int64_t gvol, int C, int64_t batch, const float2 *__restrict__ T,
-                            float2 *__restrict__ grid) {
+                            float2 *__restrict__ grid, float scale) {
     const int64_t total = batch * C * gvol;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
         int64_t cv = e % (C * gvol);
-        grid[e] = cmul(__ldg(T + cv), grid[e]);
+        float2 r = cmul(__ldg(T + cv), grid[e]);
+        grid[e] = make_float2(r.x * scale, r.y * scale);
     }
 }
 
@@ -304,19 +310,25 @@ int launch_extract(int ndim, const int *n, const int *nos, const float2 *grid, f
 }
 
 int launch_mix(int64_t gvol, int K, int lowrank, int64_t batch, const float2 *T, float2 *grid,
-               cudaStream_t s) {
+               cudaStream_t s, float scale) {
     if (gvol == 0 || batch == 0) return PFB_OK;
     if (!lowrank) {
-        diag_kernel<<<blocks_for(batch * K * gvol, 256), 256, 0, s>>>(gvol, K, batch, T, grid);
-    } else if (K <= 2) {
-        mix_kernel<2><<<blocks_for(gvol, 256), 256, 0, s>>>(gvol, K, batch, T, grid);
-    } else if (K <= 4) {
-        mix_kernel<4><<<blocks_for(gvol, 256), 256, 0, s>>>(gvol, K, batch, T, grid);
-    } else if (K <= 8) {
-        mix_kernel<8><<<blocks_for(gvol, 128), 128, 0, s>>>(gvol, K, batch, T, grid);
-    } else {
-        return fail(PFB_ERR_UNSUPPORTED, "subspace size K > 8 is not supported by the Gram mix");
+        diag_kernel<<<blocks_for(batch * K * gvol, 256), 256, 0, s>>>(gvol, K, batch, T, grid, scale);
+        PFB_CHECK_LAUNCH();
+        return PFB_OK;
     }
+    if (K > 8) return fail(PFB_ERR_UNSUPPORTED, "subspace size K > 8 is not supported by the Gram mix");
+    const int threads = K <= 4 ? 256 : 128;
+    const int bx = blocks_for(gvol, threads);
+    // batch slices so that about 8 blocks per SM run (148 SMs)
+    const int by = (int)std::max<int64_t>(1, std::min<int64_t>(batch, (148LL * 8 + bx - 1) / bx));
+    dim3 grd(bx, by);
+    if (K <= 2)
+        mix_kernel<2><<<grd, threads, 0, s>>>(gvol, K, batch, T, grid, scale);
+    else if (K <= 4)
+        mix_kernel<4><<<grd, threads, 0, s>>>(gvol, K, batch, T, grid, scale);
+    else
+        mix_kernel<8><<<grd, threads, 0, s>>>(gvol, K, batch, T, grid, scale);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
 }

@@ -92,3 +92,36 @@ def test_b0_basis_fp64_matches_oracle():
     b2, c2 = orc.mri_exp_approx(zmap, t, 6, 40)
     np.testing.assert_allclose(b1, b2, rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(c1, c2, rtol=1e-12)
+
+
+@pytest.mark.parametrize("kind", ["planes", "basis", "field_map", "line_mask"])
+def test_dense_gram_kernel_matches_oracle(kind):
+    """The Cartesian Gram kernel built on the host (torch on CPU) equals the
+    oracle's restatement of src/pyfourier/_gram/_plan.py."""
+    import torch
+
+    from oracle import nufft_oracle as orc
+    from pyfourier_b200._cgram import _dense_kernel
+
+    rng = np.random.default_rng(1)
+    N = (16, 20)
+    m = (rng.random((4, *N)) < 0.3).astype(np.float32)
+    B = np.linalg.qr(rng.standard_normal((4, 3)) + 1j * rng.standard_normal((4, 3)))[0].astype(np.complex64)
+    kw = {}
+    if kind == "basis":
+        kw = dict(basis=B)
+    elif kind == "line_mask":
+        m, kw = m[0, :, 0], dict(basis=B[:1])  # (ny,) -> (1, ny, 1), broadcast along x
+    elif kind == "field_map":
+        yy, xx = np.mgrid[:N[0], :N[1]] / N[0] - 0.5
+        kw = dict(zmap=100 * np.exp(-((xx - 0.1) ** 2 + yy ** 2) / 0.05) - 50,
+                  T=1e-4 * np.broadcast_to(np.arange(N[1]), N), L=6)
+    o = orc.plan_gram(m, N, **kw)
+    v, zs, lowrank = _dense_kernel(torch.as_tensor(m), N, kw.get("basis"), kw.get("zmap"), kw.get("T"),
+                                   kw.get("L", 6), (40, 40))
+    assert lowrank == o.islowrank and tuple(v.shape) == o.value.shape
+    np.testing.assert_allclose(v.numpy(), o.value, rtol=0, atol=1e-6 * np.abs(o.value).max())
+    if kind == "field_map":
+        np.testing.assert_allclose(zs.numpy(), o.zmap_s_kernel, rtol=0, atol=1e-6)
+    else:
+        assert zs is None

@@ -217,3 +217,64 @@ def test_oracle_sparse_fft_is_the_width_one_nufft():
             a = orc.sparse_ifftn(y, idx, N, basis=b, norm=norm)
             r = orc.nufft_adj(y, plan, basis=b, norm=norm).reshape(a.shape)
             assert orc.rel_l2(a, r) < 1e-6
+
+
+def _line_masks(rng, F, N, nsel):
+    """Cartesian phase-encode masks: per frame ``nsel`` random ky lines, fully
+    sampled along x.  Returns the centred masks (F, ny, nx) and the sampled
+    grid indexes (F, nsel, nx, 2), axes (x, y)."""
+    ny, nx = N
+    lines = np.stack([np.sort(rng.choice(ny, nsel, replace=False)) for _ in range(F)])
+    mask = np.zeros((F, ny, nx), np.float32)
+    for f in range(F):
+        mask[f, lines[f]] = 1
+    xx = np.broadcast_to(np.arange(nx), (F, nsel, nx))
+    yy = np.broadcast_to(lines[:, :, None], (F, nsel, nx))
+    return mask, np.stack([xx, yy], -1).astype(np.float32)
+
+
+def test_oracle_cartesian_gram_is_the_sparse_fft_normal_operator():
+    """Dense Gram restatement == sparse_ifftn(sparse_fftn(x)) on the mask's points,
+    per frame and with a subspace basis, for both norms."""
+    rng = np.random.default_rng(12)
+    N, F, K = (16, 20), 4, 2
+    mask, idx = _line_masks(rng, F, N, 6)
+    basis = np.linalg.qr(rng.standard_normal((F, K)) + 1j * rng.standard_normal((F, K)))[0].astype(np.complex64)
+    for b in (None, basis):
+        C = K if b is not None else F
+        gm = orc.plan_gram(mask, N, basis=b)
+        x = (rng.standard_normal((2, C, *N)) + 1j * rng.standard_normal((2, C, *N))).astype(np.complex64)
+        for norm in (None, "ortho"):
+            ref = orc.sparse_ifftn(orc.sparse_fftn(x, idx, N, basis=b, norm=norm), idx, N, basis=b, norm=norm)
+            assert orc.rel_l2(orc.gram(x, gm, norm=norm), ref.reshape(x.shape)) < 1e-5
+    # one 2D mask (no frame axis) and a (ny,) line mask broadcast along x
+    gm1 = orc.plan_gram(mask[0], N)
+    x1 = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    ref1 = orc.sparse_ifftn(orc.sparse_fftn(x1, idx[0], N), idx[0], N).reshape(N)
+    assert orc.rel_l2(orc.gram(x1, gm1), ref1) < 1e-5
+    gml = orc.plan_gram(mask[0, :, 0], N, basis=basis[:1])
+    assert gml.value.shape == (N[0] * N[1], K, K)
+
+
+def test_oracle_cartesian_gram_with_field_map_vs_exact():
+    """Dense Gram with B0 segments approximates E^H M E / (ny nx) of the exact
+    off-resonance model (A^H A for the orthonormal sparse FFT), T the sampling
+    time of every mask point (readout along x)."""
+    rng = np.random.default_rng(13)
+    N = (24, 24)
+    mask, idx = _line_masks(rng, 1, N, 10)
+    yy, xx = np.mgrid[:N[0], :N[1]] / N[0] - 0.5
+    b0 = 100 * np.exp(-((xx - 0.1) ** 2 + yy ** 2) / 0.05) - 50
+    dt = 5e-3 / N[1]
+    T = dt * np.broadcast_to(np.arange(N[1]), N)
+    gm = orc.plan_gram(mask, N, zmap=b0, T=T, L=8, nbins=40)
+    assert gm.value.shape == (8, 1, *N) and gm.zmap_s_kernel.shape == (8, *N)
+    x = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    g = orc.gram(x, gm)
+    r = orc.pixel_grid(N)
+    pts = idx.reshape(-1, 2).astype(np.float64)
+    cm = pts - np.array([N[1] // 2, N[0] // 2])
+    tm = dt * pts[:, 0]
+    E = np.exp(-2j * np.pi * (cm / np.array(N[::-1])) @ r.T) * np.exp(-2j * np.pi * tm[:, None] * b0.ravel()[None, :])
+    ref = (E.conj().T @ (E @ x.ravel().astype(np.complex128))).reshape(N) / np.prod(N)
+    assert orc.rel_l2(g, ref) < 2e-2
