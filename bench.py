@@ -448,7 +448,7 @@ def time_device(torch, fn, steps, warmup):
 
 def extra_workload(args):
     """2D radial (cfg1), Toeplitz Gram (cfg3), B0 plain vs batched (cfg4), autograd (cfg5), Pipe-Menon DCF (dcf),
-    sparse FFT (spfft), Cartesian Gram (cgram)."""
+    sparse FFT (spfft), Cartesian Gram (cgram), GROG pre-interpolation (grog)."""
     import torch
 
     import pyfourier_b200 as pf
@@ -626,6 +626,49 @@ def extra_workload(args):
                     cpu_baseline={"value": 1.0 / cpu_s, "unit": "applies/s", "cores": orc.lib().orc_num_threads(),
                                   "kind": "port", "sample": "8 of 256 readout slices (NumPy einsum + pocketfft), "
                                                             "scaled to the full apply"})
+    elif args.workload == "grog":
+        # GROG of a 3D golden-means radial acquisition, 128^3 grid, 8000 spokes x 256 samples, 32 coils,
+        # operators trained on a 24^3 calibration region (11^3 = 1331 operators)
+        N, nsp, nrd, nc, ncal = 128, 8000, 256, 32, 24
+        coord = golden_means_radial_3d(nsp, nrd, N)
+        g = torch.Generator(device="cpu").manual_seed(0)
+        cal = torch.complex(torch.randn(nc, ncal, ncal, ncal, generator=g),
+                            torch.randn(nc, ncal, ncal, ncal, generator=g)).to(dev)
+        t0 = time.perf_counter()
+        plan = pf.GrogPlan(cal, torch.as_tensor(coord, device=dev), (N, N, N), device=dev)
+        torch.cuda.synchronize()
+        plan_s = time.perf_counter() - t0
+        M = nsp * nrd
+        x = torch.complex(torch.randn(1, nc, M, generator=g), torch.randn(1, nc, M, generator=g)).to(dev)
+        step = lambda: plan.apply(x)  # noqa: E731
+        clocks.start()
+        ms = time_device(torch, step, args.steps, args.warmup)
+        clk = clocks.stop()
+        # algorithmic: the coil vectors read once and written once; 8 flops per complex MAC
+        alg = 2 * M * nc * 8
+        flops = 8.0 * M * nc * nc
+        # CPU: the oracle on 250 of the 8000 spokes (all coils), scaled to samples/s
+        ns = 250 * nrd
+        xs = x[:, :, :ns].cpu().numpy().reshape(1, nc, 250, nrd)
+        cs = coord[:250]
+        calc = cal.cpu().numpy()
+        orc.grog_interp(xs[:, :, :10], calc, cs[:10], N)
+        t1 = time.perf_counter()
+        orc.grog_interp(xs, calc, cs, N)
+        cpu_s = time.perf_counter() - t1
+        line.update(metric="GROG pre-interpolated samples/s (3D radial, 128^3, 32 coils, 1331 operators)",
+                    value=nc * M / (ms / 1e3), unit="samples/s", ms_per_step=ms,
+                    config={"workload": "GROG apply: every sample's 32-coil vector times its 32 x 32 operator",
+                            "image": [N, N, N], "spokes": nsp, "readout": nrd, "coils": nc,
+                            "calibration": [ncal] * 3, "operators": plan.ntable, "plan_seconds": round(plan_s, 3),
+                            "algorithmic_bytes": alg, "hbm_gbs_algorithmic": round(alg / (ms / 1e3) / 1e9, 1),
+                            "three_pass_gbs": round(3 * alg / (ms / 1e3) / 1e9, 1),
+                            "tflops_fp32": round(flops / (ms / 1e3) / 1e12, 2),
+                            "l2": "inputs larger than L2 (524 MB of coil vectors)"},
+                    cpu_baseline={"value": nc * ns / cpu_s, "unit": "samples/s",
+                                  "cores": orc.lib().orc_num_threads(), "kind": "port",
+                                  "sample": "250 of 8000 spokes, all coils (NumPy einsum with the operator table), "
+                                            "plan included"})
     elif args.workload == "dcf":
         # Pipe-Menon density compensation with the reference's defaults (W 6, osf 1.5, 30 iterations)
         N, nsp, nrd, niter = 128, 8000, 256, 30
@@ -697,13 +740,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg1", "cfg3", "cfg4", "cfg5", "dcf", "spfft",
-                                                                      "cgram"])
+                                                                      "cgram", "grog"])
     ap.add_argument("--cpu-coils", type=int, default=2, help="coils in the bounded CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-launch-trace", action="store_true",
                     help="skip the CUDA activity trace that counts launches (for runs under ncu)")
     args = ap.parse_args()
-    if args.workload in ("cfg1", "cfg3", "cfg4", "cfg5", "dcf", "spfft", "cgram"):
+    if args.workload in ("cfg1", "cfg3", "cfg4", "cfg5", "dcf", "spfft", "cgram", "grog"):
         extra_workload(args)
         return
     wl = WORKLOADS[args.workload]

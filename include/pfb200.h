@@ -45,6 +45,7 @@ extern "C" {
 
 typedef struct pfb_plan pfb_plan;
 typedef struct pfb_gram pfb_gram;
+typedef struct pfb_grog pfb_grog;
 
 /* Options of an operator apply.
  *   batch    B: product of the leading batch axes (coils, slices, ...);
@@ -295,6 +296,33 @@ int pfb_gram_workspace_size(pfb_gram *gram, int64_t batch, size_t *bytes);
  * _gram / _do_gram (src/pyfourier/_gram/_gram.py:11-133). */
 int pfb_gram_apply(pfb_gram *gram, const void *image, void *out, int64_t batch, const void *b0_space,
                    void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- GROG pre-interpolation (src/pyfourier/_preinterp/_grog.py) ------------------ */
+
+/* Create a GROG operator set for one trajectory.
+ *   lut      device int32 (nsamples): operator index of each sample in [0, ntable),
+ *            -1 for samples outside the grid (their output is zero);
+ *   ntable   operators per set (nsteps^ndim);
+ *   ncoils   nc, 1 .. 64;
+ *   nslices  operator sets: 2D GROG trains one set per calibration slice and applies
+ *            set b to batch item b; 1 otherwise;
+ *   table    device complex64 (ntable, nslices, nc, nc), [i][j] maps source coil i to
+ *            target coil j; copied.
+ * Sorts the samples by operator (once).  Replaces the operator lookup of
+ * src/pyfourier/_preinterp/_grog.py:172-185 and the kernel launch of :399-439. */
+int pfb_grog_create(const int *lut, int64_t nsamples, int ntable, int ncoils, int nslices, const void *table,
+                    int device, void *stream, pfb_grog **out);
+int pfb_grog_destroy(pfb_grog *grog);
+/* Workspace of an apply: batch x (samples inside the grid) x nc complex64. */
+int pfb_grog_workspace_size(pfb_grog *grog, int64_t batch, size_t *bytes);
+
+/* Apply: in (batch, nc, nsamples) complex64 -> out (same), out[b, :, m] =
+ * in[b, :, m] @ table[lut[m], slice b]; zeros where lut[m] == -1.  in and out must not
+ * overlap.  Replaces _interp / do_interpolation (src/pyfourier/_preinterp/_grog.py:399-439;
+ * the shipped per-sample product computes in * colsum(G), the evident intent is
+ * in @ G). */
+int pfb_grog_apply(pfb_grog *grog, const void *in, void *out, int64_t batch, void *workspace,
+                   size_t workspace_bytes, void *stream);
 
 #ifdef __cplusplus
 }

@@ -744,6 +744,121 @@ def pipe_menon_dcf(coord, shape, niter=30, width=6, oversamp=1.5):
 
 
 # --------------------------------------------------------------------------------------
+# GROG pre-interpolation
+# --------------------------------------------------------------------------------------
+def grog_operators(calib, ndim, lamda=0.01):
+    """_preinterp/_grog.py:253-356 (``_calc_grappaop``, ``_grappa_op_2d/3d``) in complex128.
+
+    Per axis the GRAPPA operator G solving (S^H S + l0 I) G = S^H T, with source rows S
+    the calibration coil vectors and targets T their neighbours one step further along
+    the axis, l0 = lamda * ||S||_F / nc.  2D: one operator per calibration slice,
+    (nz, nc, nc); 3D: (nc, nc).  Returned in (x, y[, z]) order.  (The shipped helpers
+    take their array backend from the builtin ``input``, :288, :326, :359; the
+    calibration array's is the evident intent.)
+    """
+    c = np.asarray(calib, np.complex128)
+    if c.ndim == 3:
+        c = c[:, None]
+    c = np.moveaxis(c, 0, -1)  # (nz, ny, nx, nc)
+    nc = c.shape[-1]
+
+    def train(S, T):
+        Sh = np.conj(np.swapaxes(S, -1, -2))
+        l0 = lamda * np.linalg.norm(Sh, axis=(-2, -1)) / nc
+        A = Sh @ S + l0[..., None, None] * np.eye(nc)
+        return np.linalg.solve(A, Sh @ T)
+
+    nz = c.shape[0]
+    if ndim == 2:
+        gy = train(c[:, :-1].reshape(nz, -1, nc), c[:, 1:].reshape(nz, -1, nc))
+        gx = train(c[:, :, :-1].reshape(nz, -1, nc), c[:, :, 1:].reshape(nz, -1, nc))
+        return [gx, gy]
+    gz = train(c[:-1].reshape(-1, nc), c[1:].reshape(-1, nc))
+    gy = train(c[:, :-1].reshape(-1, nc), c[:, 1:].reshape(-1, nc))
+    gx = train(c[:, :, :-1].reshape(-1, nc), c[:, :, 1:].reshape(-1, nc))
+    return [gx, gy, gz]
+
+
+def _fractional_powers(A, deltas):
+    """_grog.py:369-396 (``_weight_grid``): A^d = V diag(L^d) V^-1, principal branch."""
+    L, V = np.linalg.eig(A)
+    Vi = np.linalg.inv(V)
+    return np.stack([(V * (L ** d)[..., None, :]) @ Vi for d in deltas])  # (nsteps, ..., nc, nc)
+
+
+def grog_table(ops, nsteps=11):
+    """_grog.py:131-170: G[(iz n + iy) n + ix] = Gx^dx @ Gy^dy (@ Gz^dz), the steps
+    d = (i - (n - 1) / 2) / (n - 1).  2D: (n^2, nz, nc, nc); 3D: (n^3, nc, nc)."""
+    n = 2 * (nsteps // 2) + 1
+    deltas = (np.arange(n) - (n - 1) // 2) / (n - 1)
+    P = [_fractional_powers(o, deltas) for o in ops]
+    if len(ops) == 2:
+        G = P[0][None, :] @ P[1][:, None]  # [iy, ix] = Gx[ix] @ Gy[iy]
+        return G.reshape(n * n, *G.shape[2:])
+    G = (P[0][None, None, :] @ P[1][None, :, None]) @ P[2][:, None, None]
+    return G.reshape(n ** 3, *G.shape[3:])
+
+
+def grog_lut(coord, nsteps=11):
+    """_grog.py:172-182: indexes = round(coord) (float32, half to even); per axis the step
+    floor((n - 1) * (index - coord)) + n // 2, combined as sum_a step_a n^a over (x, y, z).
+    The shipped code scales by a literal 10, which is n - 1 for the default n = 11."""
+    n = 2 * (nsteps // 2) + 1
+    c = np.asarray(coord, np.float32)
+    idx = np.round(c)
+    d = idx - c
+    st = np.floor(d * np.float32(n - 1)).astype(np.int64) + n // 2
+    w = np.array([1, n, n * n], np.int64)[: c.shape[-1]]
+    return idx, (st.reshape(-1, c.shape[-1]) * w).sum(-1)
+
+
+def grog_interp(input, calib, coord, shape, lamda=0.01, nsteps=11):
+    """_preinterp/_grog.py:22-250 with its intent fixes: returns (output, indexes, weights).
+
+    input (..., nc, *coord.shape[:-1]); calib (nc, [nz,] ny, nx) (2D: one operator set per
+    calibration slice, the leading input axes being those slices) or (nc, nz, ny, nx) (3D).
+    Each sample's coil vector is moved to its nearest grid point by the GRAPPA operator of
+    its quantised offset, out = in @ G[lut] (the shipped ``_dot_product``, :406-412, adds
+    G[i][j] * in[j], i.e. in * colsum(G); the 3D branch treats the sample axis as a batch
+    axis, :205-207).  Indexes are round(coord) + N // 2; weights 1 / (occurrences of each
+    flattened index over all samples, before clipping); samples outside the grid are zeroed
+    and their indexes clipped (:224-236).
+    """
+    coord = np.asarray(coord, np.float32)
+    ndim = coord.shape[-1]
+    shape = [int(shape)] * ndim if np.isscalar(shape) else [int(s) for s in list(shape)[-ndim:]]
+    cal = np.asarray(calib)
+    cal = cal / np.linalg.norm(cal)
+    G = grog_table(grog_operators(cal, ndim, lamda), nsteps).astype(np.complex64)
+    idx, lut = grog_lut(coord, nsteps)
+    x = np.asarray(input, np.complex64)
+    M = int(np.prod(coord.shape[:-1]))
+    nc = cal.shape[0]
+    ishape = x.shape
+    rows = np.swapaxes(x.reshape(-1, nc, M), 1, 2)  # (B, M, nc)
+    out = np.empty_like(rows)
+    nsl = G.shape[1] if ndim == 2 else 1
+    if nsl > 1 and rows.shape[0] != nsl:
+        raise ValueError("2D GROG with per-slice operators needs one input slice per calibration slice")
+    for b in range(rows.shape[0]):
+        Gb = (G[:, b if nsl > 1 else 0] if ndim == 2 else G)[lut]
+        out[b] = np.einsum("mi,mij->mj", rows[b], Gb)
+    out = np.swapaxes(out, 1, 2).reshape(ishape)
+    n_xyz = shape[::-1]
+    ind = (idx + np.array([s // 2 for s in n_xyz], np.float32)).astype(np.int64)
+    unfold = np.array([1, n_xyz[0], n_xyz[0] * (n_xyz[1] if ndim > 1 else 1)], np.int64)[:ndim]
+    flat = (ind * unfold).sum(-1).ravel()
+    _, inv, counts = np.unique(flat, return_inverse=True, return_counts=True)
+    weights = (1.0 / counts[inv].astype(np.float32)).reshape(ind.shape[:-1]).astype(np.float32)
+    outside = np.zeros(ind.shape[:-1], bool)
+    for a in range(ndim):
+        outside |= (ind[..., a] < 0) | (ind[..., a] >= n_xyz[a])
+        ind[..., a] = np.clip(ind[..., a], 0, n_xyz[a] - 1)
+    out[..., outside] = 0
+    return out, ind, weights
+
+
+# --------------------------------------------------------------------------------------
 # FP64 references
 # --------------------------------------------------------------------------------------
 def pixel_grid(shape_zyx):

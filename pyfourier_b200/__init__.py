@@ -4,7 +4,8 @@ Drop-in entry points (same names, arguments and shape conventions as
 pyfourier): ``nufft``, ``nufft_adj``, ``plan_nufft`` / ``NUFFTPlan``,
 ``plan_spgram`` / ``sparse_gram`` / ``GramMatrix``, ``plan_spfft`` /
 ``sparse_fftn`` / ``sparse_ifftn``, ``plan_gram`` / ``gram`` (Cartesian
-Gram), ``pipe_menon_dcf`` (also
+Gram), ``grog_interp`` (GROG pre-interpolation, also as
+``_preinterp.grog_interp``), ``pipe_menon_dcf`` (also
 as ``pipemenon.pipe_menon_dcf``).  Everything computes in
 ``libpfb200.so`` through its C ABI (include/pfb200.h); there is no CPU
 fallback and importing an operator without the library raises.
@@ -17,6 +18,7 @@ from ._cgram import gram, plan_gram
 from ._dcf import pipe_menon_dcf
 from ._gram import GramMatrix, plan_spgram, sparse_gram
 from ._nufft import nufft, nufft_adj
+from ._preinterp import GrogPlan, grog_interp
 from ._plan import Interpolator, NUFFTPlan, plan_nufft
 from ._sparsefft import FFTPlan, plan_spfft, sparse_fftn, sparse_ifftn
 from . import pipemenon  # noqa: E402  (module path of the reference: pyfourier.pipemenon)
@@ -27,4 +29,5 @@ __all__ = [
     "nufft", "nufft_adj", "plan_nufft", "NUFFTPlan", "Interpolator",
     "plan_spgram", "sparse_gram", "GramMatrix", "mri_exp_approx", "autotune", "pipe_menon_dcf",
     "pipemenon", "plan_spfft", "sparse_fftn", "sparse_ifftn", "FFTPlan", "plan_gram", "gram",
+    "grog_interp", "GrogPlan",
 ]

@@ -32,6 +32,7 @@ EXPORTS = (
     "pfb_nufft_fwd", "pfb_nufft_adj", "pfb_spread", "pfb_interp", "pfb_deapod_pad",
     "pfb_crop_deapod", "pfb_grid_fft", "pfb_traj_grad", "pfb_gram_create", "pfb_gram_destroy",
     "pfb_gram_workspace_size", "pfb_gram_apply", "pfb_nufft_adj_noalloc",
+    "pfb_grog_create", "pfb_grog_destroy", "pfb_grog_workspace_size", "pfb_grog_apply",
     "pfb_apply_workspace_size", "pfb_nufft_traj_grad", "pfb_nufft_stage",
 )
 
@@ -115,6 +116,10 @@ def load(path=LIB_PATH):
         "pfb_gram_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),
         "pfb_gram_apply": (i32, [vp, vp, vp, i64, vp, vp, ctypes.c_size_t, vp]),
         "pfb_nufft_adj_noalloc": (i32, [vp, P(ApplyT), vp, vp, vp]),
+        "pfb_grog_create": (i32, [vp, i64, i32, i32, i32, vp, i32, vp, P(vp)]),
+        "pfb_grog_destroy": (i32, [vp]),
+        "pfb_grog_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),
+        "pfb_grog_apply": (i32, [vp, vp, vp, i64, vp, ctypes.c_size_t, vp]),
         "pfb_apply_workspace_size": (i32, [vp, P(ApplyT), P(ctypes.c_size_t)]),
         "pfb_nufft_traj_grad": (i32, [vp, P(ApplyT), vp, vp, vp, f32, vp, ctypes.c_size_t, vp]),
         "pfb_nufft_stage": (i32, [vp, P(ApplyT), i32, vp, vp, f32, vp, ctypes.c_size_t, vp]),

@@ -125,3 +125,36 @@ def test_dense_gram_kernel_matches_oracle(kind):
         np.testing.assert_allclose(zs.numpy(), o.zmap_s_kernel, rtol=0, atol=1e-6)
     else:
         assert zs is None
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_grog_tables_and_offsets_match_oracle(ndim):
+    """GROG host math (torch on CPU): operators, fractional-power table and offset
+    lookup equal the oracle's restatement of src/pyfourier/_preinterp/_grog.py."""
+    import torch
+
+    from oracle import nufft_oracle as orc
+    from pyfourier_b200 import _preinterp as P
+    from tests.test_oracle import shift_invariant_kspace
+
+    rng = np.random.default_rng(2)
+    _, cal = shift_invariant_kspace(rng, 5, ndim)
+    cal = cal + 0.05 * (rng.standard_normal(cal.shape) + 1j * rng.standard_normal(cal.shape))
+    if ndim == 2:
+        cal = np.stack([cal, 0.5 * cal[:, ::-1]], 1)  # two calibration slices
+    cal = cal / np.linalg.norm(cal)
+    ops_o = orc.grog_operators(cal, ndim, 0.01)
+    ops_p = P._operators(torch.as_tensor(cal), ndim, 0.01)
+    for a, b in zip(ops_p, ops_o):
+        np.testing.assert_allclose(a.numpy(), b, rtol=0, atol=1e-10 * np.abs(b).max())
+    t_o = orc.grog_table(ops_o, 11)
+    t_p = P._table(ops_p, 11).numpy()
+    assert t_p.shape == t_o.shape
+    np.testing.assert_allclose(t_p, t_o, rtol=0, atol=1e-9 * np.abs(t_o).max())
+    coord = ((rng.random((3, 50, ndim)) - 0.5) * 20).astype(np.float32)
+    coord[0, :4] = np.array([0.5, -0.5, 1.5, 2.5], np.float32)[:, None]  # ties round half to even
+    i_o, l_o = orc.grog_lut(coord, 11)
+    i_p, l_p = P._lut(torch.as_tensor(coord), 11)
+    np.testing.assert_array_equal(i_p.numpy(), i_o)
+    np.testing.assert_array_equal(l_p.numpy(), l_o)
+    assert l_o.min() >= 0 and l_o.max() < 11 ** ndim

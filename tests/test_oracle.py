@@ -278,3 +278,47 @@ def test_oracle_cartesian_gram_with_field_map_vs_exact():
     E = np.exp(-2j * np.pi * (cm / np.array(N[::-1])) @ r.T) * np.exp(-2j * np.pi * tm[:, None] * b0.ravel()[None, :])
     ref = (E.conj().T @ (E @ x.ravel().astype(np.complex128))).reshape(N) / np.prod(N)
     assert orc.rel_l2(g, ref) < 2e-2
+
+
+def shift_invariant_kspace(rng, nc, ndim, theta=0.8):
+    """k(p) = u0 diag(exp(i p . th)) V^-1 for commuting shift operators
+    G_a = V diag(exp(i th_a)) V^-1: a calibration on which GROG's least-squares
+    operators are exact (lamda = 0).  Returns (k(p) for real positions p (..., ndim)
+    in (x, y, z) order, calibration (nc, [nz,] ny, nx) on an 8^ndim grid)."""
+    V = rng.standard_normal((nc, nc)) + 1j * rng.standard_normal((nc, nc))
+    Vi = np.linalg.inv(V)
+    th = rng.uniform(-theta, theta, (ndim, nc))
+    u0 = (rng.standard_normal(nc) + 1j * rng.standard_normal(nc)) @ V
+
+    def k_at(p):
+        return (u0 * np.exp(1j * (np.asarray(p, np.float64) @ th))) @ Vi
+
+    n = 8
+    grid = np.stack(np.meshgrid(*([np.arange(n)] * ndim), indexing="ij"), -1)[..., ::-1]  # (z, y, x) -> (x, y, z)
+    cal = np.moveaxis(k_at(grid.reshape(-1, ndim)).reshape(*([n] * ndim), nc), -1, 0)
+    return k_at, cal
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_oracle_grog_exact_on_shift_invariant_calibration(ndim):
+    """Operator training, fractional powers, their composition order and the offset
+    lookup: each sample at c = g - d (d = 0.05 + 0.1 q) must land on k(c + delta),
+    delta = q / 10 the quantised offset, exactly up to rounding (the opposite shift
+    direction or no shift at all misses by > 0.1)."""
+    rng = np.random.default_rng(14)
+    nc = 6
+    k_at, cal = shift_invariant_kspace(rng, nc, ndim)
+    g = rng.integers(-6, 6, (2, 30, ndim)).astype(np.float64)
+    q = rng.integers(-5, 5, (2, 30, ndim))
+    coord = (g - (0.05 + 0.1 * q)).astype(np.float32)
+    x = np.moveaxis(k_at(coord.astype(np.float64)), -1, 0).astype(np.complex64)  # (nc, 2, 30)
+    out, ind, w = orc.grog_interp(x, cal, coord, 16, lamda=0.0)
+    delta = (np.floor(10 * (np.round(coord) - coord)).astype(np.float64)) / 10
+    ref = np.moveaxis(k_at(coord.astype(np.float64) + delta), -1, 0)
+    assert orc.rel_l2(out, ref) < 1e-5
+    assert orc.rel_l2(out, np.moveaxis(k_at(coord.astype(np.float64) - delta), -1, 0)) > 0.1
+    assert orc.rel_l2(x, ref) > 0.05
+    np.testing.assert_array_equal(ind, np.round(coord).astype(np.int64) + 8)
+    flat = (ind * np.array([1, 16, 256])[:ndim]).sum(-1).ravel()
+    cnt = np.array([np.sum(flat == f) for f in flat])
+    np.testing.assert_allclose(w.ravel(), 1.0 / cnt)
