@@ -29,7 +29,7 @@ import torch
 from . import _lib
 from ._b0 import mri_exp_approx
 from ._nufft import nufft_adj
-from ._plan import _as_tensor, plan_nufft, resolve_device
+from ._plan import _as_tensor, plan_nufft, resolve_device, to_caller
 
 
 class _GramHandle:
@@ -238,5 +238,5 @@ def sparse_gram(image, gram_matrix, norm=None, device="cpu", threadsperblock=128
     y = y.reshape(xc.shape)
     if not torch.is_complex(torch.empty((), dtype=dtype)):
         y = y.real
-    y = y.to(idevice).to(dtype)
+    y = to_caller(y, idevice, dtype)
     return y.detach().numpy() if as_numpy else y

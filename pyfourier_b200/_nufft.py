@@ -18,7 +18,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._plan import NUFFTPlan, _as_tensor, plan_nufft, resolve_device
+from ._plan import NUFFTPlan, _as_tensor, plan_nufft, resolve_device, to_caller
 
 
 def norm_code(norm):
@@ -250,8 +250,55 @@ def _to_compute(x, dev):
 def _finish(out, dtype, idevice, as_numpy):
     if not torch.is_complex(torch.empty((), dtype=dtype)):
         out = out.real
-    out = out.to(idevice).to(dtype)
+    out = to_caller(out, idevice, dtype)
     return out.detach().numpy() if as_numpy else out
+
+
+# Host inputs of at least this many bytes are processed in batch chunks whose
+# host->device copy, compute and device->host copy overlap (three streams).
+_HOST_PIPELINE_MIN_BYTES = 64 << 20
+_HOST_PIPELINE_CHUNKS = 4
+
+
+def _host_pipelined(t, grad_coord):
+    """A CPU complex64 input without autograd history takes the chunked host path."""
+    return (t.device.type == "cpu" and t.dtype == torch.complex64 and not t.requires_grad and grad_coord is None
+            and t.numel() * 8 >= _HOST_PIPELINE_MIN_BYTES)
+
+
+def _pipeline(xh, run, out_tail, dev):
+    """Apply ``run`` (device (b, ...) complex64 -> device (b, *out_tail) complex64, on the
+    current stream) to a CPU batch ``xh`` (B, ...) in up to _HOST_PIPELINE_CHUNKS chunks:
+    chunk j + 1 is copied to the device on one stream and chunk j - 1's result copied back
+    on another while chunk j computes.  Pageable inputs are staged chunk by chunk through
+    page-locked buffers.  Returns a page-locked CPU tensor (B, *out_tail)."""
+    B = xh.shape[0]
+    out = torch.empty((B, *out_tail), dtype=torch.complex64, pin_memory=True)
+    n = max(1, min(B, _HOST_PIPELINE_CHUNKS))
+    bounds = [(B * j // n, B * (j + 1) // n) for j in range(n)]
+    pinned = xh.is_pinned()
+    with torch.cuda.device(dev):
+        comp = torch.cuda.current_stream(dev)
+        h2d, d2h = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        h2d.wait_stream(comp)
+        for b0, b1 in bounds:
+            src = xh[b0:b1]
+            if not pinned:
+                stage = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+                stage.copy_(src)
+                src = stage
+            with torch.cuda.stream(h2d):
+                xd = torch.empty(src.shape, dtype=torch.complex64, device=dev)
+                xd.copy_(src, non_blocking=True)
+            comp.wait_stream(h2d)
+            xd.record_stream(comp)
+            yd = run(xd)
+            d2h.wait_stream(comp)
+            with torch.cuda.stream(d2h):
+                out[b0:b1].copy_(yd, non_blocking=True)
+            yd.record_stream(d2h)
+        d2h.synchronize()
+    return out
 
 
 def nufft(image, coord=None, shape=None, nufft_plan=None, basis=None, zmap=None, L=6, nbins=(40, 40),
@@ -286,7 +333,9 @@ def nufft(image, coord=None, shape=None, nufft_plan=None, basis=None, zmap=None,
     ip = plan.interpolator
     nd = plan.ndim
     dtype = image_t.dtype
-    _, x = _to_compute(image_t, dev)
+    c_in = coord_t if (coord_t is not None and coord_t.requires_grad) else None
+    host = _host_pipelined(image_t, c_in)
+    x = image_t if host else _to_compute(image_t, dev)[1]
     basis_t = _prep_basis(basis, dev)
     has_c = ip.nframes > 1 or basis_t is not None
     C = basis_t.shape[1] if basis_t is not None else ip.nframes
@@ -296,11 +345,15 @@ def nufft(image, coord=None, shape=None, nufft_plan=None, basis=None, zmap=None,
         raise ValueError(f"image needs a contrast/coefficient axis of size {C} before the spatial axes")
     batch_shape = x.shape[: x.ndim - nd - (1 if has_c else 0)]
     B = int(np.prod(batch_shape)) if len(batch_shape) else 1
-    xb = x.reshape(B, C, *plan.shape)
     sshape = _sample_shape(ip)
     wps, wfull = _split_weight(weight, sshape, dev)
     ctx = _Ctx(plan, basis_t, wps, norm_code(norm))
-    c_in = coord_t if (coord_t is not None and coord_t.requires_grad) else None
+    if host and B >= 2 and wfull is None:
+        y = _pipeline(x.reshape(B, C, *plan.shape), lambda xd: fwd_core(ctx, xd), (ip.total_samples,), dev)
+        return _finish(y.reshape(*batch_shape, *sshape), dtype, idevice, as_numpy)
+    if host:
+        x = _to_compute(x, dev)[1]
+    xb = x.reshape(B, C, *plan.shape)
     y = NUFFTFunction.apply(xb, c_in, ctx)
     y = y.reshape(*batch_shape, *sshape)
     if wfull is not None:
@@ -331,7 +384,9 @@ def nufft_adj(kspace, coord=None, shape=None, nufft_plan=None, basis=None, zmap=
     plan = nufft_plan
     ip = plan.interpolator
     dtype = k_t.dtype
-    _, k = _to_compute(k_t, dev)
+    c_in = coord_t if (coord_t is not None and coord_t.requires_grad) else None
+    host = _host_pipelined(k_t, c_in)
+    k = k_t if host else _to_compute(k_t, dev)[1]
     basis_t = _prep_basis(basis, dev)
     has_c = ip.nframes > 1 or basis_t is not None
     C = basis_t.shape[1] if basis_t is not None else ip.nframes
@@ -341,11 +396,16 @@ def nufft_adj(kspace, coord=None, shape=None, nufft_plan=None, basis=None, zmap=
     batch_shape = k.shape[: k.ndim - len(sshape)]
     B = int(np.prod(batch_shape)) if len(batch_shape) else 1
     wps, wfull = _split_weight(weight, sshape, dev)
+    ctx = _Ctx(plan, basis_t, wps, norm_code(norm))
+    if host and B >= 2 and wfull is None:
+        x = _pipeline(k.reshape(B, ip.total_samples), lambda kd: adj_core(ctx, kd), (C, *plan.shape), dev)
+        x = x.reshape(*batch_shape, *((C,) if has_c else ()), *plan.shape)
+        return _finish(x, dtype, idevice, as_numpy)
+    if host:
+        k = _to_compute(k, dev)[1]
     if wfull is not None:
         k = wfull * k
     kb = k.reshape(B, ip.total_samples)
-    ctx = _Ctx(plan, basis_t, wps, norm_code(norm))
-    c_in = coord_t if (coord_t is not None and coord_t.requires_grad) else None
     x = NUFFTAdjointFunction.apply(kb, c_in, ctx)
     x = x.reshape(*batch_shape, *((C,) if has_c else ()), *plan.shape)
     return _finish(x, dtype, idevice, as_numpy)

@@ -47,6 +47,29 @@ def resolve_device(device, fallback=None):
     return torch.device(f"cuda:{torch.cuda.current_device()}")
 
 
+def to_caller(t, idevice, dtype=None):
+    """Move a result computed on the GPU to the caller's device, in ``dtype``.
+
+    A result for a CPU caller is copied into page-locked host memory taken from
+    torch's caching host allocator (reused from the second call on, so no fresh
+    pages are faulted in per call) with an asynchronous copy, then the stream is
+    synchronised: the transfer runs at the link's pinned-memory bandwidth instead
+    of through the driver's pageable staging.  Results that carry autograd history
+    take the ordinary differentiable ``.to`` path.
+    """
+    if dtype is not None and t.dtype != dtype:
+        t = t.to(dtype)
+    idevice = torch.device(idevice)
+    if idevice.type != "cpu" or t.device.type != "cuda" or (t.requires_grad and torch.is_grad_enabled()):
+        return t.to(idevice)
+    t = t.contiguous()
+    out = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    with torch.cuda.device(t.device):
+        out.copy_(t, non_blocking=True)
+        torch.cuda.current_stream(t.device).synchronize()
+    return out
+
+
 def beta_f32(width, oversamp):
     """Kaiser-Bessel beta of src/pyfourier/_nufft/_plan.py:128 (int16 width, float32 osf)."""
     w = np.asarray(width, dtype=np.int16)

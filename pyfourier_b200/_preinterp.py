@@ -35,7 +35,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._plan import _as_tensor, resolve_device
+from ._plan import _as_tensor, resolve_device, to_caller
 
 
 def _operators(calib, ndim, lamda):
@@ -200,6 +200,7 @@ def grog_interp(input, calib, coord, shape, lamda=0.01, nsteps=11, device=None, 
     x = (x if torch.is_complex(x) else x.to(torch.float32)).to(torch.complex64).reshape(-1, plan.nc, plan.M)
     out = plan.apply(x).reshape(ishape)
     ind, w = plan.indexes, plan.weights
+    out, ind, w = to_caller(out, idevice), to_caller(ind, idevice), to_caller(w, idevice)
     if as_numpy:
-        return out.cpu().numpy(), ind.cpu().numpy(), w.cpu().numpy()
-    return out.to(idevice), ind.to(idevice), w.to(idevice)
+        return out.numpy(), ind.numpy(), w.numpy()
+    return out, ind, w
