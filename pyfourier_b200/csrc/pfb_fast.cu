@@ -30,6 +30,8 @@
 //   traj_il      d/dk of sum_b Re(conj(A x)_b v_b) (analytic Kaiser-Bessel derivative)
 #include <cmath>
 
+#include <type_traits>
+
 #include "pfb_common.cuh"
 
 namespace pfb {
@@ -420,9 +422,9 @@ __host__ __device__ constexpr int ipow(int b) { return D == 1 ? b : (D == 2 ? b 
 // offset 0 (an in-bounds address).  The offset is the element offset point * nch
 // when that fits in 32 bits (WIDE = false), else the point index.  Lanes build
 // 32 taps at a time.
-template <int D, int WM, bool WIDE>
+template <int D, int WM, bool WIDE, typename WT>
 __device__ __forceinline__ void build_tap_list(const InterpIL &P, const float *sw, const int *sp, int nch,
-                                               int *s_off, float *s_wt, int lane) {
+                                               int *s_off, WT *s_wt, int lane) {
     constexpr int NT = ipow<D>(WM);
     const int nx = P.g.nos[0], nxy = P.g.nos[0] * P.g.nos[1];
     for (int t = lane; t < NT; t += 32) {
@@ -436,17 +438,25 @@ __device__ __forceinline__ void build_tap_list(const InterpIL &P, const float *s
             if (!WIDE) off *= nch;
         }
         s_off[t] = off;
-        s_wt[t] = w;
+        if constexpr (sizeof(WT) == sizeof(float2))
+            s_wt[t] = make_float2(w, w);  // the broadcast operand of a packed FFMA2
+        else
+            s_wt[t] = w;
     }
 }
 
 template <int D, int WM, bool WIDE>
 __global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const InterpIL P) {
     constexpr int NT = ipow<D>(WM);
+    // up to 64 taps the weights are kept as (w, w) pairs for FFMA2 and, with one
+    // channel per lane, the gather loop takes 4 taps per 16-byte offset load
+    constexpr bool PAIRS = NT <= 64;
+    constexpr bool VEC = PAIRS && NT % 4 == 0;
+    using WT = typename std::conditional<PAIRS, float2, float>::type;
     __shared__ float s_w[kTileWarps][3 * WM];
     __shared__ int s_p[kTileWarps][3 * WM];
-    __shared__ int s_off[kTileWarps][NT];
-    __shared__ float s_wt[kTileWarps][NT];
+    __shared__ __align__(16) int s_off[kTileWarps][NT];
+    __shared__ __align__(16) WT s_wt[kTileWarps][NT];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cw = P.cw, lcw = log2i(cw), tg_n = 32 >> lcw;
     const int cl = lane & (cw - 1), tg = lane >> lcw;
@@ -466,10 +476,33 @@ __global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const Interp
             const int c = c0 + cl;
             const float2 *Gc = G + (c < nch ? c : nch - 1);  // in-bounds address; result discarded
             float2 acc = make_float2(0.f, 0.f);
+            if (VEC && tg_n == 1) {
+                // taps in order 0, 1, 2, ...: the same sums as the loop below
+                const int4 *o4 = reinterpret_cast<const int4 *>(s_off[warp]);
+                const float4 *w4 = reinterpret_cast<const float4 *>(s_wt[warp]);
+#pragma unroll 4
+                for (int t4 = 0; t4 < NT / 4; ++t4) {
+                    const int4 o = o4[t4];
+                    const float4 wa = w4[2 * t4], wb = w4[2 * t4 + 1];
+                    float2 v[4];
+                    const int oo[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        v[u] = WIDE ? __ldg(Gc + (int64_t)oo[u] * nch) : __ldg(Gc + oo[u]);
+                    acc = __ffma2_rn(make_float2(wa.x, wa.y), v[0], acc);
+                    acc = __ffma2_rn(make_float2(wa.z, wa.w), v[1], acc);
+                    acc = __ffma2_rn(make_float2(wb.x, wb.y), v[2], acc);
+                    acc = __ffma2_rn(make_float2(wb.z, wb.w), v[3], acc);
+                }
+            } else {
 #pragma unroll 8
-            for (int t = tg; t < NT; t += tg_n) {
-                const float2 v = WIDE ? __ldg(Gc + (int64_t)s_off[warp][t] * nch) : __ldg(Gc + s_off[warp][t]);
-                acc = cfma(s_wt[warp][t], v, acc);
+                for (int t = tg; t < NT; t += tg_n) {
+                    const float2 v = WIDE ? __ldg(Gc + (int64_t)s_off[warp][t] * nch) : __ldg(Gc + s_off[warp][t]);
+                    if constexpr (PAIRS)
+                        acc = __ffma2_rn(s_wt[warp][t], v, acc);
+                    else
+                        acc = cfma(s_wt[warp][t], v, acc);
+                }
             }
             // reduce over tap groups (lanes that share the channel)
             for (int off = cw; off < 32; off <<= 1) {
@@ -840,12 +873,13 @@ constexpr int kRegBatch = 128;                // samples per staged batch
 constexpr int kRegTile = 8;                   // packed tile extent per axis
 constexpr int kRegPts = kRegTile * kRegTile * kRegTile;
 // one staging buffer: raw values [B][32] f2, raw weights [B][24] f, raw first
-// taps [B][4] i, neighbour bits [B] i, tile weights [B][24] f, masks [B] u
+// taps [B][4] i, neighbour bits [B] i, tile weights [B][24] f2 (each weight held
+// twice, the broadcast operand of a packed FFMA2), masks [B] u
 constexpr size_t kRegOffW = (size_t)kRegBatch * 32 * sizeof(float2);
 constexpr size_t kRegOffX = kRegOffW + (size_t)kRegBatch * 24 * sizeof(float);
 constexpr size_t kRegOffD = kRegOffX + (size_t)kRegBatch * 4 * sizeof(int);
 constexpr size_t kRegOffTW = kRegOffD + (size_t)kRegBatch * sizeof(int);
-constexpr size_t kRegOffM = kRegOffTW + (size_t)kRegBatch * 24 * sizeof(float);
+constexpr size_t kRegOffM = kRegOffTW + (size_t)kRegBatch * 24 * sizeof(float2);
 constexpr size_t kRegBuf = kRegOffM + (size_t)kRegBatch * sizeof(unsigned);
 constexpr size_t kRegSmemOut = (size_t)kRegPts * 33 * sizeof(float2);
 constexpr size_t kRegSmem = kRegPts * sizeof(int) + (kRegSmemOut > 2 * kRegBuf ? kRegSmemOut : 2 * kRegBuf);
@@ -951,12 +985,9 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
     const int wrapa = la == 0 ? wrap[0] : (la == 1 ? wrap[1] : wrap[2]);
     const int nosa = la == 0 ? P.g.nos[0] : (la == 1 ? P.g.nos[1] : P.g.nos[2]);
     const int wa = la == 0 ? P.g.w[0] : (la == 1 ? P.g.w[1] : P.g.w[2]);
-    float ax[32], ay[32];
+    float2 acc[32];
 #pragma unroll
-    for (int q = 0; q < 32; ++q) {
-        ax[q] = 0.f;
-        ay[q] = 0.f;
-    }
+    for (int q = 0; q < 32; ++q) acc[q] = make_float2(0.f, 0.f);
     if (nbat > 0) issue(0, 0);
     cp_async_commit();
     for (int b = 0; b < nbat; ++b) {
@@ -970,7 +1001,7 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
         const float *rw = reinterpret_cast<const float *>(B + kRegOffW);
         const int *rx = reinterpret_cast<const int *>(B + kRegOffX);
         const int *rd = reinterpret_cast<const int *>(B + kRegOffD);
-        float *tw = reinterpret_cast<float *>(B + kRegOffTW);
+        float2 *tw = reinterpret_cast<float2 *>(B + kRegOffTW);
         unsigned *tm = reinterpret_cast<unsigned *>(B + kRegOffM);
         const int nb = batch_size(b);
         for (int q = warp; q < nb; q += kSpreadWarps) {
@@ -981,7 +1012,7 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
                 int i = lt - d;
                 if (wrapa && i < 0) i += wrapa;
                 if (lt < texta && i >= 0 && i < wa) wv = rw[q * 24 + la * WM + i];
-                tw[q * 24 + lane] = wv;
+                tw[q * 24 + lane] = make_float2(wv, wv);
             }
             const unsigned m = __ballot_sync(0xffffffffu, wv != 0.f);
             if (lane == 0) tm[q] = m;
@@ -1000,25 +1031,29 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
                 const unsigned m = tm[q];
                 const unsigned ym = (m >> (8 + by0)) & 0xFu, zm = (m >> (16 + bz0)) & 0x3u;
                 const float2 v = rv[q * 32 + lane];
-                const float4 wx = *reinterpret_cast<const float4 *>(tw + q * 24 + bx0);
-                const float4 wy = *reinterpret_cast<const float4 *>(tw + q * 24 + 8 + by0);
-                const float2 wz = *reinterpret_cast<const float2 *>(tw + q * 24 + 16 + bz0);
-                const float wxa[4] = {wx.x, wx.y, wx.z, wx.w};
-                const float wya[4] = {wy.x, wy.y, wy.z, wy.w};
+                // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..
+                const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 24);
+                const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
+                const float4 y01 = t4[(8 + by0) >> 1], y23 = t4[((8 + by0) >> 1) + 1];
+                const float4 z01 = t4[(16 + bz0) >> 1];
+                const float2 wx2[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
+                                       make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
+                const float2 wy2[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w),
+                                       make_float2(y23.x, y23.y), make_float2(y23.z, y23.w)};
+                const float2 wz2[2] = {make_float2(z01.x, z01.y), make_float2(z01.z, z01.w)};
 #pragma unroll
                 for (int pz = 0; pz < 2; ++pz) {
                     if (!((zm >> pz) & 1u)) continue;
-                    const float wzz = pz ? wz.y : wz.x;
 #pragma unroll
                     for (int py = 0; py < 4; ++py) {
                         if ((ym >> py) & 1u) {
-                            const float wyz = wzz * wya[py];
-                            const float vx = wyz * v.x, vy = wyz * v.y;
+                            // packed: (wz wy, wz wy), then (wyz v.x, wyz v.y), then per x
+                            // acc += (wx, wx) * that -- the same roundings as scalar fmaf
+                            const float2 vv = __fmul2_rn(__fmul2_rn(wz2[pz], wy2[py]), v);
 #pragma unroll
                             for (int px = 0; px < 4; ++px) {
                                 const int q2 = px + 4 * (py + 4 * pz);
-                                ax[q2] = fmaf(wxa[px], vx, ax[q2]);
-                                ay[q2] = fmaf(wxa[px], vy, ay[q2]);
+                                acc[q2] = __ffma2_rn(wx2[px], vv, acc[q2]);
                             }
                         }
                     }
@@ -1028,7 +1063,7 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
     }
     __syncthreads();  // staging no longer read: reuse it for the output tile
 #pragma unroll
-    for (int q = 0; q < 32; ++q) s_out[(warp * 32 + q) * 33 + lane] = make_float2(ax[q], ay[q]);
+    for (int q = 0; q < 32; ++q) s_out[(warp * 32 + q) * 33 + lane] = acc[q];
     __syncthreads();
     const int grp = P.ch.K ? 0 : (it.frame < 0 ? 0 : it.frame);
     for (int e = threadIdx.x; e < 32 * kRegPts; e += blockDim.x) {
