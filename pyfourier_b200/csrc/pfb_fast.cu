@@ -621,6 +621,65 @@ __device__ __forceinline__ void bin_range(const SpreadIL &P, int bin, int code, 
     }
 }
 
+// Prefix table of the (neighbour delta, edge code) ranges that reach the item's
+// tile: the samples of bins t - delta, delta in {0,1}^D, whose edge code contains
+// delta.  Entry r, in the fixed order (delta ascending, then code ascending among
+// the codes containing delta) in which the plan's owner items count positions,
+// holds the first sorted position s_beg[r], the delta s_dlt[r] and the prefix
+// s_pre[r] of the range sizes; s_pre[NR] is the total.  A delta that would wrap a
+// single-tile axis onto itself gives an empty range.  The calling warp computes
+// one range per lane (the loads go out together) and scans the sizes.
+template <int D>
+__device__ __forceinline__ void neighbour_ranges(const SpreadIL &P, const OwnerItem &it, int *s_pre, int *s_beg,
+                                                 int *s_dlt, int lane) {
+    constexpr int NR = D == 1 ? 3 : (D == 2 ? 9 : 27);
+    int dlt = 0, code = 0;
+    {
+        int r = 0;
+#pragma unroll
+        for (int d = 0; d < (1 << D); ++d)
+#pragma unroll
+            for (int cd = 0; cd < (1 << D); ++cd)
+                if ((cd & d) == d) {
+                    if (r == lane) {
+                        dlt = d;
+                        code = cd;
+                    }
+                    ++r;
+                }
+    }
+    int cnt = 0, s0 = 0;
+    if (lane < NR) {
+        int bin = 0, stride = 1;
+        bool ok = true;
+        for (int a = 0; a < D; ++a) {
+            const int da = (dlt >> a) & 1, nb = P.g.nbins[a];
+            if (da && nb == 1) ok = false;
+            int tc = tile_coord(it.tile, a, P.g) - da;
+            tc = tc < 0 ? tc + nb : tc;
+            bin += tc * stride;
+            stride *= nb;
+        }
+        if (ok) {
+            int s1;
+            bin_range(P, bin, code, it.frame < 0 ? 0 : it.frame, &s0, &s1);
+            cnt = s1 - s0;
+        }
+    }
+    int inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+    }
+    if (lane < NR) {
+        s_pre[lane] = inc - cnt;
+        s_beg[lane] = s0;
+        s_dlt[lane] = dlt;
+    }
+    if (lane == NR - 1) s_pre[NR] = inc;
+}
+
 // Per-sample kernel taps for the spread, computed once per apply: weights
 // w[j][a * WM + i] and the wrapped first tap x0m[j][a] (bin-sorted order).
 template <int D, int WM>
@@ -706,35 +765,7 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
     }
     // samples of the neighbour bins t - delta, delta in {0,1}^D (no wrap onto
     // itself), whose edge code contains delta: exactly those reaching this tile
-    int nrng = 0;
-    if (threadIdx.x == 0) {
-        int run = 0;
-        for (int dlt = 0; dlt < (1 << D); ++dlt) {
-            int bin = 0, stride = 1;
-            bool ok = true;
-            for (int a = 0; a < D; ++a) {
-                int da = (dlt >> a) & 1;
-                int nb = P.g.nbins[a];
-                if (da && nb == 1) ok = false;
-                int tc = tile_coord(it.tile, a, P.g) - da;
-                tc = tc < 0 ? tc + nb : tc;
-                bin += tc * stride;
-                stride *= nb;
-            }
-            if (!ok) continue;
-            for (int code = 0; code < (1 << D); ++code) {
-                if ((code & dlt) != dlt) continue;
-                int s0, s1;
-                bin_range(P, bin, code, it.frame < 0 ? 0 : it.frame, &s0, &s1);
-                s_pre[nrng] = run;
-                s_beg[nrng] = s0;
-                s_dlt[nrng] = dlt;
-                run += s1 - s0;
-                ++nrng;
-            }
-        }
-        for (int q = nrng; q <= NR; ++q) s_pre[q] = run;
-    }
+    if (warp == 0) neighbour_ranges<D>(P, it, s_pre, s_beg, s_dlt, lane);
     __syncthreads();
     constexpr int DW = D * WM;
     // virtual index v in [it.v0, it.v1) over the concatenated neighbour ranges
@@ -869,21 +900,25 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
 // 24-bit mask of the non-zero entries, by which each warp picks (ballot) the
 // samples that touch its block.  The tile leaves through shared memory,
 // coalesced along x.
-constexpr int kRegBatch = 128;                // samples per staged batch
+constexpr int kRegBatch = 224;                // samples per staged batch
 constexpr int kRegTile = 8;                   // packed tile extent per axis
 constexpr int kRegPts = kRegTile * kRegTile * kRegTile;
-// one staging buffer: raw values [B][32] f2, raw weights [B][24] f, raw first
-// taps [B][4] i, neighbour bits [B] i, tile weights [B][24] f2 (each weight held
-// twice, the broadcast operand of a packed FFMA2), masks [B] u
+// staging: two raw buffers (values [B][32] f2, weights [B][24] f, first taps
+// [B][4] i, neighbour bits [B] i), filled by cp.async one batch ahead, then one
+// set of derived arrays (tile weights [B][24] f2, each weight held twice as the
+// broadcast operand of a packed FFMA2; masks [B] u), written and read within
+// one batch
 constexpr size_t kRegOffW = (size_t)kRegBatch * 32 * sizeof(float2);
 constexpr size_t kRegOffX = kRegOffW + (size_t)kRegBatch * 24 * sizeof(float);
 constexpr size_t kRegOffD = kRegOffX + (size_t)kRegBatch * 4 * sizeof(int);
-constexpr size_t kRegOffTW = kRegOffD + (size_t)kRegBatch * sizeof(int);
+constexpr size_t kRegBuf = kRegOffD + (size_t)kRegBatch * sizeof(int);
+constexpr size_t kRegOffTW = 2 * kRegBuf;
 constexpr size_t kRegOffM = kRegOffTW + (size_t)kRegBatch * 24 * sizeof(float2);
-constexpr size_t kRegBuf = kRegOffM + (size_t)kRegBatch * sizeof(unsigned);
+constexpr size_t kRegStage = kRegOffM + (size_t)kRegBatch * sizeof(unsigned);
 constexpr size_t kRegSmemOut = (size_t)kRegPts * 33 * sizeof(float2);
-constexpr size_t kRegSmem = kRegPts * sizeof(int) + (kRegSmemOut > 2 * kRegBuf ? kRegSmemOut : 2 * kRegBuf);
+constexpr size_t kRegSmem = kRegPts * sizeof(int) + (kRegSmemOut > kRegStage ? kRegSmemOut : kRegStage);
 static_assert(kRegBuf % 16 == 0 && kRegOffTW % 16 == 0, "16-byte aligned staging arrays");
+static_assert(kRegSmem <= 227 * 1024, "shared memory of one CTA");
 
 
 
@@ -921,33 +956,7 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
         }
         s_pos[pt] = pos;
     }
-    if (threadIdx.x == 0) {
-        int run = 0, nrng = 0;
-        for (int dlt = 0; dlt < 8; ++dlt) {
-            int bin = 0, stride = 1;
-            bool ok = true;
-            for (int a = 0; a < D; ++a) {
-                const int da = (dlt >> a) & 1, nb = P.g.nbins[a];
-                if (da && nb == 1) ok = false;
-                int tc = tile_coord(it.tile, a, P.g) - da;
-                tc = tc < 0 ? tc + nb : tc;
-                bin += tc * stride;
-                stride *= nb;
-            }
-            if (!ok) continue;
-            for (int code = 0; code < 8; ++code) {
-                if ((code & dlt) != dlt) continue;
-                int s0, s1;
-                bin_range(P, bin, code, it.frame < 0 ? 0 : it.frame, &s0, &s1);
-                s_pre[nrng] = run;
-                s_beg[nrng] = s0;
-                s_dlt[nrng] = dlt;
-                run += s1 - s0;
-                ++nrng;
-            }
-        }
-        for (int q = nrng; q <= NR; ++q) s_pre[q] = run;
-    }
+    if (warp == 0) neighbour_ranges<3>(P, it, s_pre, s_beg, s_dlt, lane);
     __syncthreads();
     const int nvis = it.v1 - it.v0;
     const int nbat = (nvis + kRegBatch - 1) / kRegBatch;
@@ -1001,8 +1010,8 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
         const float *rw = reinterpret_cast<const float *>(B + kRegOffW);
         const int *rx = reinterpret_cast<const int *>(B + kRegOffX);
         const int *rd = reinterpret_cast<const int *>(B + kRegOffD);
-        float2 *tw = reinterpret_cast<float2 *>(B + kRegOffTW);
-        unsigned *tm = reinterpret_cast<unsigned *>(B + kRegOffM);
+        float2 *tw = reinterpret_cast<float2 *>(ub + kRegOffTW);
+        unsigned *tm = reinterpret_cast<unsigned *>(ub + kRegOffM);
         const int nb = batch_size(b);
         for (int q = warp; q < nb; q += kSpreadWarps) {
             float wv = 0.f;
@@ -1028,10 +1037,10 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
             while (hm) {
                 const int q = q0 + __ffs(hm) - 1;
                 hm &= hm - 1;
-                const unsigned m = tm[q];
-                const unsigned ym = (m >> (8 + by0)) & 0xFu, zm = (m >> (16 + bz0)) & 0x3u;
                 const float2 v = rv[q * 32 + lane];
-                // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..
+                // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..; zero
+                // outside the sample's support, so every row of the block is updated
+                // without a test (a branch per row costs more than the row)
                 const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 24);
                 const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
                 const float4 y01 = t4[(8 + by0) >> 1], y23 = t4[((8 + by0) >> 1) + 1];
@@ -1040,21 +1049,17 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
                                        make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
                 const float2 wy2[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w),
                                        make_float2(y23.x, y23.y), make_float2(y23.z, y23.w)};
-                const float2 wz2[2] = {make_float2(z01.x, z01.y), make_float2(z01.z, z01.w)};
+                const float2 vz[2] = {__fmul2_rn(make_float2(z01.x, z01.y), v),
+                                      __fmul2_rn(make_float2(z01.z, z01.w), v)};
 #pragma unroll
                 for (int pz = 0; pz < 2; ++pz) {
-                    if (!((zm >> pz) & 1u)) continue;
 #pragma unroll
                     for (int py = 0; py < 4; ++py) {
-                        if ((ym >> py) & 1u) {
-                            // packed: (wz wy, wz wy), then (wyz v.x, wyz v.y), then per x
-                            // acc += (wx, wx) * that -- the same roundings as scalar fmaf
-                            const float2 vv = __fmul2_rn(__fmul2_rn(wz2[pz], wy2[py]), v);
+                        const float2 vv = __fmul2_rn(wy2[py], vz[pz]);  // wy (wz v)
 #pragma unroll
-                            for (int px = 0; px < 4; ++px) {
-                                const int q2 = px + 4 * (py + 4 * pz);
-                                acc[q2] = __ffma2_rn(wx2[px], vv, acc[q2]);
-                            }
+                        for (int px = 0; px < 4; ++px) {
+                            const int q2 = px + 4 * (py + 4 * pz);
+                            acc[q2] = __ffma2_rn(wx2[px], vv, acc[q2]);
                         }
                     }
                 }
