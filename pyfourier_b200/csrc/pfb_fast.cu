@@ -900,36 +900,48 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
 // 24-bit mask of the non-zero entries, by which each warp picks (ballot) the
 // samples that touch its block.  The tile leaves through shared memory,
 // coalesced along x.
-constexpr int kRegBatch = 224;                // samples per staged batch
 constexpr int kRegTile = 8;                   // packed tile extent per axis
 constexpr int kRegPts = kRegTile * kRegTile * kRegTile;
-// staging: two raw buffers (values [B][32] f2, weights [B][24] f, first taps
+// Launch shape of the register spread for CPW channels per lane group: the 32
+// lanes of a warp are G = 32 / CPW groups of CPW channels, each group owning one
+// of the 16 blocks of 4 x 4 x 2 points, so a CTA has 16 / G warps.
+// Staging: two raw buffers (values [B][CPW] f2, weights [B][24] f, first taps
 // [B][4] i, neighbour bits [B] i), filled by cp.async one batch ahead, then one
 // set of derived arrays (tile weights [B][24] f2, each weight held twice as the
-// broadcast operand of a packed FFMA2; masks [B] u), written and read within
-// one batch
-constexpr size_t kRegOffW = (size_t)kRegBatch * 32 * sizeof(float2);
-constexpr size_t kRegOffX = kRegOffW + (size_t)kRegBatch * 24 * sizeof(float);
-constexpr size_t kRegOffD = kRegOffX + (size_t)kRegBatch * 4 * sizeof(int);
-constexpr size_t kRegBuf = kRegOffD + (size_t)kRegBatch * sizeof(int);
-constexpr size_t kRegOffTW = 2 * kRegBuf;
-constexpr size_t kRegOffM = kRegOffTW + (size_t)kRegBatch * 24 * sizeof(float2);
-constexpr size_t kRegStage = kRegOffM + (size_t)kRegBatch * sizeof(unsigned);
-constexpr size_t kRegSmemOut = (size_t)kRegPts * 33 * sizeof(float2);
-constexpr size_t kRegSmem = kRegPts * sizeof(int) + (kRegSmemOut > kRegStage ? kRegSmemOut : kRegStage);
-static_assert(kRegBuf % 16 == 0 && kRegOffTW % 16 == 0, "16-byte aligned staging arrays");
-static_assert(kRegSmem <= 227 * 1024, "shared memory of one CTA");
+// broadcast operand of a packed FFMA2; masks [B] u), written and read within one
+// batch.  With 32 channels one CTA fills an SM (registers); smaller groups use
+// smaller batches so that 2 (16 channels) or 3 (8) CTAs share an SM.
+template <int CPW>
+struct RegCfg {
+    static constexpr int G = 32 / CPW;
+    static constexpr int NW = 16 / G;
+    static constexpr int Batch = CPW == 32 ? 224 : 128;
+    static constexpr int MinBlocks = CPW == 32 ? 1 : (CPW == 16 ? 2 : 3);
+    static constexpr size_t OffW = (size_t)Batch * CPW * sizeof(float2);
+    static constexpr size_t OffX = OffW + (size_t)Batch * 24 * sizeof(float);
+    static constexpr size_t OffD = OffX + (size_t)Batch * 4 * sizeof(int);
+    static constexpr size_t Buf = OffD + (size_t)Batch * sizeof(int);
+    static constexpr size_t OffTW = 2 * Buf;
+    static constexpr size_t OffM = OffTW + (size_t)Batch * 24 * sizeof(float2);
+    static constexpr size_t Stage = OffM + (size_t)Batch * sizeof(unsigned);
+    static constexpr size_t Out = (size_t)kRegPts * (CPW + 1) * sizeof(float2);
+    static constexpr size_t Smem = kRegPts * sizeof(int) + (Out > Stage ? Out : Stage);
+    static_assert(Buf % 16 == 0 && OffTW % 16 == 0, "16-byte aligned staging arrays");
+    static_assert(Smem * MinBlocks + MinBlocks * 1024 <= 228 * 1024, "shared memory of the CTAs of one SM");
+};
 
 
 
-template <int WM>
-__global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const SpreadIL P) {
-    static_assert(kSpreadWarps == 16, "16 warps own the 2 x 2 x 4 blocks of the tile");
+template <int WM, int CPW>
+__global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
+    spread_reg3_kernel(const SpreadIL P) {
+    using C = RegCfg<CPW>;
+    constexpr int G = C::G, NW = C::NW;
     constexpr int D = 3, DW = D * WM;
     extern __shared__ __align__(16) unsigned char smraw[];
     int *s_pos = reinterpret_cast<int *>(smraw);
     unsigned char *ub = smraw + kRegPts * sizeof(int);
-    float2 *s_out = reinterpret_cast<float2 *>(ub);  // [512][33], after the last batch
+    float2 *s_out = reinterpret_cast<float2 *>(ub);  // [16 blocks x 32 points][CPW + 1], after the last batch
     constexpr int NR = 27;
     __shared__ int s_pre[NR + 1];
     __shared__ int s_beg[NR];
@@ -937,7 +949,8 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
     const OwnerItem it = P.items[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nch = P.ch.nch;
-    const int c0 = blockIdx.y * 32, c = c0 + lane;
+    const int cl = lane % CPW, grpl = lane / CPW;  // channel and block group of this lane
+    const int c0 = blockIdx.y * CPW, c = c0 + cl;
     int org[3], text[3], wrap[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -959,17 +972,17 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
     if (warp == 0) neighbour_ranges<3>(P, it, s_pre, s_beg, s_dlt, lane);
     __syncthreads();
     const int nvis = it.v1 - it.v0;
-    const int nbat = (nvis + kRegBatch - 1) / kRegBatch;
+    const int nbat = (nvis + C::Batch - 1) / C::Batch;
     auto batch_size = [&](int bb) { return (nvis - bb + nbat - 1) / nbat; };
-    // issue the copies of batch bb into buffer buf (warps take samples warp, warp + 16, ...)
+    // issue the copies of batch bb into buffer buf (warps take samples warp, warp + NW, ...)
     auto issue = [&](int bb, int buf) {
-        unsigned char *B = ub + buf * kRegBuf;
+        unsigned char *B = ub + buf * C::Buf;
         float2 *rv = reinterpret_cast<float2 *>(B);
-        float *rw = reinterpret_cast<float *>(B + kRegOffW);
-        int *rx = reinterpret_cast<int *>(B + kRegOffX);
-        int *rd = reinterpret_cast<int *>(B + kRegOffD);
+        float *rw = reinterpret_cast<float *>(B + C::OffW);
+        int *rx = reinterpret_cast<int *>(B + C::OffX);
+        int *rd = reinterpret_cast<int *>(B + C::OffD);
         const int nb = batch_size(bb);
-        for (int q = warp; q < nb; q += kSpreadWarps) {
+        for (int q = warp; q < nb; q += NW) {
             // batch bb takes visits bb, bb + nbat, bb + 2 nbat, ...: every batch
             // mixes the neighbour ranges, so all warps find work in it
             const int v = it.v0 + bb + q * nbat;
@@ -978,15 +991,24 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
             const unsigned le = __ballot_sync(0xffffffffu, lane < NR && s_pre[lane] <= v);
             const int r = 31 - __clz(le);
             const int64_t j = (int64_t)s_beg[r] + (v - s_pre[r]);
-            cp_async8(rv + q * 32 + lane, P.vals + j * nch + (c < nch ? c : 0), c < nch);
+            if (lane < CPW) cp_async8(rv + q * CPW + lane, P.vals + j * nch + (c < nch ? c : 0), c < nch);
             if (lane < DW) cp_async4(rw + q * 24 + lane, P.wtap + j * DW + lane);
             if (lane < D) cp_async4(rx + q * 4 + lane, P.xtap + j * D + lane);
             if (lane == 0) rd[q] = s_dlt[r];
         }
     };
-    // this warp's block and its bits in the sample masks
-    const int bx0 = (warp & 1) * 4, by0 = ((warp >> 1) & 1) * 4, bz0 = (warp >> 2) * 2;
-    const unsigned bmx = 0xFu << bx0, bmy = 0xFu << (8 + by0), bmz = 0x3u << (16 + bz0);
+    // this lane's block (block id warp * G + group) and the warp's blocks' bits in the
+    // sample masks
+    const int bid = warp * G + grpl;
+    const int bx0 = (bid & 1) * 4, by0 = ((bid >> 1) & 1) * 4, bz0 = (bid >> 2) * 2;
+    unsigned bmx[G], bmy[G], bmz[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const int b2 = warp * G + g;
+        bmx[g] = 0xFu << ((b2 & 1) * 4);
+        bmy[g] = 0xFu << (8 + ((b2 >> 1) & 1) * 4);
+        bmz[g] = 0x3u << (16 + (b2 >> 2) * 2);
+    }
     // lane (a, t): tile coordinate t on axis a (lanes 0..23)
     const int la = lane >> 3, lt = lane & 7;
     const int orga = la == 0 ? org[0] : (la == 1 ? org[1] : org[2]);
@@ -1005,15 +1027,15 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
         __syncthreads();  // batch b landed; every warp is done with batch b - 1
         if (b + 1 < nbat) issue(b + 1, cur ^ 1);
         cp_async_commit();
-        unsigned char *B = ub + cur * kRegBuf;
+        unsigned char *B = ub + cur * C::Buf;
         const float2 *rv = reinterpret_cast<const float2 *>(B);
-        const float *rw = reinterpret_cast<const float *>(B + kRegOffW);
-        const int *rx = reinterpret_cast<const int *>(B + kRegOffX);
-        const int *rd = reinterpret_cast<const int *>(B + kRegOffD);
-        float2 *tw = reinterpret_cast<float2 *>(ub + kRegOffTW);
-        unsigned *tm = reinterpret_cast<unsigned *>(ub + kRegOffM);
+        const float *rw = reinterpret_cast<const float *>(B + C::OffW);
+        const int *rx = reinterpret_cast<const int *>(B + C::OffX);
+        const int *rd = reinterpret_cast<const int *>(B + C::OffD);
+        float2 *tw = reinterpret_cast<float2 *>(ub + C::OffTW);
+        unsigned *tm = reinterpret_cast<unsigned *>(ub + C::OffM);
         const int nb = batch_size(b);
-        for (int q = warp; q < nb; q += kSpreadWarps) {
+        for (int q = warp; q < nb; q += NW) {
             float wv = 0.f;
             if (lane < 24) {
                 int d = rx[q * 4 + la] - orga;
@@ -1031,13 +1053,14 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
             bool hit = false;
             if (q0 + lane < nb) {
                 const unsigned m = tm[q0 + lane];
-                hit = (m & bmx) && (m & bmy) && (m & bmz);
+#pragma unroll
+                for (int g = 0; g < G; ++g) hit = hit || ((m & bmx[g]) && (m & bmy[g]) && (m & bmz[g]));
             }
             unsigned hm = __ballot_sync(0xffffffffu, hit);
             while (hm) {
                 const int q = q0 + __ffs(hm) - 1;
                 hm &= hm - 1;
-                const float2 v = rv[q * 32 + lane];
+                const float2 v = rv[q * CPW + cl];
                 // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..; zero
                 // outside the sample's support, so every row of the block is updated
                 // without a test (a branch per row costs more than the row)
@@ -1068,22 +1091,22 @@ __global__ void __launch_bounds__(kSpreadWarps * 32, 1) spread_reg3_kernel(const
     }
     __syncthreads();  // staging no longer read: reuse it for the output tile
 #pragma unroll
-    for (int q = 0; q < 32; ++q) s_out[(warp * 32 + q) * 33 + lane] = acc[q];
+    for (int q = 0; q < 32; ++q) s_out[(bid * 32 + q) * (CPW + 1) + cl] = acc[q];
     __syncthreads();
     const int grp = P.ch.K ? 0 : (it.frame < 0 ? 0 : it.frame);
-    for (int e = threadIdx.x; e < 32 * kRegPts; e += blockDim.x) {
-        const int cl = e / kRegPts, pt = e - cl * kRegPts;
-        const int ch = c0 + cl;
+    for (int e = threadIdx.x; e < CPW * kRegPts; e += blockDim.x) {
+        const int ce = e / kRegPts, pt = e - ce * kRegPts;
+        const int ch = c0 + ce;
         if (ch >= nch) break;
         const int pos = s_pos[pt];
         if (pos < 0) continue;
         const int x = pt & 7, y = (pt >> 3) & 7, z = pt >> 6;
         const int w = (x >> 2) | ((y >> 2) << 1) | ((z >> 1) << 2);
         const int q = (x & 3) | ((y & 3) << 2) | ((z & 1) << 4);
-        const float2 vv = s_out[(w * 32 + q) * 33 + cl];
-        float2 *G = P.grid + ((int64_t)grp * nch + ch) * P.g.gvol;
-        if (it.atomic) atomicAdd(G + pos, vv);
-        else G[pos] = vv;
+        const float2 vv = s_out[(w * 32 + q) * (CPW + 1) + ce];
+        float2 *Gp = P.grid + ((int64_t)grp * nch + ch) * P.g.gvol;
+        if (it.atomic) atomicAdd(Gp + pos, vv);
+        else Gp[pos] = vv;
     }
 }
 
@@ -1168,14 +1191,23 @@ int launch_traj_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
     return PFB_OK;
 }
 
-template <int WM>
+template <int WM, int CPW>
 int launch_spread_reg3_t(const SpreadIL &P, int nitems, int nchunks, cudaStream_t s) {
-    auto k = spread_reg3_kernel<WM>;
-    PFB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRegSmem));
+    using C = RegCfg<CPW>;
+    auto k = spread_reg3_kernel<WM, CPW>;
+    PFB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::Smem));
     dim3 grid(nitems, nchunks);
-    k<<<grid, kSpreadWarps * 32, kRegSmem, s>>>(P);
+    k<<<grid, C::NW * 32, C::Smem, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
+}
+
+template <int WM>
+int launch_spread_reg3_w(const SpreadIL &P, int nitems, int nch, cudaStream_t s) {
+    // channel groups of 8 or 16 keep few-channel spreads on register tiles
+    if (nch <= 8) return launch_spread_reg3_t<WM, 8>(P, nitems, 1, s);
+    if (nch <= 16) return launch_spread_reg3_t<WM, 16>(P, nitems, 1, s);
+    return launch_spread_reg3_t<WM, 32>(P, nitems, (nch + 31) / 32, s);
 }
 
 template <int D, int WM>
@@ -1455,12 +1487,12 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             S.cw = spread_cw(p, c);
             S.per_frame = basis ? 0 : 1;
             if (p->g.ndim == 3 && p->g.tile[0] <= kRegTile && p->g.tile[1] <= kRegTile &&
-                p->g.tile[2] <= kRegTile && c.nch > 16) {
-                // register-tile form: 32 channels per CTA, no shared atomics
-                const int nchunks = (c.nch + 31) / 32;
-                return wmv == 1 ? launch_spread_reg3_t<1>(S, nitems, nchunks, s)
-                                : (wmv == 4 ? launch_spread_reg3_t<4>(S, nitems, nchunks, s)
-                                            : launch_spread_reg3_t<8>(S, nitems, nchunks, s));
+                p->g.tile[2] <= kRegTile) {
+                // register-tile form: channels in groups of 8, 16 or 32 per block, no
+                // shared atomics
+                return wmv == 1 ? launch_spread_reg3_w<1>(S, nitems, c.nch, s)
+                                : (wmv == 4 ? launch_spread_reg3_w<4>(S, nitems, c.nch, s)
+                                            : launch_spread_reg3_w<8>(S, nitems, c.nch, s));
             }
             const size_t smem = spread_smem(p, S.cw);
             const int nchunks = (c.nch + S.cw - 1) / S.cw;
