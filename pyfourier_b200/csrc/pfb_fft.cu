@@ -43,13 +43,13 @@ constexpr int kStreams = kThreads / kCols;        // load / store: 16 lanes per 
 constexpr int kPairStreams = kThreads / (kCols / 2);  // butterflies: a thread takes 2 columns
 constexpr int kMaxN = 512;                // longest axis handled here (else the library FFT)
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex add / subtract / scale-and-add as packed (re, im) FP32 instructions: the
+// same roundings as the componentwise forms (a - b is b * -1 + a, the product exact).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 // -i * a
 __device__ __forceinline__ float2 cmi(float2 a) { return make_float2(a.y, -a.x); }
-__device__ __forceinline__ float2 caxpy(float s, float2 a, float2 y) {
-    return make_float2(fmaf(s, a.x, y.x), fmaf(s, a.y, y.y));
-}
+__device__ __forceinline__ float2 caxpy(float s, float2 a, float2 y) { return __ffma2_rn(make_float2(s, s), a, y); }
 
 // forward r-point DFTs, b_k = sum_q a_q exp(-2 pi i q k / r), in place
 template <int R>
