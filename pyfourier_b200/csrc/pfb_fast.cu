@@ -446,12 +446,13 @@ __device__ __forceinline__ void build_tap_list(const InterpIL &P, const float *s
 }
 
 template <int D, int WM, bool WIDE>
-__global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const InterpIL P) {
+__global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const InterpIL P) {
     constexpr int NT = ipow<D>(WM);
     // up to 64 taps the weights are kept as (w, w) pairs for FFMA2 and, with one
     // channel per lane, the gather loop takes 4 taps per 16-byte offset load
     constexpr bool PAIRS = NT <= 64;
     constexpr bool VEC = PAIRS && NT % 4 == 0;
+    constexpr bool VEC16 = PAIRS && NT % 16 == 0;
     using WT = typename std::conditional<PAIRS, float2, float>::type;
     __shared__ float s_w[kTileWarps][3 * WM];
     __shared__ int s_p[kTileWarps][3 * WM];
@@ -476,7 +477,31 @@ __global__ void __launch_bounds__(kTileWarps * 32) interp_il_kernel(const Interp
             const int c = c0 + cl;
             const float2 *Gc = G + (c < nch ? c : nch - 1);  // in-bounds address; result discarded
             float2 acc = make_float2(0.f, 0.f);
-            if (VEC && tg_n == 1) {
+            if (VEC16 && tg_n == 1) {
+                // 16 gathers issued before their sums (more loads in flight per warp);
+                // taps summed in order 0, 1, 2, ...: the same sums as the loops below
+                const int4 *o4 = reinterpret_cast<const int4 *>(s_off[warp]);
+                const float4 *w4 = reinterpret_cast<const float4 *>(s_wt[warp]);
+                for (int t16 = 0; t16 < NT / 16; ++t16) {
+                    float2 v[16];
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) {
+                        const int4 o = o4[4 * t16 + g];
+                        const int oo[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            v[4 * g + u] = WIDE ? __ldg(Gc + (int64_t)oo[u] * nch) : __ldg(Gc + oo[u]);
+                    }
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) {
+                        const float4 wa = w4[2 * (4 * t16 + g)], wb = w4[2 * (4 * t16 + g) + 1];
+                        acc = __ffma2_rn(make_float2(wa.x, wa.y), v[4 * g + 0], acc);
+                        acc = __ffma2_rn(make_float2(wa.z, wa.w), v[4 * g + 1], acc);
+                        acc = __ffma2_rn(make_float2(wb.x, wb.y), v[4 * g + 2], acc);
+                        acc = __ffma2_rn(make_float2(wb.z, wb.w), v[4 * g + 3], acc);
+                    }
+                }
+            } else if (VEC && tg_n == 1) {
                 // taps in order 0, 1, 2, ...: the same sums as the loop below
                 const int4 *o4 = reinterpret_cast<const int4 *>(s_off[warp]);
                 const float4 *w4 = reinterpret_cast<const float4 *>(s_wt[warp]);
