@@ -277,6 +277,29 @@ def fp32_roofline(wl, plan, B, ms):
             "unit": "TFLOP/s", "frac": round(achieved / peak, 4), "flops": 8 * taps}
 
 
+def bind_to_gpu_cpus(torch, dev):
+    """Best effort: run this process on the CPUs that NVML reports as local to the GPU,
+    so that the page-locked host buffers of the end-to-end measurement are placed on
+    the GPU's NUMA node (a buffer on the other socket crosses the inter-socket link).
+    Returns the previous affinity (to restore), or None when nothing changed."""
+    try:
+        import pynvml
+
+        p = torch.cuda.get_device_properties(dev)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        pynvml.nvmlInit()
+        h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        masks = pynvml.nvmlDeviceGetCpuAffinity(h, (os.cpu_count() + 63) // 64)
+        before = os.sched_getaffinity(0)
+        cpus = {64 * i + b for i, m in enumerate(masks) for b in range(64) if (m >> b) & 1} & before
+        if not cpus or cpus == before:
+            return None
+        os.sched_setaffinity(0, cpus)
+        return before
+    except Exception:
+        return None
+
+
 def gpu_arm(args, wl, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -327,7 +350,8 @@ def gpu_arm(args, wl, rank, world, local_rank):
         ms = float(t.item())
     value = world * samples_per_step / (ms / 1e3)
 
-    # end to end through the public API with host buffers (pinned)
+    # end to end through the public API with host buffers (pinned), on the GPU's CPUs
+    prev_cpus = bind_to_gpu_cpus(torch, dev)
     x_host = x.cpu().pin_memory()
     # two warm-up calls: the steady state holds two page-locked result buffers of each kind
     for _ in range(2):
@@ -348,6 +372,8 @@ def gpu_arm(args, wl, rank, world, local_rank):
     h2d = x_host.numel() * 8 + yk.numel() * 8
     d2h = yk.numel() * 8 + xa.numel() * 8
     del x_host, yk, xa
+    if prev_cpus is not None:
+        os.sched_setaffinity(0, prev_cpus)
 
     mine_l, all_l = (None, None) if args.no_launch_trace else count_launches(torch, lambda: step(x))
     stages = stage_times(torch, pf, plan, x, max(3, args.steps))
