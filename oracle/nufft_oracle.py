@@ -688,43 +688,73 @@ def _sparse_index(indexes, shape):
     return idx.reshape(ds[0], -1, nd)[..., ::-1], tuple(ds[1:])
 
 
+def dense_to_sparse(dense, idx, basis_adj=None):
+    """_mask/_dense2sparse/_{2,3}D[_subspace].py (``_mask_nb``): gather the sampled grid
+    points.  dense (F, B, *N) (or (K, B, *N) with a basis), idx (F, npts, d) in (z, y, x)
+    order; returns (F, B, npts): sparse[f, b, p] = dense[f, b, idx[f, p]], or
+    sum_k basis_adj[f, k] dense[k, b, idx[f, p]] accumulated over k in order."""
+    dense = np.asarray(dense, np.complex64)
+    F, npts, d = idx.shape
+    B = dense.shape[1]
+    out = np.zeros((F, B, npts), np.complex64)
+    for f in range(F):
+        sel = tuple(idx[f, :, a] for a in range(d))
+        if basis_adj is None:
+            out[f] = dense[f][(slice(None),) + sel]
+        else:
+            for k in range(dense.shape[0]):
+                out[f] += np.complex64(basis_adj[f, k]) * dense[k][(slice(None),) + sel]
+    return out
+
+
+def sparse_to_dense(sparse, idx, shape, basis=None):
+    """_mask/_sparse2dense/_{2,3}D[_subspace].py (``_zerofill_nb``): scatter-add the samples
+    (repeated points add, frame by frame and point by point).  sparse (F, B, npts), idx
+    (F, npts, d) (z, y, x); returns (F, B, *shape), or with basis (K, F) the projection
+    dense[k] += basis[k, f] sparse[f] -> (K, B, *shape)."""
+    sparse = np.asarray(sparse, np.complex64)
+    F, B, npts = sparse.shape
+    d = idx.shape[-1]
+    C = F if basis is None else basis.shape[0]
+    out = np.zeros((C, B, *shape), np.complex64)
+    for c in range(C):
+        for b in range(B):
+            for f in range(F):
+                if basis is None and f != c:
+                    continue
+                sel = tuple(idx[f, :, a] for a in range(d))
+                v = sparse[f, b] if basis is None else np.complex64(basis[c, f]) * sparse[f, b]
+                np.add.at(out[c, b], sel, v)
+    return out
+
+
 def sparse_fftn(image, indexes, shape, basis=None, norm=None):
-    """src/pyfourier/_sparsefft/_sparsefft.py:98-108 + _mask/_dense2sparse: centred FFT,
-    then y[b, f, p] = X[b, f][idx] (or sum_k basis[f, k] X[b, k][idx])."""
+    """src/pyfourier/_sparsefft/_sparsefft.py:98-108: centred FFT, then the masking gather
+    (``dense_to_sparse``; with a basis the adjoint projection sum_k basis[f, k] X[k])."""
     nd = len(shape)
     idx, ds = _sparse_index(indexes, shape)
     F = idx.shape[0]
     X = fft_c(np.asarray(image, np.complex64), nd, norm)
     C = X.shape[-nd - 1] if (basis is not None or F > 1) else 1
     X = X.reshape(-1, C, *shape)
-    out = np.zeros((X.shape[0], F, idx.shape[1]), np.complex64)
-    for f in range(F):
-        sel = tuple(idx[f, :, a] for a in range(nd))
-        if basis is None:
-            out[:, f] = X[:, f if C > 1 else 0][(slice(None),) + sel]
-        else:
-            out[:, f] = np.einsum("k,bkp->bp", np.asarray(basis)[f], X[(slice(None), slice(None)) + sel])
-    return out
+    if basis is None and C == 1 and F > 1:
+        X = np.broadcast_to(X, (X.shape[0], F, *shape))
+    dense = np.ascontiguousarray(np.swapaxes(X, 0, 1))  # (C, B, *N)
+    out = dense_to_sparse(dense, idx, None if basis is None else np.asarray(basis, np.complex64))
+    return np.ascontiguousarray(np.swapaxes(out, 0, 1))  # (B, F, npts)
 
 
 def sparse_ifftn(kspace, indexes, shape, basis=None, norm=None):
-    """src/pyfourier/_sparsefft/_sparsefft.py:111-121 + _mask/_sparse2dense: scatter-add
-    (duplicates add; basis conj-transposed), then the centred inverse FFT."""
+    """src/pyfourier/_sparsefft/_sparsefft.py:111-121: the masking scatter-add
+    (``sparse_to_dense``; with a basis the conj-transposed projection), then the centred
+    inverse FFT."""
     nd = len(shape)
     idx, ds = _sparse_index(indexes, shape)
     F = idx.shape[0]
     y = np.asarray(kspace, np.complex64).reshape(-1, F, idx.shape[1])
-    C = np.asarray(basis).shape[1] if basis is not None else F
-    grid = np.zeros((y.shape[0], C, *shape), np.complex64)
-    for f in range(F):
-        sel = tuple(idx[f, :, a] for a in range(nd))
-        for b in range(y.shape[0]):
-            if basis is None:
-                np.add.at(grid[b, f], sel, y[b, f])
-            else:
-                for k in range(C):
-                    np.add.at(grid[b, k], sel, np.conj(np.asarray(basis)[f, k]) * y[b, f])
-    return ifft_c(grid, nd, norm)
+    bt = None if basis is None else np.ascontiguousarray(np.asarray(basis, np.complex64).conj().T)
+    grid = sparse_to_dense(np.ascontiguousarray(np.swapaxes(y, 0, 1)), idx, tuple(shape), bt)
+    return ifft_c(np.ascontiguousarray(np.swapaxes(grid, 0, 1)), nd, norm)
 
 
 # --------------------------------------------------------------------------------------

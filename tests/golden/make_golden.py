@@ -17,6 +17,8 @@ Kernels exercised (paths inside the pyfourier project):
       _prepare_interpolator_nb
   _subroutines/_grid/_noncart2cart/_{1,2,3}D[_subspace].py: _grid_nb
   _subroutines/_grid/_cart2noncart/_{1,2,3}D[_subspace].py: _degrid_nb
+  _subroutines/_mask/_dense2sparse/_{2,3}D[_subspace].py: _mask_nb
+  _subroutines/_mask/_sparse2dense/_{2,3}D[_subspace].py: _zerofill_nb
 
 The inputs are seeded; coordinates are scaled onto the oversampled grid with
 the float32 arithmetic of _subroutines/_traj.py:57-65 before the table build,
@@ -55,6 +57,11 @@ def load_reference_kernels():
         _stub_package(
             "pyfourier._subroutines._grid." + d, os.path.join(root, "_subroutines", "_grid", d)
         )
+    _stub_package("pyfourier._subroutines._mask", os.path.join(root, "_subroutines", "_mask"))
+    for d in ("_dense2sparse", "_sparse2dense"):
+        _stub_package(
+            "pyfourier._subroutines._mask." + d, os.path.join(root, "_subroutines", "_mask", d)
+        )
 
     def load(modname, relpath):
         spec = importlib.util.spec_from_file_location(modname, os.path.join(root, relpath))
@@ -74,6 +81,16 @@ def load_reference_kernels():
                 f"pyfourier._subroutines._grid._cart2noncart._{d}D{sfx}",
                 f"_subroutines/_grid/_cart2noncart/_{d}D{sfx}.py",
             )._degrid["cpu"]
+    for d in (2, 3):
+        for sfx in ("", "_subspace"):
+            k[f"mask{d}{sfx}"] = load(
+                f"pyfourier._subroutines._mask._dense2sparse._{d}D{sfx}",
+                f"_subroutines/_mask/_dense2sparse/_{d}D{sfx}.py",
+            )._mask["cpu"]
+            k[f"zerofill{d}{sfx}"] = load(
+                f"pyfourier._subroutines._mask._sparse2dense._{d}D{sfx}",
+                f"_subroutines/_mask/_sparse2dense/_{d}D{sfx}.py",
+            )._zerofill["cpu"][True]
     return k
 
 
@@ -191,6 +208,30 @@ def main():
         })
         for a in range(d):
             out[p + f"index{a}"], out[p + f"value{a}"] = idx[a], val[a]
+
+    # 4. Cartesian masking kernels (sparse FFT gather / scatter-add), 2D and 3D, plain
+    # and subspace; a separate seeded generator keeps the arrays above unchanged
+    mrng = np.random.default_rng(20240608)
+    for d, (N_zyx, F, B, npts, K) in {2: ((12, 16), 3, 2, 40, 2), 3: ((6, 8, 10), 2, 2, 50, 3)}.items():
+        idx = np.stack([mrng.integers(0, n, (F, npts)) for n in N_zyx], -1).astype(np.int32)  # (F, npts, d) z, y, x
+        idx[0, :6] = idx[0, 6]  # repeated points: the scatter adds them
+        index = tuple(np.ascontiguousarray(idx[..., a]) for a in range(d))
+        dense = (mrng.standard_normal((F, B, *N_zyx)) + 1j * mrng.standard_normal((F, B, *N_zyx))).astype(np.complex64)
+        sparse = np.zeros((F, B, npts), np.complex64)
+        k[f"mask{d}"](sparse, dense, index)
+        ksp = (mrng.standard_normal((F, B, npts)) + 1j * mrng.standard_normal((F, B, npts))).astype(np.complex64)
+        fill = np.zeros((F, B, *N_zyx), np.complex64)
+        k[f"zerofill{d}"](fill, ksp, index)
+        basis = (mrng.standard_normal((F, K)) + 1j * mrng.standard_normal((F, K))).astype(np.complex64)
+        dense_s = (mrng.standard_normal((K, B, *N_zyx)) + 1j * mrng.standard_normal((K, B, *N_zyx))).astype(np.complex64)
+        sparse_s = np.zeros((F, B, npts), np.complex64)
+        k[f"mask{d}_subspace"](sparse_s, dense_s, index, basis)  # basis_adjoint (F, K)
+        fill_s = np.zeros((K, B, *N_zyx), np.complex64)
+        k[f"zerofill{d}_subspace"](fill_s, ksp, index, np.ascontiguousarray(basis.conj().T))  # basis (K, F)
+        p = f"m{d}d_"
+        out.update({p + "shape": np.array(N_zyx, np.int32), p + "index": idx, p + "dense": dense,
+                    p + "sparse": sparse, p + "ksp": ksp, p + "fill": fill, p + "basis": basis,
+                    p + "dense_sub": dense_s, p + "sparse_sub": sparse_s, p + "fill_sub": fill_s})
 
     path = os.path.join(HERE, "kernels.npz")
     np.savez_compressed(path, **out)

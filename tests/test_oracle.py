@@ -322,3 +322,17 @@ def test_oracle_grog_exact_on_shift_invariant_calibration(ndim):
     flat = (ind * np.array([1, 16, 256])[:ndim]).sum(-1).ravel()
     cnt = np.array([np.sum(flat == f) for f in flat])
     np.testing.assert_allclose(w.ravel(), 1.0 / cnt)
+
+
+@pytest.mark.parametrize("d", [2, 3])
+def test_masking_kernels_match_reference(golden, d):
+    """The oracle's gather / scatter-add (the sparse FFT's masking step) against outputs
+    of the reference's own _dense2sparse / _sparse2dense Numba kernels: gathers exact,
+    sums within float32 rounding (the reference compiles with fastmath)."""
+    p = f"m{d}d_"
+    idx, shape, basis = golden[p + "index"], tuple(golden[p + "shape"]), golden[p + "basis"]
+    np.testing.assert_array_equal(orc.dense_to_sparse(golden[p + "dense"], idx), golden[p + "sparse"])
+    assert orc.rel_l2(orc.sparse_to_dense(golden[p + "ksp"], idx, shape), golden[p + "fill"]) < 1e-6
+    assert orc.rel_l2(orc.dense_to_sparse(golden[p + "dense_sub"], idx, basis), golden[p + "sparse_sub"]) < 1e-6
+    fill_s = orc.sparse_to_dense(golden[p + "ksp"], idx, shape, np.ascontiguousarray(basis.conj().T))
+    assert orc.rel_l2(fill_s, golden[p + "fill_sub"]) < 1e-6
