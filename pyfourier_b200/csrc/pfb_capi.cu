@@ -2,6 +2,10 @@
 #include <cmath>
 #include <cstring>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "pfb_common.cuh"
 
 namespace pfb {
@@ -9,6 +13,19 @@ namespace pfb {
 static thread_local std::string g_last_error;
 
 void set_error(const std::string &msg) { g_last_error = msg; }
+
+int raise_smem_limit(const void *kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> granted;
+    int dev = 0;
+    PFB_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    size_t &g = granted[{kernel, dev}];
+    if (g >= bytes) return PFB_OK;
+    PFB_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    g = bytes;
+    return PFB_OK;
+}
 
 int fail(int code, const std::string &msg) {
     g_last_error = msg;

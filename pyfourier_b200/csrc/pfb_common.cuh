@@ -44,6 +44,17 @@ int fail(int code, const std::string &msg);
 
 #define PFB_CHECK_LAUNCH() PFB_CUDA_TRY(cudaGetLastError())
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the current
+// device.  The attribute stays with the context, so each (kernel, device) pays the
+// driver call once; later launches only look it up.
+int raise_smem_limit(const void *kernel, size_t bytes);
+#define PFB_RAISE_SMEM(kernel, bytes) PFB_TRY_ST_RAISE(::pfb::raise_smem_limit((const void *)(kernel), (size_t)(bytes)))
+#define PFB_TRY_ST_RAISE(expr)        \
+    do {                               \
+        int _st = (expr);              \
+        if (_st) return _st;           \
+    } while (0)
+
 // Per-axis geometry, x-first.
 struct Geom {
     int ndim;

@@ -565,7 +565,7 @@ int launch_col(const ColPass &P, cudaStream_t s) {
     vec = vec && (img_in || img_out ? P.nvol % 2 == 0 : true);
     vec = vec && (img_in ? true : P.in_plane % 2 == 0) && (img_out ? true : P.out_plane % 2 == 0);
     auto k = vec ? col_pass_kernel<true> : col_pass_kernel<false>;
-    PFB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PFB_RAISE_SMEM(k, (int)smem);
     k<<<(unsigned)blocks, kThreads, smem, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
@@ -577,7 +577,7 @@ int launch_row(const RowPass &P, bool inv, cudaStream_t s) {
     if (blocks >= (1LL << 31)) return fail(PFB_ERR_UNSUPPORTED, "too many vectors for the fused FFT");
     const size_t smem = row_smem(P.fa.n);
     auto k = inv ? row_inv_kernel : row_fwd_kernel;
-    PFB_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PFB_RAISE_SMEM(k, (int)smem);
     k<<<(unsigned)blocks, kThreads, smem, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;

@@ -435,8 +435,7 @@ int pfb_grog_apply(pfb_grog *g, const void *in, void *out, int64_t batch, void *
         const int ncs = (g->nc + 1) & ~1;
         if (g->nc <= 32) {
             const size_t sm = 2 * (size_t)kChunk * ncs * sizeof(float2);
-            PFB_CUDA_TRY(cudaFuncSetAttribute(grog_apply_reg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)(2 * kChunk * 32 * sizeof(float2))));
+            PFB_RAISE_SMEM(grog_apply_reg_kernel, (int)(2 * kChunk * 32 * sizeof(float2)));
             const int64_t nv = (int64_t)g->nchunks * batch;
             const unsigned nblk = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nv, 2LL * g->nsm));
             grog_apply_reg_kernel<<<nblk, 256, sm, s>>>(g->d_chunks, g->nchunks, g->d_G, g->nc, g->nslices, g->Mk,
@@ -444,9 +443,8 @@ int pfb_grog_apply(pfb_grog *g, const void *in, void *out, int64_t batch, void *
         } else {
             const size_t sm = ((size_t)kChunk * ncs + (size_t)g->nc * g->nc) * sizeof(float2);
             // 64 coils need 96 KB of dynamic shared memory
-            PFB_CUDA_TRY(cudaFuncSetAttribute(grog_apply_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)(((size_t)kChunk * kMaxCoils + kMaxCoils * kMaxCoils) *
-                                                    sizeof(float2))));
+            PFB_RAISE_SMEM(grog_apply_smem_kernel, (int)(((size_t)kChunk * kMaxCoils + kMaxCoils * kMaxCoils) *
+                                                    sizeof(float2)));
             const dim3 agrid((unsigned)g->nchunks, ytiles(batch));
             grog_apply_smem_kernel<<<agrid, 256, sm, s>>>(g->d_chunks, g->d_G, g->nc, g->nslices, g->Mk, batch,
                                                           rows);
