@@ -1238,7 +1238,7 @@ int launch_spread_reg3_w(const SpreadIL &P, int nitems, int nch, cudaStream_t s)
 template <int D, int WM>
 int launch_spread_il_t(const SpreadIL &P, int nitems, int nchunks, size_t smem, cudaStream_t s) {
     auto k = spread_il_kernel<D, WM>;
-    if (smem > 48 * 1024) PFB_RAISE_SMEM(k, (int)smem);
+    PFB_RAISE_SMEM(k, (int)smem);
     dim3 grid(nitems, nchunks);
     k<<<grid, kSpreadWarps * 32, smem, s>>>(P);
     PFB_CHECK_LAUNCH();
@@ -1466,16 +1466,14 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
                 O.src = samp;
                 O.dst = static_cast<float2 *>(dst);
                 size_t smem = (size_t)kOutRows * c.nch * sizeof(float2);
-                if (smem > 48 * 1024)
-                    PFB_RAISE_SMEM(out_il_kernel, (int)smem);
+                PFB_RAISE_SMEM(out_il_kernel, (int)smem);
                 out_il_kernel<<<blocks, 256, smem, s>>>(O);
             } else {
                 O.src = static_cast<const float2 *>(src);
                 O.dst = samp;
                 O.factors = 1;
                 size_t smem = (size_t)kOutRows * c.B * sizeof(float2);
-                if (smem > 48 * 1024)
-                    PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
+                PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
                 vals_il_kernel<<<blocks, 256, smem, s>>>(O);
             }
             PFB_CHECK_LAUNCH();
@@ -1585,7 +1583,7 @@ int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const flo
     V.dst = samp;
     V.factors = 0;
     size_t smem = (size_t)kOutRows * c.B * sizeof(float2);
-    if (smem > 48 * 1024) PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
+    PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
     vals_il_kernel<<<(unsigned)((p->mtot + kOutRows - 1) / kOutRows), 256, smem, s>>>(V);
     PFB_CHECK_LAUNCH();
     InterpIL Q{};

@@ -182,7 +182,7 @@ template <int D, int WM>
 int launch_spread_t(const SpreadParams &P, int nitems, int threads, size_t smem, cudaStream_t s) {
     int nchg = (P.nch_total + P.nch - 1) / P.nch;
     auto kern = spread_kernel<D, WM>;
-    if (smem > 48 * 1024) PFB_RAISE_SMEM(kern, (int)smem);
+    PFB_RAISE_SMEM(kern, (int)smem);
     dim3 grid(nitems, nchg);
     kern<<<grid, threads, smem, s>>>(P);
     PFB_CHECK_LAUNCH();

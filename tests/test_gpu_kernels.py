@@ -154,7 +154,8 @@ def _pipeline_both(plan, x, y, basis=None, zs=None, zt=None, L=1):
 
 
 @pytest.mark.parametrize("case", ["2d_coils", "2d_frames", "3d", "basis", "b0", "3d_w6_odd", "2d_single_tile",
-                                  "2d_single_tile_32ch", "3d_w6_32ch", "1d_32ch"])
+                                  "2d_single_tile_32ch", "3d_w6_32ch", "1d_32ch", "3d_12ch", "3d_single_tile",
+                                  "3d_b0_basis"])
 def test_interleaved_pipeline_matches_planar(case):
     rng = np.random.default_rng(21)
     crn = lambda *s: torch.as_tensor((rng.standard_normal(s) + 1j * rng.standard_normal(s)).astype(np.complex64)).cuda()  # noqa: E731
@@ -202,6 +203,27 @@ def test_interleaved_pipeline_matches_planar(case):
         coord = ((rng.random((1, 20, 50, 3)) - 0.5) * np.array([19, 21, 17])).astype(np.float32)
         plan = _plan(coord, N, (2.0, 1.5, 2.0), (6, 5, 7))
         _pipeline_both(plan, crn(5, 1, *N), crn(5, 20 * 50))
+    elif case == "3d_12ch":
+        N = (24, 22, 20)
+        coord = ((rng.random((1, 40, 60, 3)) - 0.5) * np.array([20, 22, 24])).astype(np.float32)
+        plan = _plan(coord, N, (1.25, 1.25, 1.25), (4, 4, 4))
+        _pipeline_both(plan, crn(12, 1, *N), crn(12, 40 * 60))
+    elif case == "3d_single_tile":
+        # a 6^3 image at osf 1.25 is an 8^3 grid, one tile: taps wrap around inside it on every axis
+        N = (6, 6, 6)
+        coord = np.concatenate([((rng.random((1, 1, 50, 3)) - 0.5) * 6),
+                                np.full((1, 1, 3, 3), -3.0), np.full((1, 1, 3, 3), 2.95)], axis=2).astype(np.float32)
+        plan = _plan(coord, N, (1.25, 1.25, 1.25), (4, 4, 4))
+        _pipeline_both(plan, crn(3, 1, *N), crn(3, 56))
+    elif case == "3d_b0_basis":
+        # 3D subspace with B0 segments: channels = segments x batch x coefficients = 12
+        N = (16, 18, 20)
+        F, K, Lseg = 4, 2, 3
+        coord = ((rng.random((F, 6, 40, 3)) - 0.5) * np.array([20, 18, 16])).astype(np.float32)
+        plan = _plan(coord, N, (1.25, 1.25, 1.25), (4, 4, 4))
+        zt = crn(Lseg, 40)
+        zs = crn(Lseg, 16 * 18 * 20)
+        _pipeline_both(plan, crn(2, K, *N), crn(2, F * 6 * 40), basis=crn(F, K), zs=zs, zt=zt, L=Lseg)
     elif case == "basis":
         N = (32, 32)
         F, K = 6, 3

@@ -120,6 +120,17 @@ def test_crowded_3d_tiles_with_many_channels():
     check_pair(coord, (N, N, N), crandn(rng, 33, N, N, N), crandn(rng, 33, 1, 6500), width=6, oversamp=2.0)
 
 
+@pytest.mark.parametrize("nch", [3, 8, 12, 16])
+def test_3d_channel_groups(nch):
+    """3D spreads take register tiles in channel groups of 8 (<= 8 channels), 16 (9-16)
+    or 32 per lane group; every group size against the oracle, with crowded tiles."""
+    rng = np.random.default_rng(40 + nch)
+    N = 20
+    coord = ((rng.random((1, 30, 90, 3)) - 0.5) * N).astype(np.float32)
+    coord[0, :3] *= 0.05  # crowd the centre tiles
+    check_pair(coord, (N, N, N), crandn(rng, nch, N, N, N), crandn(rng, nch, 30, 90), width=4, oversamp=1.25)
+
+
 def test_multiframe_and_weights():
     rng = np.random.default_rng(6)
     N, F = 40, 3
