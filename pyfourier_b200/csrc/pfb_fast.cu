@@ -249,19 +249,33 @@ struct SampIL {
     float2 *dst;        // vals_il: vals [M][nch];   out_il: k-space (B, M)
     int factors;        // vals_il: apply conj(tB) conj(basis) (1) or only the weight (0)
     int accumulate;
+    int rows;           // samples per CTA (kOutRows .. kMaxOutRows)
 };
 
-// Both transposes walk the samples in their original order, kOutRows per CTA,
-// so the k-space side is read / written coalesced and the sorted side moves
-// whole rows of nch channels (iperm: original -> sorted position).
+constexpr int kMaxOutRows = 128;
+
+// samples per CTA of a transpose whose wider side has `width` float2 per sample:
+// as many as fit about 32 KB of shared memory, between kOutRows and kMaxOutRows
+inline int out_rows(int width) {
+    int r = kOutRows;
+    while (r < kMaxOutRows && (size_t)(2 * r) * width * sizeof(float2) <= 32 * 1024) r *= 2;
+    return r;
+}
+
+// Both transposes walk the samples in their original order, P.rows per CTA, so
+// the k-space side is read / written coalesced and the sorted side moves whole
+// rows of nch channels (iperm: original -> sorted position, staged once per CTA).
 
 // vals[iperm[g]][ch] = y[b][g] * w[g] * conj(B_l(t)) * conj(basis[f, k])
 __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
-    extern __shared__ float2 sm[];  // [32][B]
-    const int64_t g0 = (int64_t)blockIdx.x * kOutRows;
+    extern __shared__ float2 sm[];  // [rows][B]
+    __shared__ int s_j[kMaxOutRows];
+    const int R = P.rows;
+    const int64_t g0 = (int64_t)blockIdx.x * R;
     const int B = P.ch.B;
-    for (int e = threadIdx.x; e < kOutRows * B; e += blockDim.x) {
-        const int b = e / kOutRows, gg = e - b * kOutRows;
+    for (int gg = threadIdx.x; gg < R; gg += blockDim.x) s_j[gg] = g0 + gg < P.mtot ? P.iperm[g0 + gg] : 0;
+    for (int e = threadIdx.x; e < R * B; e += blockDim.x) {
+        const int b = e / R, gg = e - b * R;
         const int64_t g = g0 + gg;
         float2 v = make_float2(0.f, 0.f);
         if (g < P.mtot) {
@@ -276,11 +290,11 @@ __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
     }
     __syncthreads();
     const int nch = P.ch.nch, Kc = P.ch.K ? P.ch.K : 1;
-    for (int e = threadIdx.x; e < kOutRows * nch; e += blockDim.x) {
+    for (int e = threadIdx.x; e < R * nch; e += blockDim.x) {
         const int gg = e / nch, c = e - gg * nch;
         const int64_t g = g0 + gg;
         if (g >= P.mtot) continue;
-        const int64_t j = P.iperm[g];
+        const int64_t j = s_j[gg];
         const int k = c % Kc, lb = c / Kc, b = lb % B, l = lb / B;
         float2 v = sm[gg * B + b];
         if (P.factors && (P.tB || P.ch.K)) {
@@ -297,25 +311,29 @@ __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
 
 // y[b][g] (+)= w[g] * sum_{l,k} B_l(t) basis[f, k] res[iperm[g]][(l, b, k)]
 __global__ void __launch_bounds__(256) out_il_kernel(const SampIL P) {
-    extern __shared__ float2 sm[];  // [32][nch]
-    const int64_t g0 = (int64_t)blockIdx.x * kOutRows;
+    extern __shared__ float2 sm[];  // [rows][nch]
+    __shared__ int s_j[kMaxOutRows];
+    const int R = P.rows;
+    const int64_t g0 = (int64_t)blockIdx.x * R;
     const int nch = P.ch.nch;
-    for (int e = threadIdx.x; e < kOutRows * nch; e += blockDim.x) {
+    for (int gg = threadIdx.x; gg < R; gg += blockDim.x) s_j[gg] = g0 + gg < P.mtot ? P.iperm[g0 + gg] : 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < R * nch; e += blockDim.x) {
         const int gg = e / nch, c = e - gg * nch;
         const int64_t g = g0 + gg;
-        sm[e] = g < P.mtot ? P.src[(int64_t)P.iperm[g] * nch + c] : make_float2(0.f, 0.f);
+        sm[e] = g < P.mtot ? P.src[(int64_t)s_j[gg] * nch + c] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     const int B = P.ch.B, L = P.ch.L, Kc = P.ch.K ? P.ch.K : 1;
-    for (int e = threadIdx.x; e < kOutRows * B; e += blockDim.x) {
-        const int b = e / kOutRows, gg = e - b * kOutRows;
+    for (int e = threadIdx.x; e < R * B; e += blockDim.x) {
+        const int b = e / R, gg = e - b * R;
         const int64_t g = g0 + gg;
         if (g >= P.mtot) continue;
         float2 acc = make_float2(0.f, 0.f);
         if (L == 1 && !P.ch.K) {
             acc = sm[gg * nch + b];
         } else {
-            const int f = P.sframe[P.iperm[g]];
+            const int f = P.sframe[s_j[gg]];
             const int t = P.tB ? (int)((g - P.frame_off[f]) % P.readout) : 0;
             for (int l = 0; l < L; ++l) {
                 float2 accl = make_float2(0.f, 0.f);
@@ -1461,18 +1479,19 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             O.tB = d.b0_time;
             O.ch = c;
             O.accumulate = accumulate ? 1 : 0;
-            const unsigned blocks = (unsigned)((p->mtot + kOutRows - 1) / kOutRows);
+            O.rows = out_rows(std::max(c.nch, c.B));
+            const unsigned blocks = (unsigned)((p->mtot + O.rows - 1) / O.rows);
             if (stage == PFB_STAGE_OUT) {
                 O.src = samp;
                 O.dst = static_cast<float2 *>(dst);
-                size_t smem = (size_t)kOutRows * c.nch * sizeof(float2);
+                size_t smem = (size_t)O.rows * c.nch * sizeof(float2);
                 PFB_RAISE_SMEM(out_il_kernel, (int)smem);
                 out_il_kernel<<<blocks, 256, smem, s>>>(O);
             } else {
                 O.src = static_cast<const float2 *>(src);
                 O.dst = samp;
                 O.factors = 1;
-                size_t smem = (size_t)kOutRows * c.B * sizeof(float2);
+                size_t smem = (size_t)O.rows * c.B * sizeof(float2);
                 PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
                 vals_il_kernel<<<blocks, 256, smem, s>>>(O);
             }
@@ -1582,9 +1601,10 @@ int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const flo
     V.src = vals;
     V.dst = samp;
     V.factors = 0;
-    size_t smem = (size_t)kOutRows * c.B * sizeof(float2);
+    V.rows = out_rows(std::max(c.nch, c.B));
+    size_t smem = (size_t)V.rows * c.B * sizeof(float2);
     PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
-    vals_il_kernel<<<(unsigned)((p->mtot + kOutRows - 1) / kOutRows), 256, smem, s>>>(V);
+    vals_il_kernel<<<(unsigned)((p->mtot + V.rows - 1) / V.rows), 256, smem, s>>>(V);
     PFB_CHECK_LAUNCH();
     InterpIL Q{};
     fill_interp(p, c, Q);
