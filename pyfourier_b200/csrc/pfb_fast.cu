@@ -421,17 +421,6 @@ __device__ __forceinline__ void warp_taps(const InterpIL &P, int64_t j, float *s
     }
 }
 
-// The same from the plan's per-sample taps: weights as stored, positions from
-// the first tap x0 mod n_os.
-template <int D, int WM>
-__device__ __forceinline__ void warp_taps_plan(const InterpIL &P, int64_t j, float *sw, int *sp, int lane) {
-    if (lane < D * WM) {
-        const int a = lane / WM, i = lane - a * WM;
-        sw[lane] = P.wtap[j * (D * WM) + lane];
-        sp[lane] = pmod((long long)P.xtap[j * D + a] + i - P.g.sh[a], P.g.nos[a]);
-    }
-}
-
 template <int D>
 __host__ __device__ constexpr int ipow(int b) { return D == 1 ? b : (D == 2 ? b * b : b * b * b); }
 
@@ -484,10 +473,30 @@ __global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const Int
     // from the same few tiles, which stay in L1
     const int64_t per = (P.mtot + gridDim.x - 1) / gridDim.x;
     const int64_t jbeg = (int64_t)blockIdx.x * per, jend = min(P.mtot, jbeg + per);
+    // the plan taps (weights, first taps) and frame of the warp's next sample are
+    // loaded into registers while the current sample gathers
+    constexpr int DW = D * WM;
+    float pw = 0.f;
+    int px = 0, pf = 0;
+    auto fetch = [&](int64_t jj) {
+        if (jj < jend) {
+            if (lane < DW) {
+                pw = P.wtap[jj * DW + lane];
+                px = P.xtap[jj * D + lane / WM];
+            }
+            pf = P.ch.K ? 0 : P.sframe[jj];
+        }
+    };
+    fetch(jbeg + warp);
     for (int64_t j = jbeg + warp; j < jend; j += kTileWarps) {
-        warp_taps_plan<D, WM>(P, j, s_w[warp], s_p[warp], lane);
+        if (lane < DW) {  // weights as stored, positions from the first tap x0 mod n_os
+            const int a = lane / WM, i = lane - a * WM;
+            s_w[warp][lane] = pw;
+            s_p[warp][lane] = pmod((long long)px + i - P.g.sh[a], P.g.nos[a]);
+        }
+        const int grp = pf;
+        fetch(j + kTileWarps);
         __syncwarp();
-        const int grp = P.ch.K ? 0 : P.sframe[j];
         const float2 *G = P.grid + (int64_t)grp * P.g.gvol * nch;
         build_tap_list<D, WM, WIDE>(P, s_w[warp], s_p[warp], nch, s_off[warp], s_wt[warp], lane);
         __syncwarp();
