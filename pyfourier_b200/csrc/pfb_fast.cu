@@ -1162,6 +1162,193 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
     }
 }
 
+// Register-tile spread for 2D tiles of up to 16 x 16 points: the 2D form of
+// spread_reg3_kernel.  Eight blocks of 4 (x) x 8 (y) points tile the packed
+// 16 x 16 tile; a lane group of CPW channels owns one block, its 32 points x
+// its lane's channel in registers (no atomics), so a CTA has 8 / (32 / CPW)
+// warps and 2 (32 channels), 3 (16) or 4 (8) CTAs share an SM.  A sample's tile
+// weights are 16 x-weights and 16 y-weights (lanes (axis, t) build them), its
+// occupancy mask holds x in bits 0..15 and y in bits 16..31.
+constexpr int kReg2Tile = 16;
+constexpr int kReg2Pts = kReg2Tile * kReg2Tile;
+template <int CPW>
+struct Reg2Cfg {
+    static constexpr int G = 32 / CPW;
+    static constexpr int NW = 8 / G;
+    static constexpr int MinBlocks = CPW == 32 ? 2 : (CPW == 16 ? 3 : 4);
+    static constexpr int Batch = CPW == 32 ? 96 : (CPW == 16 ? 96 : 80);
+    static constexpr size_t OffW = (size_t)Batch * CPW * sizeof(float2);
+    static constexpr size_t OffX = OffW + (size_t)Batch * 16 * sizeof(float);
+    static constexpr size_t OffD = OffX + (size_t)Batch * 4 * sizeof(int);
+    static constexpr size_t Buf = OffD + (size_t)Batch * sizeof(int);
+    static constexpr size_t OffTW = 2 * Buf;
+    static constexpr size_t OffM = OffTW + (size_t)Batch * 32 * sizeof(float2);
+    static constexpr size_t Stage = OffM + (size_t)Batch * sizeof(unsigned);
+    static constexpr size_t Out = (size_t)kReg2Pts * (CPW + 1) * sizeof(float2);
+    static constexpr size_t Smem = kReg2Pts * sizeof(int) + (Out > Stage ? Out : Stage);
+    static_assert(Buf % 16 == 0 && OffTW % 16 == 0, "16-byte aligned staging arrays");
+    static_assert(Smem * MinBlocks + MinBlocks * 1024 <= 228 * 1024, "shared memory of the CTAs of one SM");
+};
+
+template <int WM, int CPW>
+__global__ void __launch_bounds__(Reg2Cfg<CPW>::NW * 32, Reg2Cfg<CPW>::MinBlocks)
+    spread_reg2_kernel(const SpreadIL P) {
+    using C = Reg2Cfg<CPW>;
+    constexpr int G = C::G, NW = C::NW;
+    constexpr int D = 2, DW = D * WM;
+    static_assert(DW <= 16, "raw weights of one sample fit 16 entries");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    int *s_pos = reinterpret_cast<int *>(smraw);
+    unsigned char *ub = smraw + kReg2Pts * sizeof(int);
+    float2 *s_out = reinterpret_cast<float2 *>(ub);  // [8 blocks x 32 points][CPW + 1], after the last batch
+    constexpr int NR = 9;
+    __shared__ int s_pre[NR + 1];
+    __shared__ int s_beg[NR];
+    __shared__ int s_dlt[NR];
+    const OwnerItem it = P.items[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nch = P.ch.nch;
+    const int cl = lane % CPW, grpl = lane / CPW;
+    const int c0 = blockIdx.y * CPW, c = c0 + cl;
+    int org[2], text[2], wrap[2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const int tc = tile_coord(it.tile, a, P.g);
+        org[a] = tc * P.g.tile[a];
+        text[a] = min(P.g.tile[a], P.g.nos[a] - org[a]);
+        wrap[a] = P.g.nbins[a] == 1 ? text[a] : 0;
+    }
+    for (int pt = threadIdx.x; pt < kReg2Pts; pt += blockDim.x) {
+        const int t0 = pt & 15, t1 = pt >> 4;
+        int pos = -1;
+        if (t0 < text[0] && t1 < text[1])
+            pos = pmod(org[0] + t0 - P.g.sh[0], P.g.nos[0]) + pmod(org[1] + t1 - P.g.sh[1], P.g.nos[1]) * P.g.nos[0];
+        s_pos[pt] = pos;
+    }
+    if (warp == 0) neighbour_ranges<2>(P, it, s_pre, s_beg, s_dlt, lane);
+    __syncthreads();
+    const int nvis = it.v1 - it.v0;
+    const int nbat = (nvis + C::Batch - 1) / C::Batch;
+    auto batch_size = [&](int bb) { return (nvis - bb + nbat - 1) / nbat; };
+    auto issue = [&](int bb, int buf) {
+        unsigned char *B = ub + buf * C::Buf;
+        float2 *rv = reinterpret_cast<float2 *>(B);
+        float *rw = reinterpret_cast<float *>(B + C::OffW);
+        int *rx = reinterpret_cast<int *>(B + C::OffX);
+        int *rd = reinterpret_cast<int *>(B + C::OffD);
+        const int nb = batch_size(bb);
+        for (int q = warp; q < nb; q += NW) {
+            const int v = it.v0 + bb + q * nbat;  // batches mix the neighbour ranges
+            const unsigned le = __ballot_sync(0xffffffffu, lane < NR && s_pre[lane] <= v);
+            const int r = 31 - __clz(le);
+            const int64_t j = (int64_t)s_beg[r] + (v - s_pre[r]);
+            if (lane < CPW) cp_async8(rv + q * CPW + lane, P.vals + j * nch + (c < nch ? c : 0), c < nch);
+            if (lane < DW) cp_async4(rw + q * 16 + lane, P.wtap + j * DW + lane);
+            if (lane < D) cp_async4(rx + q * 4 + lane, P.xtap + j * D + lane);
+            if (lane == 0) rd[q] = s_dlt[r];
+        }
+    };
+    // this lane's block: bid = warp * G + group, 4 blocks along x, 2 along y
+    const int bid = warp * G + grpl;
+    const int bx0 = (bid & 3) * 4, by0 = (bid >> 2) * 8;
+    unsigned bmx[G], bmy[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        const int b2 = warp * G + g;
+        bmx[g] = 0xFu << ((b2 & 3) * 4);
+        bmy[g] = 0xFFu << (16 + (b2 >> 2) * 8);
+    }
+    // lane (a, t): tile coordinate t (0..15) on axis a (lanes 0..15 x, 16..31 y)
+    const int la = lane >> 4, lt = lane & 15;
+    const int orga = la == 0 ? org[0] : org[1];
+    const int texta = la == 0 ? text[0] : text[1];
+    const int wrapa = la == 0 ? wrap[0] : wrap[1];
+    const int nosa = la == 0 ? P.g.nos[0] : P.g.nos[1];
+    const int wa = la == 0 ? P.g.w[0] : P.g.w[1];
+    float2 acc[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) acc[q] = make_float2(0.f, 0.f);
+    if (nbat > 0) issue(0, 0);
+    cp_async_commit();
+    for (int b = 0; b < nbat; ++b) {
+        const int cur = b & 1;
+        cp_async_wait_all();
+        __syncthreads();  // batch b landed; every warp is done with batch b - 1
+        if (b + 1 < nbat) issue(b + 1, cur ^ 1);
+        cp_async_commit();
+        unsigned char *B = ub + cur * C::Buf;
+        const float2 *rv = reinterpret_cast<const float2 *>(B);
+        const float *rw = reinterpret_cast<const float *>(B + C::OffW);
+        const int *rx = reinterpret_cast<const int *>(B + C::OffX);
+        const int *rd = reinterpret_cast<const int *>(B + C::OffD);
+        float2 *tw = reinterpret_cast<float2 *>(ub + C::OffTW);
+        unsigned *tm = reinterpret_cast<unsigned *>(ub + C::OffM);
+        const int nb = batch_size(b);
+        for (int q = warp; q < nb; q += NW) {
+            float wv = 0.f;
+            int d = rx[q * 4 + la] - orga;
+            if (((rd[q] >> la) & 1) && d >= 0) d -= nosa;
+            int i = lt - d;
+            if (wrapa && i < 0) i += wrapa;
+            if (lt < texta && i >= 0 && i < wa) wv = rw[q * 16 + la * WM + i];
+            tw[q * 32 + lane] = make_float2(wv, wv);
+            const unsigned m = __ballot_sync(0xffffffffu, wv != 0.f);
+            if (lane == 0) tm[q] = m;
+        }
+        __syncthreads();  // tile weights and masks of batch b ready
+        for (int q0 = 0; q0 < nb; q0 += 32) {
+            bool hit = false;
+            if (q0 + lane < nb) {
+                const unsigned m = tm[q0 + lane];
+#pragma unroll
+                for (int g = 0; g < G; ++g) hit = hit || ((m & bmx[g]) && (m & bmy[g]));
+            }
+            unsigned hm = __ballot_sync(0xffffffffu, hit);
+            while (hm) {
+                const int q = q0 + __ffs(hm) - 1;
+                hm &= hm - 1;
+                const float2 v = rv[q * CPW + cl];
+                // weight pairs (w, w): x entries bx0..bx0+3, y 16+by0..16+by0+7, zero
+                // outside the support, so every row of the block is updated without a test
+                const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 32);
+                const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
+                const float2 wx2[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
+                                       make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
+#pragma unroll
+                for (int py2 = 0; py2 < 4; ++py2) {
+                    const float4 y = t4[((16 + by0) >> 1) + py2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int py = 2 * py2 + h;
+                        const float2 vv = __fmul2_rn(h ? make_float2(y.z, y.w) : make_float2(y.x, y.y), v);
+#pragma unroll
+                        for (int px = 0; px < 4; ++px) acc[px + 4 * py] = __ffma2_rn(wx2[px], vv, acc[px + 4 * py]);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();  // staging no longer read: reuse it for the output tile
+#pragma unroll
+    for (int q = 0; q < 32; ++q) s_out[(bid * 32 + q) * (CPW + 1) + cl] = acc[q];
+    __syncthreads();
+    const int grp = P.ch.K ? 0 : (it.frame < 0 ? 0 : it.frame);
+    for (int e = threadIdx.x; e < CPW * kReg2Pts; e += blockDim.x) {
+        const int ce = e / kReg2Pts, pt = e - ce * kReg2Pts;
+        const int ch = c0 + ce;
+        if (ch >= nch) break;
+        const int pos = s_pos[pt];
+        if (pos < 0) continue;
+        const int x = pt & 15, y = pt >> 4;
+        const int w = (x >> 2) | ((y >> 3) << 2);
+        const int q = (x & 3) | ((y & 7) << 2);
+        const float2 vv = s_out[(w * 32 + q) * (CPW + 1) + ce];
+        float2 *Gp = P.grid + ((int64_t)grp * nch + ch) * P.g.gvol;
+        if (it.atomic) atomicAdd(Gp + pos, vv);
+        else Gp[pos] = vv;
+    }
+}
+
 // zero the tiles that several CTAs combine with atomics (planar grid)
 template <int D>
 __global__ void zero_tiles_kernel(Geom g, const OwnerItem *zero, int nch, float2 *grid, int basis) {
@@ -1252,6 +1439,24 @@ int launch_spread_reg3_t(const SpreadIL &P, int nitems, int nchunks, cudaStream_
     k<<<grid, C::NW * 32, C::Smem, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
+}
+
+template <int WM, int CPW>
+int launch_spread_reg2_t(const SpreadIL &P, int nitems, int nchunks, cudaStream_t s) {
+    using C = Reg2Cfg<CPW>;
+    auto k = spread_reg2_kernel<WM, CPW>;
+    PFB_RAISE_SMEM(k, (int)C::Smem);
+    dim3 grid(nitems, nchunks);
+    k<<<grid, C::NW * 32, C::Smem, s>>>(P);
+    PFB_CHECK_LAUNCH();
+    return PFB_OK;
+}
+
+template <int WM>
+int launch_spread_reg2_w(const SpreadIL &P, int nitems, int nch, cudaStream_t s) {
+    if (nch <= 8) return launch_spread_reg2_t<WM, 8>(P, nitems, 1, s);
+    if (nch <= 16) return launch_spread_reg2_t<WM, 16>(P, nitems, 1, s);
+    return launch_spread_reg2_t<WM, 32>(P, nitems, (nch + 31) / 32, s);
 }
 
 template <int WM>
@@ -1544,6 +1749,14 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
                 return wmv == 1 ? launch_spread_reg3_w<1>(S, nitems, c.nch, s)
                                 : (wmv == 4 ? launch_spread_reg3_w<4>(S, nitems, c.nch, s)
                                             : launch_spread_reg3_w<8>(S, nitems, c.nch, s));
+            }
+            if (p->g.ndim == 2 && p->g.tile[0] <= kReg2Tile && p->g.tile[1] <= kReg2Tile && c.nch > 16) {
+                // 2D register tiles (16 x 16 points), 32 channels per lane group (with
+                // fewer channels a CTA would have too few warps for the crowded tiles of
+                // radial trajectories: the shared-atomic kernel, 16 warps, is faster)
+                return wmv == 1 ? launch_spread_reg2_w<1>(S, nitems, c.nch, s)
+                                : (wmv == 4 ? launch_spread_reg2_w<4>(S, nitems, c.nch, s)
+                                            : launch_spread_reg2_w<8>(S, nitems, c.nch, s));
             }
             const size_t smem = spread_smem(p, S.cw);
             const int nchunks = (c.nch + S.cw - 1) / S.cw;

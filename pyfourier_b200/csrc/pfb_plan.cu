@@ -143,7 +143,8 @@ int fit_tile(int t, int w, int nos) {
 }
 
 int default_tile(int ndim, int nos) {
-    int t = ndim == 1 ? 1024 : (ndim == 2 ? 32 : 8);
+    // 16 x 16 in 2D and 8^3 in 3D: the register-tile spreads' tiles
+    int t = ndim == 1 ? 1024 : (ndim == 2 ? 16 : 8);
     return std::max(1, std::min(t, nos));
 }
 

@@ -131,6 +131,16 @@ def test_3d_channel_groups(nch):
     check_pair(coord, (N, N, N), crandn(rng, nch, N, N, N), crandn(rng, nch, 30, 90), width=4, oversamp=1.25)
 
 
+@pytest.mark.parametrize("N, nch", [(40, 36), (8, 33)])
+def test_2d_register_tiles(N, nch):
+    """2D spreads of more than 16 channels take 16 x 16 register tiles (32 channels per
+    lane group, a second group for the rest); N = 8 at osf 2 is one tile whose taps wrap."""
+    rng = np.random.default_rng(60 + N)
+    coord = ((rng.random((1, 24, 64, 2)) - 0.5) * N).astype(np.float32)
+    coord[0, :4] *= 0.05  # crowd the centre tiles
+    check_pair(coord, (N, N), crandn(rng, nch, N, N), crandn(rng, nch, 24, 64), width=4, oversamp=2.0)
+
+
 def test_multiframe_and_weights():
     rng = np.random.default_rng(6)
     N, F = 40, 3
