@@ -962,13 +962,13 @@ constexpr int kRegPts = kRegTile * kRegTile * kRegTile;
 // set of derived arrays (tile weights [B][24] f2, each weight held twice as the
 // broadcast operand of a packed FFMA2; masks [B] u), written and read within one
 // batch.  With 32 channels one CTA fills an SM (registers); smaller groups use
-// smaller batches so that 2 (16 channels) or 3 (8) CTAs share an SM.
+// smaller batches so that 2 (16 channels) or 4 (8) CTAs share an SM.
 template <int CPW>
 struct RegCfg {
     static constexpr int G = 32 / CPW;
     static constexpr int NW = 16 / G;
-    static constexpr int Batch = CPW == 32 ? 224 : 128;
-    static constexpr int MinBlocks = CPW == 32 ? 1 : (CPW == 16 ? 2 : 3);
+    static constexpr int Batch = CPW == 32 ? 224 : (CPW == 16 ? 128 : 80);
+    static constexpr int MinBlocks = CPW == 32 ? 1 : (CPW == 16 ? 2 : 4);
     static constexpr size_t OffW = (size_t)Batch * CPW * sizeof(float2);
     static constexpr size_t OffX = OffW + (size_t)Batch * 24 * sizeof(float);
     static constexpr size_t OffD = OffX + (size_t)Batch * 4 * sizeof(int);
