@@ -106,16 +106,66 @@ WORKLOADS = {
 # clocks
 # --------------------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU while a timed region runs (read only).
+
+    NVML polled every 10 ms from a thread (a 40 ms step then gets several samples), else
+    ``nvidia-smi -lms 200``.  The GPU is found by the UUID of the CUDA device, so that
+    CUDA_VISIBLE_DEVICES re-numbering does not pick another board."""
+
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits reported, by the nvidia-smi field names
+    NVML_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                 "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
+    PERIOD_S = 0.01
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.thread = None
+
+    def _nvml_handle(self, nv):
+        try:
+            import torch
+
+            u = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return nv.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _start_nvml(self):
+        import threading
+
+        import pynvml as nv
+
+        nv.nvmlInit()
+        h = self._nvml_handle(nv)
+        self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        self.sm, self.bits, self.stop_evt = [], 0, threading.Event()
+        reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+
+        def run():
+            while True:
+                try:
+                    self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                    self.bits |= int(reasons(h))
+                except nv.NVMLError:
+                    pass
+                if self.stop_evt.wait(self.PERIOD_S):
+                    return
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def start(self):
+        try:
+            self._start_nvml()
+            return
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(prefix="pfb_clocks_", suffix=".csv")
         os.close(fd)
         try:
@@ -126,6 +176,13 @@ class ClockSampler:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_evt.set()
+            self.thread.join()
+            self.thread = None
+            reasons = sorted(nm for nm, b in self.NVML_BITS.items() if self.bits & b)
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax,
+                    "reasons": reasons, "samples": len(self.sm), "source": "nvml, 10 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()

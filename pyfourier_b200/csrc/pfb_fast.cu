@@ -984,6 +984,26 @@ struct RegCfg {
 
 
 
+// Rows y in [YLO, YHI], z in [ZLO, ZHI] of a 4 x 4 x 2 register block:
+// acc[x + 4 (y + 4 z)] += wx[x] (wy[y] (wz[z] v)), weights as (w, w) pairs.
+template <int YLO, int YHI, int ZLO, int ZHI>
+__device__ __forceinline__ void reg3_rows(float2 (&acc)[32], const float2 (&wx2)[4], const float2 (&wy)[4],
+                                          const float2 (&wz)[2], float2 v) {
+#pragma unroll
+    for (int pz = ZLO; pz <= ZHI; ++pz) {
+        const float2 vz = __fmul2_rn(wz[pz], v);
+#pragma unroll
+        for (int py = YLO; py <= YHI; ++py) {
+            const float2 vv = __fmul2_rn(wy[py], vz);
+#pragma unroll
+            for (int px = 0; px < 4; ++px) {
+                const int q2 = px + 4 * (py + 4 * pz);
+                acc[q2] = __ffma2_rn(wx2[px], vv, acc[q2]);
+            }
+        }
+    }
+}
+
 template <int WM, int CPW>
 __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
     spread_reg3_kernel(const SpreadIL P) {
@@ -1103,8 +1123,10 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
         __syncthreads();  // tile weights and masks of batch b ready
         for (int q0 = 0; q0 < nb; q0 += 32) {
             bool hit = false;
+            unsigned mq = 0;  // mask of sample q0 + lane
             if (q0 + lane < nb) {
                 const unsigned m = tm[q0 + lane];
+                mq = m;
 #pragma unroll
                 for (int g = 0; g < G; ++g) hit = hit || ((m & bmx[g]) && (m & bmy[g]) && (m & bmz[g]));
             }
@@ -1114,29 +1136,32 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
                 hm &= hm - 1;
                 const float2 v = rv[q * CPW + cl];
                 // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..; zero
-                // outside the sample's support, so every row of the block is updated
-                // without a test (a branch per row costs more than the row)
+                // outside the sample's support.  Lane groups of fewer than 32 channels
+                // update every row of their blocks without a test (the groups of a warp
+                // hold different blocks, and a branch per row costs more than the row)
                 const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 24);
                 const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
                 const float4 y01 = t4[(8 + by0) >> 1], y23 = t4[((8 + by0) >> 1) + 1];
                 const float4 z01 = t4[(16 + bz0) >> 1];
                 const float2 wx2[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
                                        make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
-                const float2 wy2[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w),
-                                       make_float2(y23.x, y23.y), make_float2(y23.z, y23.w)};
-                const float2 vz[2] = {__fmul2_rn(make_float2(z01.x, z01.y), v),
-                                      __fmul2_rn(make_float2(z01.z, z01.w), v)};
-#pragma unroll
-                for (int pz = 0; pz < 2; ++pz) {
-#pragma unroll
-                    for (int py = 0; py < 4; ++py) {
-                        const float2 vv = __fmul2_rn(wy2[py], vz[pz]);  // wy (wz v)
-#pragma unroll
-                        for (int px = 0; px < 4; ++px) {
-                            const int q2 = px + 4 * (py + 4 * pz);
-                            acc[q2] = __ffma2_rn(wx2[px], vv, acc[q2]);
-                        }
+                const float2 wy[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w),
+                                      make_float2(y23.x, y23.y), make_float2(y23.z, y23.w)};
+                const float2 wz[2] = {make_float2(z01.x, z01.y), make_float2(z01.z, z01.w)};
+                if constexpr (G == 1) {
+                    // the whole warp works on this (sample, block): a warp-uniform jump to
+                    // the code for the block's occupied z rows (1.6 of 2 on average at W 4).
+                    // Finer cases (y ranges too) run slower: a jump table of 9 or 45 cases
+                    // costs more than the rows it skips
+                    const unsigned m = __shfl_sync(0xffffffffu, mq, q - q0);
+                    switch ((m >> (16 + bz0)) & 3u) {
+                        case 1: reg3_rows<0, 3, 0, 0>(acc, wx2, wy, wz, v); break;
+                        case 2: reg3_rows<0, 3, 1, 1>(acc, wx2, wy, wz, v); break;
+                        case 3: reg3_rows<0, 3, 0, 1>(acc, wx2, wy, wz, v); break;
+                        default: break;
                     }
+                } else {
+                    reg3_rows<0, 3, 0, 1>(acc, wx2, wy, wz, v);
                 }
             }
         }
