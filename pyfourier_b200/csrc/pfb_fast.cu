@@ -1136,9 +1136,8 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
                 hm &= hm - 1;
                 const float2 v = rv[q * CPW + cl];
                 // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..; zero
-                // outside the sample's support.  Lane groups of fewer than 32 channels
-                // update every row of their blocks without a test (the groups of a warp
-                // hold different blocks, and a branch per row costs more than the row)
+                // outside the sample's support, so the rows of an occupied z layer are
+                // all updated without a test (a branch per row costs more than the row)
                 const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 24);
                 const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
                 const float4 y01 = t4[(8 + by0) >> 1], y23 = t4[((8 + by0) >> 1) + 1];
@@ -1148,20 +1147,16 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
                 const float2 wy[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w),
                                       make_float2(y23.x, y23.y), make_float2(y23.z, y23.w)};
                 const float2 wz[2] = {make_float2(z01.x, z01.y), make_float2(z01.z, z01.w)};
-                if constexpr (G == 1) {
-                    // the whole warp works on this (sample, block): a warp-uniform jump to
-                    // the code for the block's occupied z rows (1.6 of 2 on average at W 4).
-                    // Finer cases (y ranges too) run slower: a jump table of 9 or 45 cases
-                    // costs more than the rows it skips
-                    const unsigned m = __shfl_sync(0xffffffffu, mq, q - q0);
-                    switch ((m >> (16 + bz0)) & 3u) {
-                        case 1: reg3_rows<0, 3, 0, 0>(acc, wx2, wy, wz, v); break;
-                        case 2: reg3_rows<0, 3, 1, 1>(acc, wx2, wy, wz, v); break;
-                        case 3: reg3_rows<0, 3, 0, 1>(acc, wx2, wy, wz, v); break;
-                        default: break;
-                    }
-                } else {
-                    reg3_rows<0, 3, 0, 1>(acc, wx2, wy, wz, v);
+                // the blocks of a warp share one z layer (block id bits 2-3), so a jump on
+                // the layer's occupied z rows (1.6 of 2 on average at W 4) is warp-uniform
+                // whatever the group size.  Finer cases (y ranges too, 32-channel groups)
+                // run slower: a jump table of 9 or 45 cases costs more than the rows it skips
+                const unsigned m = __shfl_sync(0xffffffffu, mq, q - q0);
+                switch ((m >> (16 + bz0)) & 3u) {
+                    case 1: reg3_rows<0, 3, 0, 0>(acc, wx2, wy, wz, v); break;
+                    case 2: reg3_rows<0, 3, 1, 1>(acc, wx2, wy, wz, v); break;
+                    case 3: reg3_rows<0, 3, 0, 1>(acc, wx2, wy, wz, v); break;
+                    default: break;
                 }
             }
         }
