@@ -255,9 +255,14 @@ def _finish(out, dtype, idevice, as_numpy):
 
 
 # Host inputs of at least this many bytes are processed in batch chunks whose
-# host->device copy, compute and device->host copy overlap (three streams).
+# host->device copy, compute and device->host copy overlap (three streams).  The
+# forward is copy-bound and takes more, smaller chunks (a shorter first copy and last
+# read-back); the adjoint is compute-bound and keeps chunks large enough for its
+# spread to stay efficient (3D radial, 32 coils of 8 M samples: forward 55.6 ms with
+# 8 chunks against 58.6 ms with 4; adjoint 68.8 ms with 4 against 99.2 ms with 8).
 _HOST_PIPELINE_MIN_BYTES = 64 << 20
-_HOST_PIPELINE_CHUNKS = 4
+_HOST_PIPELINE_CHUNKS_FWD = 8
+_HOST_PIPELINE_CHUNKS_ADJ = 4
 
 
 def _host_pipelined(t, grad_coord):
@@ -266,15 +271,15 @@ def _host_pipelined(t, grad_coord):
             and t.numel() * 8 >= _HOST_PIPELINE_MIN_BYTES)
 
 
-def _pipeline(xh, run, out_tail, dev):
+def _pipeline(xh, run, out_tail, dev, chunks):
     """Apply ``run`` (device (b, ...) complex64 -> device (b, *out_tail) complex64, on the
-    current stream) to a CPU batch ``xh`` (B, ...) in up to _HOST_PIPELINE_CHUNKS chunks:
+    current stream) to a CPU batch ``xh`` (B, ...) in up to ``chunks`` chunks:
     chunk j + 1 is copied to the device on one stream and chunk j - 1's result copied back
     on another while chunk j computes.  Pageable inputs are staged chunk by chunk through
     page-locked buffers.  Returns a page-locked CPU tensor (B, *out_tail)."""
     B = xh.shape[0]
     out = torch.empty((B, *out_tail), dtype=torch.complex64, pin_memory=True)
-    n = max(1, min(B, _HOST_PIPELINE_CHUNKS))
+    n = max(1, min(B, chunks))
     bounds = [(B * j // n, B * (j + 1) // n) for j in range(n)]
     pinned = xh.is_pinned()
     with torch.cuda.device(dev):
@@ -349,7 +354,8 @@ def nufft(image, coord=None, shape=None, nufft_plan=None, basis=None, zmap=None,
     wps, wfull = _split_weight(weight, sshape, dev)
     ctx = _Ctx(plan, basis_t, wps, norm_code(norm))
     if host and B >= 2 and wfull is None:
-        y = _pipeline(x.reshape(B, C, *plan.shape), lambda xd: fwd_core(ctx, xd), (ip.total_samples,), dev)
+        y = _pipeline(x.reshape(B, C, *plan.shape), lambda xd: fwd_core(ctx, xd), (ip.total_samples,), dev,
+                      _HOST_PIPELINE_CHUNKS_FWD)
         return _finish(y.reshape(*batch_shape, *sshape), dtype, idevice, as_numpy)
     if host:
         x = _to_compute(x, dev)[1]
@@ -398,7 +404,8 @@ def nufft_adj(kspace, coord=None, shape=None, nufft_plan=None, basis=None, zmap=
     wps, wfull = _split_weight(weight, sshape, dev)
     ctx = _Ctx(plan, basis_t, wps, norm_code(norm))
     if host and B >= 2 and wfull is None:
-        x = _pipeline(k.reshape(B, ip.total_samples), lambda kd: adj_core(ctx, kd), (C, *plan.shape), dev)
+        x = _pipeline(k.reshape(B, ip.total_samples), lambda kd: adj_core(ctx, kd), (C, *plan.shape), dev,
+                      _HOST_PIPELINE_CHUNKS_ADJ)
         x = x.reshape(*batch_shape, *((C,) if has_c else ()), *plan.shape)
         return _finish(x, dtype, idevice, as_numpy)
     if host:

@@ -1123,16 +1123,18 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
         __syncthreads();  // tile weights and masks of batch b ready
         for (int q0 = 0; q0 < nb; q0 += 32) {
             bool hit = false;
-            unsigned mq = 0;  // mask of sample q0 + lane
+            unsigned zl = 0;  // occupied z rows of the warp's z layer, sample q0 + lane
             if (q0 + lane < nb) {
                 const unsigned m = tm[q0 + lane];
-                mq = m;
+                zl = (m >> (16 + bz0)) & 3u;
 #pragma unroll
                 for (int g = 0; g < G; ++g) hit = hit || ((m & bmx[g]) && (m & bmy[g]) && (m & bmz[g]));
             }
             unsigned hm = __ballot_sync(0xffffffffu, hit);
+            // ballots are warp-uniform values: the jump below needs no convergence barrier
+            const unsigned z0 = __ballot_sync(0xffffffffu, zl & 1u), z1 = __ballot_sync(0xffffffffu, zl & 2u);
             while (hm) {
-                const int q = q0 + __ffs(hm) - 1;
+                const int k = __ffs(hm) - 1, q = q0 + k;
                 hm &= hm - 1;
                 const float2 v = rv[q * CPW + cl];
                 // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..; zero
@@ -1151,8 +1153,7 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
                 // the layer's occupied z rows (1.6 of 2 on average at W 4) is warp-uniform
                 // whatever the group size.  Finer cases (y ranges too, 32-channel groups)
                 // run slower: a jump table of 9 or 45 cases costs more than the rows it skips
-                const unsigned m = __shfl_sync(0xffffffffu, mq, q - q0);
-                switch ((m >> (16 + bz0)) & 3u) {
+                switch (((z0 >> k) & 1u) | (((z1 >> k) & 1u) << 1)) {
                     case 1: reg3_rows<0, 3, 0, 0>(acc, wx2, wy, wz, v); break;
                     case 2: reg3_rows<0, 3, 1, 1>(acc, wx2, wy, wz, v); break;
                     case 3: reg3_rows<0, 3, 0, 1>(acc, wx2, wy, wz, v); break;
