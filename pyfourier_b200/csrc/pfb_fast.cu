@@ -1151,8 +1151,9 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
                 const float2 wz[2] = {make_float2(z01.x, z01.y), make_float2(z01.z, z01.w)};
                 // the blocks of a warp share one z layer (block id bits 2-3), so a jump on
                 // the layer's occupied z rows (1.6 of 2 on average at W 4) is warp-uniform
-                // whatever the group size.  Finer cases (y ranges too, 32-channel groups)
-                // run slower: a jump table of 9 or 45 cases costs more than the rows it skips
+                // whatever the group size.  Finer cases run slower: 9 or 45 cases over the
+                // y range as well (a jump table), or a nested jump on the y halves, cost more
+                // than the rows they skip
                 switch (((z0 >> k) & 1u) | (((z1 >> k) & 1u) << 1)) {
                     case 1: reg3_rows<0, 3, 0, 0>(acc, wx2, wy, wz, v); break;
                     case 2: reg3_rows<0, 3, 1, 1>(acc, wx2, wy, wz, v); break;
