@@ -357,6 +357,25 @@ def bind_to_gpu_cpus(torch, dev):
         return None
 
 
+def max_over_ranks(x, world, device):
+    """Max of a per-rank float over the process group (the slowest rank's time);
+    the value itself with one rank."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, ms):
+    """Units all ranks processed per second, each rank doing ``units_per_rank`` per
+    step of ``ms`` milliseconds (the max over ranks): weak scaling."""
+    return world * units_per_rank / (ms / 1e3)
+
+
 def gpu_arm(args, wl, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -401,11 +420,8 @@ def gpu_arm(args, wl, rank, world, local_rank):
     barrier()
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * samples_per_step / (ms / 1e3)
+    ms = max_over_ranks(ms, world, dev)
+    value = whole_job_rate(world, samples_per_step, ms)
 
     # end to end through the public API with host buffers (pinned), on the GPU's CPUs
     prev_cpus = bind_to_gpu_cpus(torch, dev)
@@ -421,11 +437,7 @@ def gpu_arm(args, wl, rank, world, local_rank):
         yk = pf.nufft(x_host, nufft_plan=plan, device=dev)       # H2D image, D2H k-space
         xa = pf.nufft_adj(yk, nufft_plan=plan, device=dev)       # H2D k-space, D2H image
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, world, dev)
     h2d = x_host.numel() * 8 + yk.numel() * 8
     d2h = yk.numel() * 8 + xa.numel() * 8
     del x_host, yk, xa
@@ -446,8 +458,8 @@ def gpu_arm(args, wl, rank, world, local_rank):
                 "fp32": fp32_roofline(wl, plan, B, mine[dom]) if dom in ("spread", "interp") else None,
                 "stages": {k: {"ms": round(mine[k], 3), "GB/s": round(alg[k] / (mine[k] / 1e3) / 1e9, 1),
                                "frac": round(alg[k] / (mine[k] / 1e3) / 1e9 / peak, 3)} for k in mine}}
-    return dict(ms=ms, value=value, e2e=world * samples_per_step / e2e_s, h2d=h2d, d2h=d2h, stages=stages,
-                roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=mine_l,
+    return dict(ms=ms, value=value, e2e=whole_job_rate(world, samples_per_step, e2e_s * 1e3), h2d=h2d, d2h=d2h,
+                stages=stages, roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=mine_l,
                 kernels_per_step=all_l)
 
 
