@@ -1,0 +1,68 @@
+"""Property tests of the oracle (CPU, hypothesis): for random dimensions, sizes,
+kernel widths, oversampling factors and sample sets (some exactly on the -N/2
+edge), the forward and adjoint NUFFT are adjoint to each other (norm "ortho")
+and linear."""
+
+import numpy as np
+from hypothesis import HealthCheck, assume, given, settings
+from hypothesis import strategies as st
+
+from oracle import nufft_oracle as orc
+
+
+def _case(data):
+    ndim = data.draw(st.integers(1, 3), label="ndim")
+    hi = {1: 40, 2: 20, 3: 10}[ndim]
+    shape = tuple(data.draw(st.integers(4, hi), label=f"N{a}") for a in range(ndim))  # (z, y, x)
+    width = data.draw(st.integers(2, 8), label="width")
+    osf = data.draw(st.sampled_from([1.25, 1.5, 2.0]), label="oversamp")
+    os_shape = orc.oversamp_shape(np.asarray(shape, np.int64), np.full(ndim, osf, np.float32))
+    assume(all(width <= int(o) for o in os_shape))
+    M = data.draw(st.integers(1, 60), label="samples")
+    on_edge = data.draw(st.integers(0, min(M, 4)), label="edge samples")
+    rng = np.random.default_rng(data.draw(st.integers(0, 2 ** 31 - 1), label="seed"))
+    n_xyz = np.asarray(shape[::-1], np.float64)
+    coord = (rng.random((M, ndim)) - 0.5) * n_xyz
+    coord[:on_edge] = -n_xyz / 2
+    plan = orc.plan_nufft(coord.astype(np.float32), shape, width=width, oversamp=osf)
+    return rng, shape, M, plan
+
+
+def _crandn(rng, *shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+@settings(max_examples=40, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(data=st.data())
+def test_adjointness(data):
+    rng, shape, M, plan = _case(data)
+    x = _crandn(rng, 2, *shape)
+    y = _crandn(rng, 2, M)
+    ax = orc.nufft_fwd(x, plan, norm="ortho")
+    ahy = orc.nufft_adj(y, plan, norm="ortho")
+    assert ax.shape == (2, M) and ahy.shape == x.shape
+    lhs = np.vdot(y, ax.astype(np.complex128))
+    rhs = np.vdot(ahy.astype(np.complex128), x)
+    # float32 sums: the difference is small against the Cauchy-Schwarz scale of either side
+    scale = np.linalg.norm(y) * np.linalg.norm(ax) + np.linalg.norm(ahy) * np.linalg.norm(x)
+    assert abs(lhs - rhs) <= 1e-5 * scale + 1e-30
+
+
+@settings(max_examples=25, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(data=st.data())
+def test_linearity(data):
+    rng, shape, M, plan = _case(data)
+    x1, x2 = _crandn(rng, 1, *shape), _crandn(rng, 1, *shape)
+    a, b = complex(rng.standard_normal(), rng.standard_normal()), complex(rng.standard_normal(), 0.5)
+    lhs = orc.nufft_fwd((a * x1 + b * x2).astype(np.complex64), plan)
+    rhs = a * orc.nufft_fwd(x1, plan) + b * orc.nufft_fwd(x2, plan)
+    ref = np.linalg.norm(rhs)
+    if ref == 0:
+        assert np.linalg.norm(lhs) == 0
+    else:
+        assert np.linalg.norm(lhs - rhs) <= 1e-5 * (abs(a) * np.linalg.norm(orc.nufft_fwd(x1, plan))
+                                                  + abs(b) * np.linalg.norm(orc.nufft_fwd(x2, plan)))
+    y = _crandn(rng, 1, M)
+    lhs = orc.nufft_adj((a * y).astype(np.complex64), plan)
+    assert np.linalg.norm(lhs - a * orc.nufft_adj(y, plan)) <= 1e-5 * abs(a) * np.linalg.norm(
+        orc.nufft_adj(y, plan)) + 1e-30
