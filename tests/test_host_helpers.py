@@ -1,0 +1,73 @@
+"""Host-side helpers of the operators (no GPU): norm codes, sample shapes, the split of
+`weight` between the kernels (real per-sample weights) and torch (everything else),
+dtype promotion of the input and the choice of the chunked host path."""
+
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+
+from pyfourier_b200 import _lib, _nufft
+
+CPU = torch.device("cpu")
+
+
+def test_norm_code():
+    assert _nufft.norm_code(None) == _lib.PFB_NORM_NONE
+    assert _nufft.norm_code("ortho") == _lib.PFB_NORM_ORTHO
+    with pytest.raises(ValueError):
+        _nufft.norm_code("forward")
+
+
+def test_sample_shape():
+    flat = SimpleNamespace(dshape=None, total_samples=123, nframes=4)
+    assert _nufft._sample_shape(flat) == (123,)
+    one = SimpleNamespace(dshape=(16, 40), total_samples=640, nframes=1)
+    assert _nufft._sample_shape(one) == (16, 40)
+    many = SimpleNamespace(dshape=(16, 40), total_samples=1920, nframes=3)
+    assert _nufft._sample_shape(many) == (3, 16, 40)
+
+
+def test_split_weight_kernel_and_torch_parts():
+    ss = (3, 16, 40)
+    assert _nufft._split_weight(None, ss, CPU) == (None, None)
+    # a real per-sample weight goes to the kernels, flattened in sample order, float32
+    w = np.random.default_rng(0).random(ss)
+    ws, wt = _nufft._split_weight(w, ss, CPU)
+    assert wt is None and ws.dtype == torch.float32 and ws.shape == (3 * 16 * 40,)
+    assert torch.equal(ws, torch.as_tensor(w, dtype=torch.float32).reshape(-1))
+    # leading singleton axes and broadcasting over views are still per-sample
+    ws, wt = _nufft._split_weight(w[None, None], ss, CPU)
+    assert wt is None and ws.shape == (1920,)
+    ws, wt = _nufft._split_weight(np.ones((1, 1, 40)), ss, CPU)
+    assert wt is None and torch.equal(ws, torch.ones(1920))
+    # a weight with a real batch axis (one per coil) is applied with torch
+    ws, wt = _nufft._split_weight(np.ones((8,) + ss), ss, CPU)
+    assert ws is None and wt.shape == (8,) + ss and wt.dtype == torch.float32
+    # complex weights are applied with torch, in complex64
+    ws, wt = _nufft._split_weight(np.ones(ss, np.complex128), ss, CPU)
+    assert ws is None and wt.dtype == torch.complex64
+    # a shape that does not broadcast to the samples is left to torch (which will raise there)
+    ws, wt = _nufft._split_weight(np.ones((7,)), ss, CPU)
+    assert ws is None and wt is not None
+
+
+@pytest.mark.parametrize("dtype", [np.float16, np.float32, np.float64, np.complex64, np.complex128])
+def test_to_compute_promotes_to_complex64(dtype):
+    x = np.arange(6).reshape(2, 3).astype(dtype)
+    orig, xc = _nufft._to_compute(x, CPU)
+    assert xc.dtype == torch.complex64 and xc.shape == (2, 3)
+    assert np.allclose(xc.numpy(), x.astype(np.complex128))
+    assert orig.dtype == torch.as_tensor(x).dtype
+
+
+def test_host_pipeline_choice(monkeypatch):
+    monkeypatch.setattr(_nufft, "_HOST_PIPELINE_MIN_BYTES", 1024)
+    big = torch.zeros(200, dtype=torch.complex64)  # 1600 bytes
+    assert _nufft._host_pipelined(big, None)
+    assert not _nufft._host_pipelined(torch.zeros(100, dtype=torch.complex64), None)  # 800 bytes
+    assert not _nufft._host_pipelined(big.to(torch.complex128), None)
+    assert not _nufft._host_pipelined(big.clone().requires_grad_(True), None)
+    assert not _nufft._host_pipelined(big, torch.zeros(3, requires_grad=True))
+    assert _nufft._HOST_PIPELINE_CHUNKS_FWD >= _nufft._HOST_PIPELINE_CHUNKS_ADJ >= 1
