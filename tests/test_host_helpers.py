@@ -71,3 +71,23 @@ def test_host_pipeline_choice(monkeypatch):
     assert not _nufft._host_pipelined(big.clone().requires_grad_(True), None)
     assert not _nufft._host_pipelined(big, torch.zeros(3, requires_grad=True))
     assert _nufft._HOST_PIPELINE_CHUNKS_FWD >= _nufft._HOST_PIPELINE_CHUNKS_ADJ >= 1
+
+
+def test_resolve_device_maps_the_reference_arguments(monkeypatch):
+    from pyfourier_b200 import _plan
+
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: True)
+    monkeypatch.setattr(torch.cuda, "current_device", lambda: 1)
+    rd = _plan.resolve_device
+    assert rd("cpu") == torch.device("cuda:1")          # the reference's default: the current GPU
+    assert rd(-1) == torch.device("cuda:1")
+    assert rd(None) == torch.device("cuda:1")
+    assert rd(3) == torch.device("cuda:3")
+    assert rd("cuda") == torch.device("cuda:1")
+    assert rd("cuda:2") == torch.device("cuda:2")
+    assert rd(torch.device("cuda:0")) == torch.device("cuda:0")
+    assert rd("cpu", fallback=torch.device("cuda:2")) == torch.device("cuda:2")  # the input's GPU
+    assert rd("cpu", fallback=torch.device("cpu")) == torch.device("cuda:1")
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        rd("cuda:0")
