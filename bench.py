@@ -221,24 +221,83 @@ def measured_hbm_peak():
 # --------------------------------------------------------------------------------------
 # CPU baseline (the oracle: C restatement of the reference's Numba kernels + NumPy glue)
 # --------------------------------------------------------------------------------------
-def cpu_baseline(wl, coord, coils_sample, steps=1):
+def default_cpu_coils(total=32):
+    """Coils of the bounded CPU sample: one per host thread of the oracle (at
+    most all of them).
+
+    The reference's CPU spread parallelises over frames x batch only
+    (_noncart2cart/_3D.py:29, restated with the same loop in the oracle), so a
+    sample with fewer coils than threads leaves cores idle and understates it."""
     from oracle import nufft_oracle as orc
 
-    rng = np.random.default_rng(1)
+    return max(1, min(total, int(orc.lib().orc_num_threads())))
+
+
+def cpu_baseline(wl, coord, x_host, y_host=None, steps=1):
+    """The oracle (the C restatement of the reference's Numba kernels + NumPy /
+    pocketfft glue, all host threads) on the given coils of the workload.
+
+    x_host (c, N, N, N) complex64 is the forward input; y_host (c, M), when
+    given, the adjoint input (else the oracle's own forward output).  Returns the
+    rate over fwd + adj of all c coils (median of ``steps``), the plan-build time
+    (timed separately), the thread count and the outputs of the last step."""
+    from oracle import nufft_oracle as orc
+
     N = wl["N"]
-    x = (rng.standard_normal((coils_sample, N, N, N)) + 1j * rng.standard_normal((coils_sample, N, N, N))
-         ).astype(np.complex64)
+    c = x_host.shape[0]
+    t0 = time.perf_counter()
     plan = orc.plan_nufft(coord, (N, N, N), width=wl["width"], oversamp=wl["oversamp"])
-    y = orc.nufft_fwd(x, plan)  # warm-up (first-touch, thread pools)
+    plan_s = time.perf_counter() - t0
+    orc.nufft_fwd(x_host[:1], plan)  # warm-up (thread pools, first touch of the tables)
     times = []
     for _ in range(max(1, steps)):
         t0 = time.perf_counter()
-        y = orc.nufft_fwd(x, plan)
-        orc.nufft_adj(y, plan)
+        yo = orc.nufft_fwd(x_host, plan)
+        xo = orc.nufft_adj(yo if y_host is None else y_host.reshape(yo.shape), plan)
         times.append(time.perf_counter() - t0)
     t = statistics.median(times)
     M = coord.shape[0] * coord.shape[1]
-    return {"value": coils_sample * M / t, "seconds": t, "threads": orc.lib().orc_num_threads()}
+    return {"value": c * M / t, "seconds": t, "plan_seconds": plan_s, "threads": orc.lib().orc_num_threads(),
+            "cpu_count": os.cpu_count(), "y": yo.reshape(c, -1), "x": xo}
+
+
+# --------------------------------------------------------------------------------------
+# float64 direct NUDFT on the device (a checker for the error against the exact transform)
+# --------------------------------------------------------------------------------------
+def nudft_fwd_fp64(torch, image, coord, chunk=2048):
+    """y_m = sum_r x(r) exp(-2 pi i k_m . r / N) in complex128, r centred in
+    [-N//2, N - N//2) per axis (the reference's centred-FFT convention).
+
+    image (*N) with N in (z, y, x) order, coord (M, d) in cycles/FOV, (x, y, z)
+    order.  Separable: the x sum is a matrix product, y and z follow."""
+    dev = image.device
+    shp = tuple(image.shape)
+    d = len(shp)
+    x = image.to(torch.complex128)
+    k = torch.as_tensor(np.asarray(coord, np.float64), device=dev)
+    out = []
+    for m0 in range(0, k.shape[0], chunk):
+        kk = k[m0:m0 + chunk]
+        E = []
+        for a in range(d):  # a = 0: x (last image axis)
+            n = shp[d - 1 - a]
+            r = torch.arange(n, dtype=torch.float64, device=dev) - n // 2
+            E.append(torch.exp(-2j * math.pi * kk[:, a:a + 1] * r[None, :] / n))  # (m, n)
+        t = x.reshape(-1, shp[-1]) @ E[0].T  # (..., m)
+        t = t.reshape(*shp[:-1], -1)
+        if d >= 2:
+            t = (t * E[1].T.reshape(shp[-2], -1)).sum(-2) if d == 2 else \
+                (t * E[1].T.reshape(1, shp[-2], -1)).sum(-2)
+        if d == 3:
+            t = (t * E[2].T).sum(0)
+        out.append(t.reshape(-1))
+    return torch.cat(out)
+
+
+def rel_l2_t(torch, a, b):
+    a = a.to(torch.complex128).reshape(-1)
+    b = b.to(torch.complex128).reshape(-1)
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
 
 
 # --------------------------------------------------------------------------------------
@@ -297,29 +356,9 @@ def stage_times(torch, pf, plan, x, iters):
 
 
 def algorithmic_bytes(wl, plan, B):
-    """Bytes each stage must move at minimum (inputs read once, outputs written once).
-
-    3D grids use the fused pruned FFT, whose passes are the pad / fft / transpose
-    (forward) and ifft / crop (adjoint) stages: per plane, with N the image and
-    n the oversampled extent, the z pass reads N^3 and writes n N^2, the y pass
-    n N^2 -> n^2 N, the x pass n^2 N -> n^3 (and the reverse for the adjoint)."""
-    M = plan.interpolator.total_samples
-    G = int(np.prod(plan.os_shape))
-    nd = plan.ndim
-    coords = M * (4 * nd + 4 + 4)  # sorted coords, permutation, frame index
-    N, n = plan.shape[-1], plan.os_shape[-1]
-    e = 8 * B
-    return {
-        "interp": B * G * 8 + B * M * 8 + coords,   # grid read once, per-channel results written
-        "out": 2 * B * M * 8,                        # results read, k-space written
-        "vals": 2 * B * M * 8,                       # k-space read, per-channel values written
-        "spread": B * M * 8 + B * G * 8 + coords,   # values read, grid written once
-        "pad": e * (N ** 3 + n * N ** 2),            # z pass
-        "fft": e * (n * N ** 2 + n ** 2 * N),        # y pass
-        "transpose": e * (n ** 2 * N + n ** 3),      # x pass into the interleaved grid
-        "ifft": e * (n ** 3 + 2 * n ** 2 * N + n * N ** 2),  # x and y passes
-        "crop": e * (n * N ** 2 + N ** 3),           # z pass into the image
-    }
+    """Bytes each stage of the headline step must move at minimum (stage_bytes
+    with B coils, one frame, no B0 segments)."""
+    return stage_bytes(plan, B)
 
 
 def fp32_roofline(wl, plan, B, ms):
@@ -444,6 +483,10 @@ def gpu_arm(args, wl, rank, world, local_rank):
     if prev_cpus is not None:
         os.sched_setaffinity(0, prev_cpus)
 
+    # outputs of one forward + adjoint of the benchmarked step, kept for the parity checks
+    y_dev = pf.nufft(x, nufft_plan=plan, device=dev)
+    xa_dev = pf.nufft_adj(y_dev, nufft_plan=plan, device=dev)
+
     mine_l, all_l = (None, None) if args.no_launch_trace else count_launches(torch, lambda: step(x))
     stages = stage_times(torch, pf, plan, x, max(3, args.steps))
     alg = algorithmic_bytes(wl, plan, B)
@@ -460,7 +503,39 @@ def gpu_arm(args, wl, rank, world, local_rank):
                                "frac": round(alg[k] / (mine[k] / 1e3) / 1e9 / peak, 3)} for k in mine}}
     return dict(ms=ms, value=value, e2e=whole_job_rate(world, samples_per_step, e2e_s * 1e3), h2d=h2d, d2h=d2h,
                 stages=stages, roofline=roofline, clocks=clk, M=M, coord=coord, launches_per_step=mine_l,
-                kernels_per_step=all_l)
+                kernels_per_step=all_l, x=x, y=y_dev, xa=xa_dev, plan=plan)
+
+
+def parity_cfg2(torch, wl, r, cpu_coils, nudft_samples=10240):
+    """Parity of the benchmarked step on its own inputs.
+
+    * rel-L2 of the GPU forward (all 32 channels in one pass) on the first
+      ``cpu_coils`` coils against the oracle's forward of the same image, and of
+      the GPU adjoint of the GPU k-space against the oracle's adjoint of that
+      k-space (bound: 1e-5);
+    * rel-L2 of the GPU forward of coil 0 against a float64 direct NUDFT on a
+      seeded subset of samples: the accuracy of the Kaiser-Bessel kernel at
+      these parameters, which the reference's kernel shares."""
+    c = cpu_coils
+    x_host = r["x"][:c].cpu().numpy()
+    y_host = r["y"][:c].cpu().numpy()
+    res = cpu_baseline(wl, r["coord"], x_host, y_host, steps=1)
+    e_fwd = float(np.linalg.norm(y_host.astype(np.complex128) - res["y"]) / np.linalg.norm(res["y"]))
+    xg = r["xa"][:c].cpu().numpy().reshape(res["x"].shape)
+    e_adj = float(np.linalg.norm(xg.astype(np.complex128) - res["x"]) / np.linalg.norm(res["x"]))
+    rng = np.random.default_rng(0)
+    coord = r["coord"].reshape(-1, 3)
+    sel = np.sort(rng.choice(coord.shape[0], nudft_samples, replace=False))
+    ref = nudft_fwd_fp64(torch, r["x"][0], coord[sel])
+    e_nudft = rel_l2_t(torch, r["y"][0, torch.as_tensor(sel, device=r["y"].device)], ref)
+    parity = {"rel_l2_fwd": e_fwd, "rel_l2_adj": e_adj, "vs": "oracle (C restatement of the reference's "
+              f"kernels), {c} of {wl['coils']} coils, full trajectory", "tolerance": 1e-5,
+              "pass": bool(e_fwd <= 1e-5 and e_adj <= 1e-5),
+              "vs_fp64_nudft": {"rel_l2_fwd": e_nudft, "samples": nudft_samples, "coil": 0,
+                                "target": 1e-4, "meets_target": bool(e_nudft <= 1e-4),
+                                "note": "kernel accuracy of W 4 at osf 1.25 (the configuration's own parameters; "
+                                        "the reference's kernel gives the same error): above 1e-4"}}
+    return parity, res
 
 
 # --------------------------------------------------------------------------------------
@@ -543,6 +618,348 @@ def time_device(torch, fn, steps, warmup):
     return a.elapsed_time(b) / steps
 
 
+def stage_bytes(plan, B, C=1, L=1, basis=False):
+    """Bytes each stage of the channel-interleaved pipeline must move at minimum
+    (inputs read once, outputs written once), 2D or 3D.
+
+    B batch, C coefficients (K with a basis, else frames), L B0 segments.  Image
+    planes: B C; grid planes: B C L; channels per sample: B L (x K with a basis).
+    The fused transform's passes are the pad / fft / transpose stages (forward:
+    z, y, x passes in 3D; y, x in 2D) and ifft / crop (adjoint): per plane the z
+    pass reads Nx Ny Nz and writes Nx Ny nz, the y pass Nx Ny nz -> Nx ny nz,
+    the x pass Nx ny nz -> nx ny nz (the reverse for the adjoint)."""
+    M = plan.interpolator.total_samples
+    nd = plan.ndim
+    Ns = list(plan.shape)[::-1] + [1] * (3 - nd)      # (x, y, z)
+    ns = list(plan.os_shape)[::-1] + [1] * (3 - nd)
+    G = int(np.prod(ns))
+    coords = M * (4 * nd + 4 + 4)  # sorted coords, permutation, frame index
+    nch = B * L * (C if basis else 1)
+    img = B * C * int(np.prod(Ns)) * 8
+    gp = B * C * L * 8
+    out = {"interp": gp * G + nch * M * 8 + coords, "out": nch * M * 8 + B * M * 8,
+           "vals": B * M * 8 + nch * M * 8, "spread": nch * M * 8 + gp * G + coords}
+    if nd == 3:
+        a = Ns[0] * Ns[1] * ns[2]       # after the z pass
+        b = Ns[0] * ns[1] * ns[2]       # after the y pass
+        out.update(pad=img + gp * a, fft=gp * (a + b), transpose=gp * (b + G), ifft=gp * (G + 2 * b + a),
+                   crop=gp * a + img)
+    else:
+        a = Ns[0] * ns[1]
+        out.update(pad=img + gp * a, fft=0, transpose=gp * (a + G), ifft=gp * (G + a), crop=gp * a + img)
+    return out
+
+
+def stage_roofline(stages, alg, peak, peak_kind):
+    """Roofline of the slowest stage (its algorithmic bytes / its CUDA-event time)
+    and every stage's fraction of the measured copy bandwidth."""
+    mine = {k: v for k, v in stages.items() if k in alg and alg[k] > 0}
+    dom = max(mine, key=mine.get)
+    gbs = lambda k: alg[k] / (mine[k] / 1e3) / 1e9  # noqa: E731
+    return {"bound": "hbm", "kernel": dom, "achieved": round(gbs(dom), 1), "peak": peak, "peak_source": peak_kind,
+            "unit": "GB/s", "frac": round(gbs(dom) / peak, 4), "traffic": None, "algorithmic_bytes": alg[dom],
+            "stages": {k: {"ms": round(mine[k], 4), "GB/s": round(gbs(k), 1), "frac": round(gbs(k) / peak, 3)}
+                       for k in mine}}
+
+
+def gram_apply_bytes(N, B, K, L=1):
+    """Minimum bytes of one Toeplitz Gram apply on the 2N embedding (2D): image
+    read and written once, embedded grid written, two FFTs reading and writing
+    the grid once each, the per-voxel K x K mix reading the grid and kernel and
+    writing the grid, and the crop reading the image-sized corner."""
+    img = B * K * N * N * 8
+    grid = B * K * L * 4 * N * N * 8
+    kern = L * 4 * N * N * K * K * 8
+    return {"embed": img + grid, "fft": 2 * grid, "mix": 2 * grid + kern, "ifft": 2 * grid,
+            "extract": B * K * L * N * N * 8 + img}
+
+
+def nudft2_normal_subspace_fp64(torch, x, coord, basis, chunk=8192):
+    """Exact (float64) normal operator of the subspace NUFFT with unit weights:
+    out_k = sum_t conj(B[t, k]) A_t^H A_t sum_j B[t, j] x_j, A_t the direct NUDFT
+    of frame t (the operator an unnormalised Toeplitz Gram equals).
+    x (K, N, N); coord (F, ..., 2); basis (F, K)."""
+    dev = x.device
+    K, Ny, Nx = x.shape
+    xb = x.to(torch.complex128)
+    bt = torch.as_tensor(basis, device=dev).to(torch.complex128)
+    out = torch.zeros_like(xb)
+    ry = torch.arange(Ny, dtype=torch.float64, device=dev) - Ny // 2
+    rx = torch.arange(Nx, dtype=torch.float64, device=dev) - Nx // 2
+    for t in range(coord.shape[0]):
+        img = torch.einsum("j,jyx->yx", bt[t], xb)
+        back = torch.zeros((Ny, Nx), dtype=torch.complex128, device=dev)
+        k = torch.as_tensor(coord[t].reshape(-1, 2).astype(np.float64), device=dev)
+        for m0 in range(0, k.shape[0], chunk):
+            kk = k[m0:m0 + chunk]
+            Ex = torch.exp(-2j * math.pi * kk[:, :1] * rx[None] / Nx)  # (m, Nx)
+            Ey = torch.exp(-2j * math.pi * kk[:, 1:2] * ry[None] / Ny)  # (m, Ny)
+            y = ((img @ Ex.T) * Ey.T).sum(0)                           # (m,)
+            back += (Ey.conj().T * y[None]) @ Ex.conj()                 # (Ny, Nx)
+        out += bt[t].conj()[:, None, None] * back[None]
+    return out
+
+
+def wl_cfg3(torch, pf, dev, args, clocks, cpu=True):
+    """Toeplitz Gram with a K = 4 subspace (2D VD spiral, 48 frames, 16 coils)."""
+    N, B, F, K = 220, 16, 48, 4
+    coord = np.stack([vd_spiral(16, 2048, N, rot=f * np.pi * (3 - 5 ** 0.5)) for f in range(F)])
+    basis = exp_recovery_basis(K, nt=F)
+    t0 = time.perf_counter()
+    gm = pf.plan_spgram(torch.as_tensor(coord, device=dev), (N, N), basis=torch.as_tensor(basis, device=dev),
+                        device=dev)
+    torch.cuda.synchronize()
+    plan_s = time.perf_counter() - t0
+    g = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.complex(torch.randn(B, K, N, N, generator=g), torch.randn(B, K, N, N, generator=g)).to(dev)
+    step = lambda: pf.sparse_gram(x, gm)  # noqa: E731
+    clocks.start()
+    ms = time_device(torch, step, args.steps, args.warmup)
+    clk = clocks.stop()
+    peak, peak_kind = measured_hbm_peak()
+    alg = gram_apply_bytes(N, B, K)
+    total = sum(alg.values())
+    roof = {"bound": "hbm", "kernel": "whole apply (embed, 2 x cuFFT, mix, extract)",
+            "achieved": round(total / (ms / 1e3) / 1e9, 1), "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+            "frac": round(total / (ms / 1e3) / 1e9 / peak, 4), "traffic": None, "algorithmic_bytes": total,
+            "algorithmic_bytes_by_stage": alg}
+    out = {"metric": "Toeplitz Gram applies/s (2D VD spiral, K=4 subspace, 16 coils)", "value": 1e3 / ms,
+           "unit": "applies/s", "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+           "config": {"workload": "Toeplitz Gram with per-voxel 4x4 mixing", "image": [N, N], "coils": B,
+                      "frames": F, "interleaves": 16, "samples_per_interleave": 2048, "K": K,
+                      "embedding": [2 * N, 2 * N], "plan_seconds": round(plan_s, 3),
+                      "l2": "per-apply grids 16 x 4 x 440^2 complex64 = 99 MB (close to L2)"},
+           "roofline": roof, "clocks": clk}
+    # error against the exact operator: an unnormalised plan (the default divides the
+    # kernel by a scalar, as the reference does) applied to coil 0, vs float64
+    gx = pf.plan_spgram(torch.as_tensor(coord, device=dev), (N, N), basis=torch.as_tensor(basis, device=dev),
+                        device=dev, normalize=None)
+    got = pf.sparse_gram(x[:1], gx)[0]
+    ref = nudft2_normal_subspace_fp64(torch, x[0], coord, basis)
+    out["vs_fp64"] = {"rel_l2": rel_l2_t(torch, got, ref), "reference": "float64 direct-NUDFT normal operator "
+                      "sum_t conj(B_t) A_t^H A_t B_t^T x, coil 0, unnormalised plan", "target": 1e-4}
+    out["vs_fp64"]["meets_target"] = bool(out["vs_fp64"]["rel_l2"] <= 1e-4)
+    del gx
+    if cpu:
+        from oracle import nufft_oracle as orc
+
+        t0 = time.perf_counter()
+        og = orc.plan_spgram(coord, (N, N), basis=basis)
+        oplan_s = time.perf_counter() - t0
+        xc = x.cpu().numpy()
+        t1 = time.perf_counter()
+        ro = orc.sparse_gram(xc, og)
+        cpu_s = time.perf_counter() - t1
+        gpu_out = step().cpu().numpy()
+        out["parity"] = {"rel_l2_apply": float(orc.rel_l2(gpu_out, ro)),
+                         "rel_l2_kernel": float(orc.rel_l2(gm.value.cpu().numpy(), og.value)),
+                         "vs": "oracle, all 16 coils", "tolerance": 1e-5}
+        out["parity"]["pass"] = bool(max(out["parity"]["rel_l2_apply"], out["parity"]["rel_l2_kernel"]) <= 1e-5)
+        out["cpu_baseline"] = {"value": 1.0 / cpu_s, "unit": "applies/s", "cores": orc.lib().orc_num_threads(),
+                               "kind": "port", "sample": "one full apply, all 16 coils (NumPy einsum + pocketfft); "
+                               f"plan {oplan_s:.2f} s timed separately"}
+    out["_launch"] = step
+    return out
+
+
+def b0_exact_fp64(torch, x, coord, times, b0, chunk=1024):
+    """y_m = sum_r x(r) exp(-2 pi i (k_m . r / N + t_m b0(r))) in float64 (2D):
+    the exact off-resonance model the time segmentation approximates."""
+    dev = x.device
+    Ny, Nx = x.shape
+    yy, xx = torch.meshgrid(torch.arange(Ny, dtype=torch.float64, device=dev) - Ny // 2,
+                            torch.arange(Nx, dtype=torch.float64, device=dev) - Nx // 2, indexing="ij")
+    xv = x.to(torch.complex128).reshape(-1)
+    bv = torch.as_tensor(b0, device=dev).to(torch.float64).reshape(-1)
+    k = torch.as_tensor(np.asarray(coord, np.float64), device=dev)
+    t = torch.as_tensor(np.asarray(times, np.float64), device=dev)
+    out = []
+    for m0 in range(0, k.shape[0], chunk):
+        ph = (k[m0:m0 + chunk, :1] * xx.reshape(1, -1) / Nx + k[m0:m0 + chunk, 1:2] * yy.reshape(1, -1) / Ny
+              + t[m0:m0 + chunk, None] * bv[None])
+        out.append(torch.exp(-2j * math.pi * ph) @ xv)
+    return torch.cat(out)
+
+
+def wl_cfg4(torch, pf, dev, args, clocks, cpu=True):
+    """B0-corrected dynamic radial: 64 frames of 5-55 spokes, L = 8, 12 coils.
+    "plain" = one forward and one adjoint call per frame (per-frame plans, each
+    call one launch per stage over 12 coils x 8 segments); "batched" = one call
+    over all frames (ragged plan); "graph" = the batched call captured in a CUDA
+    graph."""
+    N, B, F, Lseg, nread = 192, 12, 64, 8, 256
+    rng = np.random.default_rng(0)
+    nsp = rng.integers(5, 56, F)
+    starts = np.concatenate([[0], np.cumsum(nsp)[:-1]])
+    frames = [radial_2d(int(n), nread, N, start=int(s0)) for n, s0 in zip(nsp, starts)]
+    b0 = smooth_field(N)
+    dt = 5e-3 / nread
+    kw = dict(width=4, oversamp=1.25, zmap=torch.as_tensor(b0, device=dev), L=Lseg, nbins=40, dt=dt, device=dev)
+    plans = [pf.plan_nufft(torch.as_tensor(c, device=dev), (N, N), **kw) for c in frames]
+    bplan = pf.plan_nufft([torch.as_tensor(c, device=dev) for c in frames], (N, N), **kw)
+    maps = maps_2d(torch, N, B, dev)
+    x = torch.stack([maps * phantom_2d(torch, N, dev, seed=f)[None] for f in range(F)], 1).contiguous()
+    Mtot = int(nsp.sum()) * nread
+
+    def plain():
+        for f in range(F):
+            pf.nufft_adj(pf.nufft(x[:, f], nufft_plan=plans[f]), nufft_plan=plans[f])
+
+    def batched():
+        return pf.nufft_adj(pf.nufft(x, nufft_plan=bplan), nufft_plan=bplan)
+
+    ms_plain = time_device(torch, plain, args.steps, args.warmup)
+    ms_batch = time_device(torch, batched, args.steps, args.warmup)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            batched()
+    torch.cuda.current_stream().wait_stream(s)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        batched()
+    clocks.start()
+    ms_graph = time_device(torch, graph.replay, args.steps, args.warmup)
+    clk = clocks.stop()
+    del graph
+    stages = stage_times(torch, pf, bplan, x, 5)
+    peak, peak_kind = measured_hbm_peak()
+    roof = stage_roofline(stages, stage_bytes(bplan, B, F, Lseg), peak, peak_kind)
+    out = {"metric": "B0-corrected NUFFT fwd+adj samples/s, batched graph-captured (2D radial, 64 uneven frames)",
+           "value": B * Mtot / (ms_graph / 1e3), "unit": "samples/s", "ms_per_step": ms_graph,
+           "steps": args.steps, "warmup": args.warmup,
+           "config": {"workload": "B0 time-segmented dynamic radial fwd+adj", "image": [N, N], "coils": B,
+                      "frames": F, "spokes_per_frame": [int(v) for v in nsp], "readout": nread,
+                      "segments": Lseg, "oversamp": 1.25, "width": 4, "samples_per_coil": Mtot,
+                      "plain": "one nufft + one nufft_adj call per frame with per-frame plans (64 + 64 calls), "
+                               "each call one launch per stage over 12 coils x 8 segments",
+                      "batched": "one nufft + one nufft_adj call over all 64 frames (ragged plan)",
+                      "l2": "grids 64 x 96 x 240^2 complex64 = 2.8 GB, larger than L2"},
+           "plain_ms": ms_plain, "batched_ms": ms_batch, "batched_graph_ms": ms_graph,
+           "plain_samples_per_s": B * Mtot / (ms_plain / 1e3), "batched_over_plain": ms_plain / ms_graph,
+           "roofline": roof, "clocks": clk}
+    # error against the exact off-resonance model, coil 0, 10240 seeded samples
+    yb = pf.nufft(x, nufft_plan=bplan)
+    offs = bplan.interpolator.frame_offsets
+    allc = np.concatenate([c.reshape(-1, 2) for c in frames])
+    fidx = np.concatenate([np.full(int(offs[f + 1] - offs[f]), f) for f in range(F)])
+    tm = np.concatenate([np.tile(np.arange(nread) * dt, int(n)) for n in nsp])
+    sel = np.sort(np.random.default_rng(0).choice(Mtot, 10240, replace=False))
+    ref = torch.cat([b0_exact_fp64(torch, x[0, f], allc[sel][fidx[sel] == f], tm[sel][fidx[sel] == f], b0)
+                     for f in np.unique(fidx[sel])])
+    got = yb[0, torch.as_tensor(sel, device=dev)]
+    out["vs_fp64"] = {"rel_l2": rel_l2_t(torch, got, ref), "samples": 10240, "coil": 0, "target": 1e-4,
+                      "reference": "float64 exact off-resonance model exp(-2 pi i (k r / N + t b0(r))): "
+                                   "includes the L = 8 time-segmentation error"}
+    out["vs_fp64"]["meets_target"] = bool(out["vs_fp64"]["rel_l2"] <= 1e-4)
+    if cpu:
+        from oracle import nufft_oracle as orc
+
+        nf = 16
+        okw = dict(width=4, oversamp=1.25, zmap=b0, L=Lseg, nbins=40, dt=dt)
+        t0 = time.perf_counter()
+        oplans = [orc.plan_nufft(c, (N, N), **okw) for c in frames[:nf]]
+        oplan_s = time.perf_counter() - t0
+        xc = x[:, :nf].cpu().numpy()
+        t1 = time.perf_counter()
+        ys = [orc.nufft_fwd(xc[:, f], oplans[f]) for f in range(nf)]
+        xs = [orc.nufft_adj(ys[f], oplans[f]) for f in range(nf)]
+        cpu_s = time.perf_counter() - t1
+        ybh = yb.cpu().numpy()
+        xa = pf.nufft_adj(torch.as_tensor(np.concatenate([v.reshape(B, -1) for v in ys], 1), device=dev),
+                          nufft_plan=pf.plan_nufft([torch.as_tensor(c, device=dev) for c in frames[:nf]], (N, N),
+                                                   **kw))
+        e_f = orc.rel_l2(ybh[:, :int(offs[nf])], np.concatenate([v.reshape(B, -1) for v in ys], 1))
+        e_a = orc.rel_l2(xa.cpu().numpy(), np.stack(xs, 1))
+        out["parity"] = {"rel_l2_fwd": float(e_f), "rel_l2_adj": float(e_a), "tolerance": 1e-5,
+                         "pass": bool(max(e_f, e_a) <= 1e-5),
+                         "vs": f"oracle, frames 0-{nf - 1}, all 12 coils, all 8 segments"}
+        nsamp = B * int(nsp[:nf].sum()) * nread
+        out["cpu_baseline"] = {"value": nsamp / cpu_s, "unit": "samples/s", "cores": orc.lib().orc_num_threads(),
+                               "kind": "port", "sample": f"{nf} of 64 frames, all coils, per-frame fwd+adj with "
+                               f"B0 (L = 8); plans {oplan_s:.2f} s timed separately"}
+    out["_launch"] = batched
+    return out
+
+
+def wl_cfg5(torch, pf, dev, args, clocks, cpu=True):
+    """Differentiable NUFFT: 2D VD spiral 16 x 4096, 256^2, 8 coils x 32 images,
+    loss ||A^H A x - x||^2, image and trajectory gradients."""
+    N, B, nimg = 256, 8, 32
+    coord = vd_spiral(16, 4096, N)
+    ct = torch.as_tensor(coord, device=dev).requires_grad_(True)
+    plan = pf.plan_nufft(ct.detach(), (N, N), width=4, oversamp=2.0, device=dev)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.complex(torch.randn(nimg, B, N, N, generator=g), torch.randn(nimg, B, N, N, generator=g)).to(dev)
+    x.requires_grad_(True)
+
+    def step():
+        y = pf.nufft(x, ct, nufft_plan=plan, norm="ortho")
+        z = pf.nufft_adj(y, ct, nufft_plan=plan, norm="ortho")
+        loss = torch.sum(torch.abs(z - x) ** 2)
+        loss.backward()
+        return loss
+
+    clocks.start()
+    ms = time_device(torch, step, args.steps, args.warmup)
+    clk = clocks.stop()
+    M = 16 * 4096
+    peak, peak_kind = measured_hbm_peak()
+    sb = stage_bytes(plan, nimg * B)
+    fwd_b = sb["pad"] + sb["fft"] + sb["transpose"] + sb["interp"] + sb["out"]
+    adj_b = sb["vals"] + sb["spread"] + sb["ifft"] + sb["crop"]
+    tot = 2 * fwd_b + 2 * adj_b + 2 * (sb["pad"] + sb["fft"] + sb["transpose"] + sb["interp"])
+    out = {"metric": "differentiable NUFFT step samples/s (fwd+adj+backward incl. trajectory gradient)",
+           "value": nimg * B * M / (ms / 1e3), "unit": "samples/s", "ms_per_step": ms, "steps": args.steps,
+           "warmup": args.warmup,
+           "config": {"workload": "loss ||A^H A x - x||^2 with image and trajectory gradients", "image": [N, N],
+                      "coils": B, "images": nimg, "interleaves": 16, "samples": 4096, "oversamp": 2.0, "width": 4,
+                      "norm": "ortho", "l2": "grids 256 x 512^2 complex64 = 537 MB, larger than L2"},
+           "roofline": {"bound": "hbm", "kernel": "whole step (2 forward, 2 adjoint, 2 trajectory-gradient passes)",
+                        "achieved": round(tot / (ms / 1e3) / 1e9, 1), "peak": peak, "peak_source": peak_kind,
+                        "unit": "GB/s", "frac": round(tot / (ms / 1e3) / 1e9 / peak, 4), "traffic": None,
+                        "algorithmic_bytes": tot},
+           "clocks": clk}
+    with torch.no_grad():
+        y0 = pf.nufft(x[0, :1].detach(), nufft_plan=plan)
+    sel = np.sort(np.random.default_rng(0).choice(M, 10240, replace=False))
+    ref = nudft_fwd_fp64(torch, x[0, 0].detach(), coord.reshape(-1, 2)[sel])
+    out["vs_fp64"] = {"rel_l2_fwd": rel_l2_t(torch, y0.reshape(-1)[torch.as_tensor(sel, device=dev)], ref),
+                      "samples": 10240, "target": 1e-4,
+                      "note": "kernel accuracy of W 4 at osf 2 (the reference's kernel gives the same error)"}
+    out["vs_fp64"]["meets_target"] = bool(out["vs_fp64"]["rel_l2_fwd"] <= 1e-4)
+    if cpu:
+        from oracle import nufft_oracle as orc
+
+        op = orc.plan_nufft(coord, (N, N), width=4, oversamp=2.0)
+        xs = x[:4].detach().cpu().numpy()
+        t1 = time.perf_counter()
+        # the reference's differentiable step: forward + adjoint, then the backward's
+        # adjoint and forward (image gradients) and d extra forwards for the
+        # trajectory gradient (_nufft/_nufft.py:175-209)
+        yo = orc.nufft_fwd(xs, op, norm="ortho")
+        zo = orc.nufft_adj(yo, op, norm="ortho")
+        orc.nufft_fwd(zo, op, norm="ortho")
+        orc.nufft_adj(yo, op, norm="ortho")
+        for _ in range(2):
+            orc.nufft_fwd(xs, op, norm="ortho")
+        cpu_s = time.perf_counter() - t1
+        yg = pf.nufft(x[:4].detach(), nufft_plan=plan, norm="ortho")
+        zg = pf.nufft_adj(torch.as_tensor(yo, device=dev), nufft_plan=plan, norm="ortho")
+        e_f, e_a = orc.rel_l2(yg.cpu().numpy(), yo), orc.rel_l2(zg.cpu().numpy(), zo)
+        out["parity"] = {"rel_l2_fwd": float(e_f), "rel_l2_adj": float(e_a), "tolerance": 1e-5,
+                         "pass": bool(max(e_f, e_a) <= 1e-5), "vs": "oracle, 4 of 32 images, 8 coils, norm ortho"}
+        out["cpu_baseline"] = {"value": 4 * B * M / cpu_s, "unit": "samples/s", "cores": orc.lib().orc_num_threads(),
+                               "kind": "port", "sample": "4 of 32 images x 8 coils: 4 forward + 2 adjoint NUFFTs "
+                               "(the reference's step with its d = 2 trajectory-gradient forwards)"}
+    out["_launch"] = step
+    return out
+
+
+SUB_WORKLOADS = {"cfg3": wl_cfg3, "cfg4": wl_cfg4, "cfg5": wl_cfg5}
+
+
 def extra_workload(args):
     """2D radial (cfg1), Toeplitz Gram (cfg3), B0 plain vs batched (cfg4), autograd (cfg5), Pipe-Menon DCF (dcf),
     sparse FFT (spfft), Cartesian Gram (cgram), GROG pre-interpolation (grog)."""
@@ -580,82 +997,11 @@ def extra_workload(args):
                             "readout": 256, "oversamp": 2.0, "width": 4, "l2": "fits in L2 (4 MB grids)"},
                     cpu_baseline={"value": B * M / cpu_s, "unit": "samples/s", "cores": orc.lib().orc_num_threads(),
                                   "kind": "port", "sample": "all 8 coils, median of 3 fwd+adj"})
-    elif args.workload == "cfg3":
-        N, B, F, K = 220, 16, 48, 4
-        coord = np.stack([vd_spiral(16, 2048, N, rot=f * np.pi * (3 - 5 ** 0.5)) for f in range(F)])
-        basis = exp_recovery_basis(K, nt=F)
-        t0 = time.perf_counter()
-        gm = pf.plan_spgram(torch.as_tensor(coord, device=dev), (N, N), basis=torch.as_tensor(basis, device=dev),
-                            device=dev)
-        torch.cuda.synchronize()
-        plan_s = time.perf_counter() - t0
-        g = torch.Generator(device="cpu").manual_seed(0)
-        x = torch.complex(torch.randn(B, K, N, N, generator=g), torch.randn(B, K, N, N, generator=g)).to(dev)
-        step = lambda: pf.sparse_gram(x, gm)  # noqa: E731
-        clocks.start()
-        ms = time_device(torch, step, args.steps, args.warmup)
-        clk = clocks.stop()
-        og = orc.plan_spgram(coord, (N, N), basis=basis)
-        xc = x.cpu().numpy()
-        orc.sparse_gram(xc, og)
-        t1 = time.perf_counter()
-        orc.sparse_gram(xc, og)
-        cpu_s = time.perf_counter() - t1
-        line.update(metric="Toeplitz Gram applies/s (2D VD spiral, K=4 subspace, 16 coils)", value=1e3 / ms,
-                    unit="applies/s", ms_per_step=ms,
-                    config={"workload": "Toeplitz Gram with per-voxel 4x4 mixing", "image": [N, N], "coils": B,
-                            "frames": F, "interleaves": 16, "samples_per_interleave": 2048, "K": K,
-                            "embedding": [2 * N, 2 * N], "plan_seconds": round(plan_s, 3)},
-                    cpu_baseline={"value": 1.0 / cpu_s, "unit": "applies/s", "cores": orc.lib().orc_num_threads(),
-                                  "kind": "port", "sample": "one full apply (NumPy einsum + pocketfft)"})
-    elif args.workload == "cfg4":
-        N, B, F, Lseg, nread = 192, 12, 64, 8, 256
-        rng = np.random.default_rng(0)
-        nsp = rng.integers(5, 56, F)
-        starts = np.concatenate([[0], np.cumsum(nsp)[:-1]])
-        frames = [radial_2d(int(n), nread, N, start=int(s0)) for n, s0 in zip(nsp, starts)]
-        b0 = smooth_field(N)
-        dt = 5e-3 / nread
-        kw = dict(width=4, oversamp=1.25, zmap=torch.as_tensor(b0, device=dev), L=Lseg, nbins=40, dt=dt, device=dev)
-        plans = [pf.plan_nufft(torch.as_tensor(c, device=dev), (N, N), **kw) for c in frames]
-        bplan = pf.plan_nufft([torch.as_tensor(c, device=dev) for c in frames], (N, N), **kw)
-        maps = maps_2d(torch, N, B, dev)
-        x = torch.stack([maps * phantom_2d(torch, N, dev, seed=f)[None] for f in range(F)], 1).contiguous()
-        Mtot = int(nsp.sum()) * nread
-
-        def plain():
-            for f in range(F):
-                pf.nufft_adj(pf.nufft(x[:, f], nufft_plan=plans[f]), nufft_plan=plans[f])
-
-        def batched():
-            return pf.nufft_adj(pf.nufft(x, nufft_plan=bplan), nufft_plan=bplan)
-
-        ms_plain = time_device(torch, plain, args.steps, args.warmup)
-        ms_batch = time_device(torch, batched, args.steps, args.warmup)
-        s = torch.cuda.Stream()
-        s.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(s):
-            for _ in range(2):
-                batched()
-        torch.cuda.current_stream().wait_stream(s)
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph):
-            batched()
-        clocks.start()
-        ms_graph = time_device(torch, graph.replay, args.steps, args.warmup)
-        clk = clocks.stop()
-        value = B * Mtot / (ms_graph / 1e3)
-        stages = stage_times(torch, pf, bplan, x, 5)
-        line.update(metric="B0-corrected NUFFT fwd+adj samples/s, batched graph-captured (2D radial, 64 uneven frames)",
-                    value=value, unit="samples/s", ms_per_step=ms_graph,
-                    config={"workload": "B0 time-segmented dynamic radial fwd+adj", "image": [N, N], "coils": B,
-                            "frames": F, "spokes_per_frame": [int(v) for v in nsp], "readout": nread,
-                            "segments": Lseg, "oversamp": 1.25, "width": 4,
-                            "plain_ms": ms_plain, "batched_ms": ms_batch, "batched_graph_ms": ms_graph,
-                            "plain_samples_per_s": B * Mtot / (ms_plain / 1e3),
-                            "batched_over_plain": ms_plain / ms_graph,
-                            "batched_stages_ms": {k: round(v, 4) for k, v in stages.items()}},
-                    cpu_baseline=None)
+    elif args.workload in SUB_WORKLOADS:
+        sub = SUB_WORKLOADS[args.workload](torch, pf, dev, args, clocks, cpu=not args.no_cpu_baseline)
+        clk = sub.pop("clocks")
+        launch_fn = sub.pop("_launch")
+        line.update(sub)
     elif args.workload == "spfft":
         # 3D Cartesian acquisition, 25 % of the (ky, kz) phase encodes, full readouts
         N, B = 128, 32
@@ -789,32 +1135,8 @@ def extra_workload(args):
                     cpu_baseline={"value": 1.0 / cpu_s, "unit": "iterations/s", "cores": orc.lib().orc_num_threads(),
                                   "kind": "port", "sample": "one iteration of the oracle's pipe_menon_dcf "
                                                             "(plan build included)"})
-    elif args.workload == "cfg5":
-        N, B, nimg = 256, 8, 32
-        coord = vd_spiral(16, 4096, N)
-        ct = torch.as_tensor(coord, device=dev).requires_grad_(True)
-        plan = pf.plan_nufft(ct.detach(), (N, N), width=4, oversamp=2.0, device=dev)
-        g = torch.Generator(device="cpu").manual_seed(0)
-        x = torch.complex(torch.randn(nimg, B, N, N, generator=g), torch.randn(nimg, B, N, N, generator=g)).to(dev)
-        x.requires_grad_(True)
-
-        def step():
-            y = pf.nufft(x, ct, nufft_plan=plan, norm="ortho")
-            z = pf.nufft_adj(y, ct, nufft_plan=plan, norm="ortho")
-            loss = torch.sum(torch.abs(z - x) ** 2)
-            loss.backward()
-            return loss
-
-        clocks.start()
-        ms = time_device(torch, step, args.steps, args.warmup)
-        clk = clocks.stop()
-        M = 16 * 4096
-        line.update(metric="differentiable NUFFT step samples/s (fwd+adj+backward incl. trajectory gradient)",
-                    value=nimg * B * M / (ms / 1e3), unit="samples/s", ms_per_step=ms,
-                    config={"workload": "loss ||A^H A x - x||^2 with image and trajectory gradients",
-                            "image": [N, N], "coils": B, "images": nimg, "interleaves": 16, "samples": 4096},
-                    cpu_baseline=None)
-    launch_fn = batched if args.workload == "cfg4" else step
+    if args.workload not in SUB_WORKLOADS:
+        launch_fn = step
     if not args.no_launch_trace:
         mine_l, all_l = count_launches(torch, launch_fn)
         line["gpu_launches"] = mine_l * args.steps
@@ -838,7 +1160,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg1", "cfg3", "cfg4", "cfg5", "dcf", "spfft",
                                                                       "cgram", "grog"])
-    ap.add_argument("--cpu-coils", type=int, default=2, help="coils in the bounded CPU baseline sample")
+    ap.add_argument("--cpu-coils", type=int, default=0,
+                    help="coils in the bounded CPU baseline sample (default: one per oracle thread, at most 32)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="headline workload only (skip the Gram, B0 and differentiable sub-workloads)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-launch-trace", action="store_true",
                     help="skip the CUDA activity trace that counts launches (for runs under ncu)")
@@ -859,17 +1184,39 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        coord = golden_means_radial_3d(wl["nspokes"], wl["nread"], wl["N"])
-        res = cpu_baseline(wl, coord, args.cpu_coils, steps=max(1, args.steps))
-        sample = (f"{args.cpu_coils} of {wl['coils']} coils, full trajectory "
-                  f"({wl['nspokes'] * wl['nread']} samples/coil), median of {max(1, args.steps)} fwd+adj")
-        line = {"metric": METRIC, "value": res["value"], "unit": "samples/s", "impl": "reference",
+        from oracle import nufft_oracle as orc
+
+        cpu_coils = args.cpu_coils or default_cpu_coils(wl["coils"])
+
+        N = wl["N"]
+        coord = golden_means_radial_3d(wl["nspokes"], wl["nread"], N)
+        rng = np.random.default_rng(1)
+        x = (rng.standard_normal((cpu_coils, N, N, N), np.float32)
+             + 1j * rng.standard_normal((cpu_coils, N, N, N), np.float32)).astype(np.complex64)
+        t0 = time.perf_counter()
+        plan = orc.plan_nufft(coord, (N, N, N), width=wl["width"], oversamp=wl["oversamp"])
+        plan_s = time.perf_counter() - t0
+        # warm-up steps: thread pools and first touch of the plan tables, one coil each
+        for _ in range(args.warmup):
+            orc.nufft_adj(orc.nufft_fwd(x[:1], plan), plan)
+        times = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            orc.nufft_adj(orc.nufft_fwd(x, plan), plan)
+            times.append(time.perf_counter() - t0)
+        t = statistics.median(times)
+        value = cpu_coils * coord.shape[0] * coord.shape[1] / t
+        threads = orc.lib().orc_num_threads()
+        sample = (f"{cpu_coils} of {wl['coils']} coils (one per oracle thread), full trajectory "
+                  f"({wl['nspokes'] * wl['nread']} samples/coil), median of {max(1, args.steps)} fwd+adj; "
+                  f"warm-up steps of one coil; plan build {plan_s:.2f} s timed separately")
+        line = {"metric": METRIC, "value": value, "unit": "samples/s", "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": res["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+                "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "complex64", "data": "synthetic (seeded)", "config": config,
-                "cpu_baseline": {"value": res["value"], "unit": "samples/s", "cores": res["threads"],
-                                 "kind": "port", "sample": sample},
-                "e2e": {"value": res["value"], "unit": "samples/s", "h2d_bytes_per_step": 0,
+                "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "port",
+                                 "sample": sample, "plan_seconds": plan_s, "cpu_count": os.cpu_count()},
+                "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -884,12 +1231,15 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     r = gpu_arm(args, wl, rank, world, local_rank)
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        res = cpu_baseline(wl, r["coord"], args.cpu_coils, steps=1)
+        cpu_coils = args.cpu_coils or default_cpu_coils(wl["coils"])
+        parity, res = parity_cfg2(torch, wl, r, cpu_coils)
         cpu = {"value": res["value"], "unit": "samples/s", "cores": res["threads"], "kind": "port",
-               "sample": f"{args.cpu_coils} of {wl['coils']} coils, full trajectory, one fwd+adj "
-                         "(oracle: C restatement of the reference's Numba kernels + NumPy/pocketfft glue)"}
+               "sample": f"{cpu_coils} of {wl['coils']} coils (one per oracle thread), full trajectory, one fwd+adj "
+                         "(oracle: C restatement of the reference's Numba kernels + NumPy/pocketfft glue); "
+                         f"plan build {res['plan_seconds']:.2f} s timed separately",
+               "plan_seconds": res["plan_seconds"], "cpu_count": res["cpu_count"]}
     if rank == 0:
         config["stages_ms"] = {k: round(v, 4) for k, v in r["stages"].items()}
         line = {"metric": METRIC, "value": r["value"], "unit": "samples/s", "n_gpus": world, "steps": args.steps,
@@ -900,7 +1250,27 @@ def main():
                 "gpu_launches": (r["launches_per_step"] or 0) * args.steps,
                 "kernels_per_step": {"pyfourier_b200": r["launches_per_step"],
                                      "all (incl. cuFFT)": r["kernels_per_step"]},
-                "roofline": r["roofline"], "cpu_baseline": cpu, "clocks": r["clocks"]}
+                "roofline": r["roofline"], "cpu_baseline": cpu, "parity": parity, "clocks": r["clocks"]}
+        for k in ("x", "y", "xa", "plan"):
+            r.pop(k, None)
+        torch.cuda.empty_cache()
+        if world == 1 and not args.no_extra:
+            # the rest of the metric (Gram applies/s, batched vs plain, the differentiable
+            # step), each in its own timed region after the headline measurement
+            import pyfourier_b200 as pf
+
+            dev = torch.device(f"cuda:{local_rank}")
+            subs = {}
+            for name, fn in SUB_WORKLOADS.items():
+                sub = fn(torch, pf, dev, args, ClockSampler(local_rank), cpu=not args.no_cpu_baseline)
+                launch = sub.pop("_launch")
+                if not args.no_launch_trace:
+                    mine_l, all_l = count_launches(torch, launch)
+                    sub["gpu_launches"] = mine_l * args.steps
+                    sub["kernels_per_step"] = {"pyfourier_b200": mine_l, "all (incl. cuFFT, torch)": all_l}
+                subs[name] = sub
+                torch.cuda.empty_cache()
+            line["workloads"] = subs
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

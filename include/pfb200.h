@@ -156,14 +156,17 @@ int pfb_nufft_adj(pfb_plan *plan, const pfb_apply_t *opt, const void *kspace, vo
  * counterpart in the reference.  It exists for callers that cannot call
  * cudaMalloc at apply time: code running inside a host framework that owns all
  * device memory through its own pool, real-time loops with a fixed memory
- * budget, processes that must not grow after start-up.  Same result as
- * pfb_nufft_adj; its scratch (grid + cuFFT work area) is one static device
- * array of PFB_NOALLOC_SCRATCH_BYTES, held by every GPU that loads it until the
- * process exits.  Larger requests are rejected (PFB_ERR_INVALID).  Set-up: the
- * first call on a device looks up the array's address (make it before any
- * stream capture), and pfb_workspace_size(plan, nplanes) must have been called
- * once to create the cuFFT plan.  All calls share the array: calls that overlap
- * on the GPU race and must be serialised by the caller. */
+ * budget, processes that must not grow after set-up.  Same result as
+ * pfb_nufft_adj and the same argument checks; its scratch (grid + cuFFT work
+ * area) is one static device array of PFB_NOALLOC_SCRATCH_BYTES.  Larger
+ * requests are rejected (PFB_ERR_INVALID).  Set-up, once per device: a call
+ * with opt->batch == 0 (kspace and image may then be NULL) looks up the array's
+ * address; CUDA loads the array lazily, so that call is when the 64 MiB are
+ * reserved on the device, until the process exits.  Make it before any stream
+ * capture (otherwise the first real call does it).  pfb_workspace_size(plan,
+ * nplanes) must also have been called once to create the cuFFT plan.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller. */
 #define PFB_NOALLOC_SCRATCH_BYTES (64u << 20)
 int pfb_nufft_adj_noalloc(pfb_plan *plan, const pfb_apply_t *opt, const void *kspace, void *image,
                           void *stream);

@@ -85,9 +85,15 @@ int get_fft_plan(std::mutex &mu, std::map<int64_t, cufftHandle> &plans, std::map
     return PFB_OK;
 }
 
-int run_fft(cufftHandle h, size_t wbytes, float2 *data, int direction, void *work, size_t work_avail,
-            cudaStream_t s) {
+// The plan's cuFFT handle is shared by every apply on the plan: its stream and
+// work area are set per call, so `mu` (the plan's fft_mu) is held from
+// cufftSetStream to the end of cufftExecC2C, and concurrent applies of one plan
+// from several host threads cannot run one call's transform with another's work
+// area.
+int run_fft(std::mutex &mu, cufftHandle h, size_t wbytes, float2 *data, int direction, void *work,
+            size_t work_avail, cudaStream_t s) {
     if (wbytes > work_avail) return fail(PFB_ERR_WORKSPACE, "workspace too small for the cuFFT work area");
+    std::lock_guard<std::mutex> lk(mu);
     PFB_CUFFT_TRY(cufftSetStream(h, s));
     PFB_CUFFT_TRY(cufftSetWorkArea(h, work));
     PFB_CUFFT_TRY(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(data), reinterpret_cast<cufftComplex *>(data),
@@ -95,9 +101,10 @@ int run_fft(cufftHandle h, size_t wbytes, float2 *data, int direction, void *wor
     return PFB_OK;
 }
 
-int run_fft_to(cufftHandle h, size_t wbytes, const float2 *src, float2 *dst, int direction, void *work,
-               size_t work_avail, cudaStream_t s) {
+int run_fft_to(std::mutex &mu, cufftHandle h, size_t wbytes, const float2 *src, float2 *dst, int direction,
+               void *work, size_t work_avail, cudaStream_t s) {
     if (wbytes > work_avail) return fail(PFB_ERR_WORKSPACE, "workspace too small for the cuFFT work area");
+    std::lock_guard<std::mutex> lk(mu);
     PFB_CUFFT_TRY(cufftSetStream(h, s));
     PFB_CUFFT_TRY(cufftSetWorkArea(h, work));
     // a C2C transform leaves an out-of-place input unchanged
@@ -105,8 +112,6 @@ int run_fft_to(cufftHandle h, size_t wbytes, const float2 *src, float2 *dst, int
                                reinterpret_cast<cufftComplex *>(dst), direction < 0 ? CUFFT_FORWARD : CUFFT_INVERSE));
     return PFB_OK;
 }
-
-namespace {
 
 int to_desc(const pfb_plan *p, const pfb_apply_t *o, ApplyDesc &d) {
     if (!o) return fail(PFB_ERR_INVALID, "apply options are NULL");
@@ -130,6 +135,8 @@ int to_desc(const pfb_plan *p, const pfb_apply_t *o, ApplyDesc &d) {
         return fail(PFB_ERR_INVALID, "too many channels");
     return PFB_OK;
 }
+
+namespace {
 
 int64_t planes_of(const ApplyDesc &d) { return (int64_t)d.nseg * d.batch * d.ncoeff; }
 
@@ -248,7 +255,7 @@ int pfb_grid_fft(pfb_plan *p, void *grid, int64_t nplanes, int direction, void *
     size_t wb = 0;
     int st = get_fft_plan(p->fft_mu, p->fft_plans, p->fft_work, p->g.ndim, p->g.nos, nplanes, &h, &wb);
     if (st) return st;
-    return run_fft(h, wb, static_cast<float2 *>(grid), direction, workspace, workspace_bytes,
+    return run_fft(p->fft_mu, h, wb, static_cast<float2 *>(grid), direction, workspace, workspace_bytes,
                    static_cast<cudaStream_t>(stream));
 }
 
@@ -278,7 +285,7 @@ int pfb_nufft_fwd(pfb_plan *p, const pfb_apply_t *opt, const void *image, void *
     float2 *grid = static_cast<float2 *>(workspace);
     void *work = static_cast<char *>(workspace) + gbytes;
     if ((st = launch_deapod_pad(p, d, static_cast<const float2 *>(image), grid, (float)fac, s))) return st;
-    if ((st = run_fft(h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
+    if ((st = run_fft(p->fft_mu, h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
     return launch_interp(p, d, grid, static_cast<float2 *>(kspace), true, s, opt->flags & PFB_FLAG_ACCUMULATE);
 }
 
@@ -307,7 +314,7 @@ int pfb_nufft_adj(pfb_plan *p, const pfb_apply_t *opt, const void *kspace, void 
     float2 *grid = static_cast<float2 *>(workspace);
     void *work = static_cast<char *>(workspace) + gbytes;
     if ((st = launch_spread(p, d, static_cast<const float2 *>(kspace), grid, true, s))) return st;
-    if ((st = run_fft(h, wb, grid, +1, work, workspace_bytes - gbytes, s))) return st;
+    if ((st = run_fft(p->fft_mu, h, wb, grid, +1, work, workspace_bytes - gbytes, s))) return st;
     return launch_crop_deapod(p, d, grid, static_cast<float2 *>(image), (float)fac, s,
                               opt->flags & PFB_FLAG_ACCUMULATE);
 }
@@ -357,7 +364,7 @@ int pfb_nufft_traj_grad(pfb_plan *p, const pfb_apply_t *opt, const void *image, 
     float2 *grid = static_cast<float2 *>(workspace);
     void *work = static_cast<char *>(workspace) + gbytes;
     if ((st = launch_deapod_pad(p, d, static_cast<const float2 *>(image), grid, factor, s))) return st;
-    if ((st = run_fft(h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
+    if ((st = run_fft(p->fft_mu, h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
     return launch_traj_grad(p, d, grid, static_cast<const float2 *>(values), grad, true, s, acc);
 }
 
@@ -531,11 +538,11 @@ int pfb_gram_apply(pfb_gram *g, const void *image, void *out, int64_t batch, con
         // embed / extract copies)
         if (workspace_bytes < wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
         float2 *o = static_cast<float2 *>(out);
-        if ((st = run_fft_to(h, wb, static_cast<const float2 *>(image), o, -1, workspace, workspace_bytes, s)))
+        if ((st = run_fft_to(g->fft_mu, h, wb, static_cast<const float2 *>(image), o, -1, workspace, workspace_bytes, s)))
             return st;
         if ((st = launch_mix(g->gvol, g->K, g->lowrank, batch, g->d_T, o, s, (float)(1.0 / (double)g->gvol))))
             return st;
-        return run_fft(h, wb, o, +1, workspace, workspace_bytes, s);
+        return run_fft(g->fft_mu, h, wb, o, +1, workspace, workspace_bytes, s);
     }
     size_t gbytes = align_up((size_t)P * g->gvol * sizeof(float2));
     if (workspace_bytes < gbytes + wb) return fail(PFB_ERR_WORKSPACE, "workspace too small");
@@ -544,12 +551,12 @@ int pfb_gram_apply(pfb_gram *g, const void *image, void *out, int64_t batch, con
     const float2 *Cl = static_cast<const float2 *>(b0_space);
     if ((st = launch_embed(g->ndim, g->n, g->nos, static_cast<const float2 *>(image), grid, bk, Cl, L, s)))
         return st;
-    if ((st = run_fft(h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
+    if ((st = run_fft(g->fft_mu, h, wb, grid, -1, work, workspace_bytes - gbytes, s))) return st;
     const size_t tplane = (size_t)g->gvol * (g->lowrank ? (size_t)g->K * g->K : (size_t)g->K);
     for (int l = 0; l < L; ++l)  // segment l's kernel on segment l's planes
         if ((st = launch_mix(g->gvol, g->K, g->lowrank, batch, g->d_T + l * tplane, grid + l * bk * g->gvol, s)))
             return st;
-    if ((st = run_fft(h, wb, grid, +1, work, workspace_bytes - gbytes, s))) return st;
+    if ((st = run_fft(g->fft_mu, h, wb, grid, +1, work, workspace_bytes - gbytes, s))) return st;
     // forward and inverse FFT scalings multiply to 1/G whatever `norm` is
     return launch_extract(g->ndim, g->n, g->nos, grid, static_cast<float2 *>(out), bk,
                           (float)(1.0 / (double)g->gvol), Cl, L, s);

@@ -344,11 +344,15 @@ int rebuild_items(pfb_plan *p, int chunk);
 // capi.cu: planar batched cuFFT plans (cached per plane count) and execution
 int get_fft_plan(std::mutex &mu, std::map<int64_t, cufftHandle> &plans, std::map<int64_t, size_t> &work,
                  int ndim, const int *nos_xyz, int64_t nplanes, cufftHandle *out, size_t *wbytes);
-int run_fft(cufftHandle h, size_t wbytes, float2 *data, int direction, void *work, size_t work_avail,
-            cudaStream_t s);
+// Both hold `mu` (the owner's fft_mu) from cufftSetStream to the end of the exec:
+// the handle, its stream and its work area are shared by all applies of a plan.
+int run_fft(std::mutex &mu, cufftHandle h, size_t wbytes, float2 *data, int direction, void *work,
+            size_t work_avail, cudaStream_t s);
 // Out-of-place C2C transform src -> dst (src is read only; dst may equal src).
-int run_fft_to(cufftHandle h, size_t wbytes, const float2 *src, float2 *dst, int direction, void *work,
-               size_t work_avail, cudaStream_t s);
+int run_fft_to(std::mutex &mu, cufftHandle h, size_t wbytes, const float2 *src, float2 *dst, int direction,
+               void *work, size_t work_avail, cudaStream_t s);
+// Apply options -> ApplyDesc with every argument check of the C entry points.
+int to_desc(const pfb_plan *p, const pfb_apply_t *o, ApplyDesc &d);
 
 // fast.cu (channel-interleaved pipeline)
 int fast_supported(const pfb_plan *p, const ApplyDesc &d, std::string *why);

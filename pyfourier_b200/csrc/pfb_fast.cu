@@ -1672,7 +1672,7 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
         }
         case PFB_STAGE_FFT:
         case PFB_STAGE_IFFT:
-            return run_fft(h, wb, gridp, stage == PFB_STAGE_FFT ? -1 : +1, work, L.work, s);
+            return run_fft(p->fft_mu, h, wb, gridp, stage == PFB_STAGE_FFT ? -1 : +1, work, L.work, s);
         case PFB_STAGE_TRANSPOSE: {
             const int tc = std::min(32, pow2ceil(c.nch));
             if (tc == 32) {

@@ -4,19 +4,20 @@
 // Who needs it: code that runs where cudaMalloc is not allowed or not wanted at
 // apply time -- inside a host framework that owns all device memory through its
 // own pool, on a real-time reconstruction loop with a fixed memory budget, or
-// in a process that must never grow its footprint after start-up.  Such a
+// in a process that must never grow its footprint after set-up.  Such a
 // caller cannot provide the workspace that pfb_nufft_adj needs.
 //
 // This entry point keeps its scratch (the oversampled grid and cuFFT's work
-// area) in one file-scope device array of PFB_NOALLOC_SCRATCH_BYTES bytes.
-// Every GPU on which this part of the library is loaded holds that array
-// until the process exits.  The caller still passes the input k-space and the
-// output image.
+// area) in one file-scope device array of PFB_NOALLOC_SCRATCH_BYTES bytes.  The
+// caller still passes the input k-space and the output image.
 //
 // Rules of use:
-//   * The first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current).  Make that first call
-//     before any stream capture.
+//   * Set-up, once per device, with the plan's device current: call it with
+//     opt->batch == 0.  That call only looks up the array's device address
+//     (cudaGetSymbolAddress).  CUDA loads this file's device code lazily, so
+//     the lookup is the moment the 64 MiB array is reserved on that device; it
+//     stays reserved until the process exits.  Make the set-up call before any
+//     stream capture.  Without it, the first real call does the same lookup.
 //   * The cuFFT plan for the call's number of grid planes must already exist:
 //     call pfb_workspace_size(plan, nplanes, ...) once during set-up (that call
 //     may allocate; this one does not).  Without it the call returns
@@ -28,9 +29,15 @@
 //     that overlap on the GPU (different streams, or different threads without
 //     ordering) race on the array and give wrong results: serialise them.
 //
+// The address is looked up on every call (after the first, a table lookup in
+// the runtime that allocates nothing), so a device reset that reloads the
+// module never leaves a stale pointer behind.  Argument checks are the same
+// as pfb_nufft_adj's (pfb::to_desc).
+//
 // It calls no cudaMalloc, cudaFree or allocating library routine.
 #include <cmath>
 #include <mutex>
+#include <string>
 
 #include "pfb_common.cuh"
 
@@ -38,22 +45,13 @@ namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PFB_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_addr_mu;
-void *g_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on `dev` (which must be current).
-int scratch_address(int dev, void **out) {
-    if (dev < 0 || dev >= kMaxDevices) return pfb::fail(PFB_ERR_INVALID, "device index out of range");
-    std::lock_guard<std::mutex> lk(g_addr_mu);
-    if (!g_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return pfb::fail(PFB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-        g_addr[dev] = p;
-    }
-    *out = g_addr[dev];
+// Device address of the scratch array on the current device.
+int scratch_address(void **out) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return pfb::fail(PFB_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    *out = p;
     return PFB_OK;
 }
 
@@ -64,24 +62,11 @@ size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 extern "C" int pfb_nufft_adj_noalloc(pfb_plan *p, const pfb_apply_t *o, const void *kspace, void *image,
                                      void *stream) {
     using namespace pfb;
-    if (!p || !o || !kspace || !image) return fail(PFB_ERR_INVALID, "NULL argument");
+    if (!p || !o) return fail(PFB_ERR_INVALID, "NULL argument");
     ApplyDesc d;
-    d.batch = o->batch;
-    d.ncoeff = o->ncoeff;
-    d.basis = static_cast<const float2 *>(o->basis);
-    d.weight = o->weight;
-    d.nseg = o->nseg < 1 ? 1 : o->nseg;
-    d.b0_time = static_cast<const float2 *>(o->b0_time);
-    d.b0_space = static_cast<const float2 *>(o->b0_space);
-    d.norm = o->norm;
-    if (d.batch < 0 || d.ncoeff < 1) return fail(PFB_ERR_INVALID, "batch < 0 or ncoeff < 1");
-    if (!d.basis && d.ncoeff != p->nframes)
-        return fail(PFB_ERR_INVALID, "without a basis ncoeff must equal the number of frames");
-    if ((d.b0_time == nullptr) != (d.b0_space == nullptr))
-        return fail(PFB_ERR_INVALID, "b0_time and b0_space must be given together");
-    if (!d.b0_time && d.nseg != 1) return fail(PFB_ERR_INVALID, "nseg > 1 needs B0 coefficients");
-    if (d.norm != PFB_NORM_NONE && d.norm != PFB_NORM_ORTHO) return fail(PFB_ERR_INVALID, "unknown norm");
-    if (d.batch == 0) return PFB_OK;
+    int st = to_desc(p, o, d);
+    if (st) return st;
+    if (d.batch > 0 && (!kspace || !image)) return fail(PFB_ERR_INVALID, "NULL argument");
 
     int prev = -1;
     if (cudaGetDevice(&prev) != cudaSuccess) return fail(PFB_ERR_CUDA, "cudaGetDevice failed");
@@ -94,6 +79,10 @@ extern "C" int pfb_nufft_adj_noalloc(pfb_plan *p, const pfb_apply_t *o, const vo
             if (dev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != dev) cudaSetDevice(dev);
         }
     } restore{prev};
+
+    void *base = nullptr;
+    if ((st = scratch_address(&base))) return st;
+    if (d.batch == 0) return PFB_OK;  // set-up call: the array is now resident on this device
 
     const int64_t nplanes = (int64_t)d.nseg * d.batch * d.ncoeff;
     cufftHandle h;
@@ -112,9 +101,6 @@ extern "C" int pfb_nufft_adj_noalloc(pfb_plan *p, const pfb_apply_t *o, const vo
     if (need > (size_t)PFB_NOALLOC_SCRATCH_BYTES)
         return fail(PFB_ERR_INVALID, "request needs " + std::to_string(need) + " bytes of scratch; the static "
                                      "array holds " + std::to_string((size_t)PFB_NOALLOC_SCRATCH_BYTES));
-    void *base = nullptr;
-    int st = scratch_address(p->device, &base);
-    if (st) return st;
     float2 *grid = static_cast<float2 *>(base);
     void *work = static_cast<unsigned char *>(base) + gbytes;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -123,10 +109,8 @@ extern "C" int pfb_nufft_adj_noalloc(pfb_plan *p, const pfb_apply_t *o, const vo
     fac /= (d.norm == PFB_NORM_ORTHO) ? std::sqrt((double)p->g.gvol) : (double)p->g.gvol;
     // launch_spread clears the grid part of the scratch before adding into it
     if ((st = launch_spread(p, d, static_cast<const float2 *>(kspace), grid, true, s))) return st;
-    PFB_CUFFT_TRY(cufftSetStream(h, s));
-    PFB_CUFFT_TRY(cufftSetWorkArea(h, work));
-    PFB_CUFFT_TRY(cufftExecC2C(h, reinterpret_cast<cufftComplex *>(grid), reinterpret_cast<cufftComplex *>(grid),
-                               CUFFT_INVERSE));
+    // run_fft holds the plan's fft_mu across cufftSetStream / SetWorkArea / Exec
+    if ((st = run_fft(p->fft_mu, h, wbytes, grid, +1, work, up256(wbytes), s))) return st;
     return launch_crop_deapod(p, d, grid, static_cast<float2 *>(image), (float)fac, s,
                               (o->flags & PFB_FLAG_ACCUMULATE) != 0);
 }

@@ -1,9 +1,9 @@
 """Generate golden vectors from the reference's own Numba CPU kernels.
 
-Run in a container where the pyfourier reference source tree is available
-(default location /root/reference, override with PYFOURIER_REF_SRC):
+Run where the pyfourier reference source tree is available, naming its
+``src`` directory (the one holding the ``pyfourier`` package):
 
-    python tests/golden/make_golden.py
+    PYFOURIER_REF_SRC=<reference checkout>/src python tests/golden/make_golden.py
 
 The reference package cannot be imported as shipped on a GPU-less host
 (``detect_gpu_backend`` leaves ``gpu_backend`` unbound, and
@@ -33,7 +33,7 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = os.environ.get("PYFOURIER_REF_SRC", "/root/reference/src")
+REF_SRC = os.environ.get("PYFOURIER_REF_SRC", "")
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/pyfourier_golden_numba_cache")
 
 
@@ -45,6 +45,8 @@ def _stub_package(name, path=None):
 
 
 def load_reference_kernels():
+    if not REF_SRC or not os.path.isdir(os.path.join(REF_SRC, "pyfourier")):
+        raise SystemExit("set PYFOURIER_REF_SRC to the reference's src directory (holding the pyfourier package)")
     root = os.path.join(REF_SRC, "pyfourier")
     _stub_package("pyfourier", root)
     sub = _stub_package("pyfourier._subroutines", os.path.join(root, "_subroutines"))

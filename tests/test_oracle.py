@@ -336,3 +336,17 @@ def test_masking_kernels_match_reference(golden, d):
     assert orc.rel_l2(orc.dense_to_sparse(golden[p + "dense_sub"], idx, basis), golden[p + "sparse_sub"]) < 1e-6
     fill_s = orc.sparse_to_dense(golden[p + "ksp"], idx, shape, np.ascontiguousarray(basis.conj().T))
     assert orc.rel_l2(fill_s, golden[p + "fill_sub"]) < 1e-6
+
+
+def test_threaded_glue_is_identical_to_per_item_glue():
+    """The oracle's apodize / resize / centred FFT split large batches over host
+    threads; every item sees the same operations, so the result is bit-identical."""
+    rng = np.random.default_rng(30)
+    x = (rng.standard_normal((5, 96, 96, 96)) + 1j * rng.standard_normal((5, 96, 96, 96))).astype(np.complex64)
+    args = (3, (1.25,) * 3, (4,) * 3, (6.9966590477,) * 3)
+    a = orc.apodize(x, *args)
+    assert all(np.array_equal(a[i], orc.apodize(x[i:i + 1], *args)[0]) for i in range(5))
+    r = orc.resize(x, (120, 120, 120))
+    assert all(np.array_equal(r[i], orc.resize(x[i:i + 1], (120, 120, 120))[0]) for i in range(5))
+    f = orc.fft_c(x, 3)
+    assert all(np.array_equal(f[i], orc.fft_c(x[i:i + 1], 3)[0]) for i in range(5))
