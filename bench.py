@@ -517,8 +517,10 @@ def parity_cfg2(torch, wl, r, cpu_coils, nudft_samples=10240):
       seeded subset of samples: the accuracy of the Kaiser-Bessel kernel at
       these parameters, which the reference's kernel shares."""
     c = cpu_coils
+    B = r["y"].shape[0]
+    y_dev = r["y"].reshape(B, -1)
     x_host = r["x"][:c].cpu().numpy()
-    y_host = r["y"][:c].cpu().numpy()
+    y_host = y_dev[:c].cpu().numpy()
     res = cpu_baseline(wl, r["coord"], x_host, y_host, steps=1)
     e_fwd = float(np.linalg.norm(y_host.astype(np.complex128) - res["y"]) / np.linalg.norm(res["y"]))
     xg = r["xa"][:c].cpu().numpy().reshape(res["x"].shape)
@@ -527,7 +529,7 @@ def parity_cfg2(torch, wl, r, cpu_coils, nudft_samples=10240):
     coord = r["coord"].reshape(-1, 3)
     sel = np.sort(rng.choice(coord.shape[0], nudft_samples, replace=False))
     ref = nudft_fwd_fp64(torch, r["x"][0], coord[sel])
-    e_nudft = rel_l2_t(torch, r["y"][0, torch.as_tensor(sel, device=r["y"].device)], ref)
+    e_nudft = rel_l2_t(torch, y_dev[0, torch.as_tensor(sel, device=y_dev.device)], ref)
     parity = {"rel_l2_fwd": e_fwd, "rel_l2_adj": e_adj, "vs": "oracle (C restatement of the reference's "
               f"kernels), {c} of {wl['coils']} coils, full trajectory", "tolerance": 1e-5,
               "pass": bool(e_fwd <= 1e-5 and e_adj <= 1e-5),

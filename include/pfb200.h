@@ -129,6 +129,20 @@ int pfb_plan_set_chunk(pfb_plan *plan, int chunk);
  * Debug / parity aid; not used by the operators. */
 int pfb_plan_tables(const pfb_plan *plan, int axis, int32_t *index, float *value, void *stream);
 
+/* Status of the plan's kernels since the last call: 0, or 1 when a kernel gave up
+ * a bounded wait on its own shared-memory barriers (every such wait gives up
+ * after about two seconds instead of hanging; the kernel then leaves its tile
+ * unwritten).  Synchronises the device, reads and clears the word.  No
+ * counterpart in the reference (its kernels have no waits). */
+int pfb_plan_status(pfb_plan *plan, int32_t *status);
+
+/* The plan's sample order after the stable counting sort by bin key: order[j] =
+ * the sample (caller's index) at sorted position j, int32 (total samples) on the
+ * device.  Equal keys keep the caller's order.  Debug / parity aid; the
+ * reference has no sorted order (its kernels walk the samples as given,
+ * src/pyfourier/_subroutines/_grid/_noncart2cart/_3D.py:29-50). */
+int pfb_plan_order(const pfb_plan *plan, int32_t *order, void *stream);
+
 /* Workspace bytes for an apply over `nplanes` oversampled grid planes
  * (nplanes = nseg * batch * ncoeff).  May create the cuFFT plan. */
 int pfb_workspace_size(pfb_plan *plan, int64_t nplanes, size_t *bytes);
@@ -283,6 +297,17 @@ int pfb_pipe_menon_dcf(pfb_plan *plan, float *weights, int niter, void *workspac
  *   kernel  device complex64, uncentred (ifftshift-ed) layout, copied.
  * Replaces GramMatrix (src/pyfourier/_sparsegram/_plan.py:253-270,
  * src/pyfourier/_gram/_plan.py:160-177). */
+/* Plan-time float64 spread for the Toeplitz PSF: grid[ch, frame(m), idx] +=
+ * KB64 taps of sample m * values[ch, m], for every sample m of the plan (in the
+ * plan's sample order) and ch < nch.  values (nch, total samples) and grid
+ * (nch, nframes, *os_shape) are device complex128; the grid is in the
+ * reference's table layout (index (x0 + i) mod n_os, no FFT shift), not divided
+ * by the kernel scale, and accumulated (the caller zeroes it).  Kernel weights,
+ * products and sums are float64.  Replaces the complex64 spread inside the PSF
+ * construction (src/pyfourier/_sparsegram/_plan.py:201-208, the adjoint NUFFT
+ * of the sample weights). */
+int pfb_spread_f64(pfb_plan *plan, const void *values, int nch, void *grid, void *stream);
+
 int pfb_gram_create(int ndim, const int *shape, const int *os_shape, int ncoeff, int lowrank,
                     int nseg, const void *kernel, int device, void *stream, pfb_gram **out);
 int pfb_gram_destroy(pfb_gram *gram);

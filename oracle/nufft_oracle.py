@@ -73,6 +73,8 @@ def lib():
         L.orc_degrid_subspace.argtypes = [vp, vp] + tab + [vp, i64, i64, i64, i64] + [ci] * 6
         for f in (L.orc_grid, L.orc_degrid, L.orc_grid_subspace, L.orc_degrid_subspace):
             f.restype = None
+        L.orc_grid_f64.restype = None
+        L.orc_grid_f64.argtypes = [vp, vp, vp, ci, i64, i64, i64, vp, vp, vp, vp]
         L.orc_num_threads.restype = ci
         _LIB = L
     return _LIB
@@ -565,12 +567,70 @@ class OracleGram:
     zmap_s_kernel: object = None  # (L, *shape) spatial B0 coefficients C_l
 
 
+def apod_vector64(n, oversamp, width, beta):
+    """apod_vector in float64 throughout (the plan-time float64 PSF)."""
+    os_i = float(np.ceil(np.float32(oversamp) * np.float32(n)))
+    idx = np.arange(n, dtype=np.float64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        a = np.sqrt(float(beta) ** 2 - (math.pi * int(width) * (idx - n // 2) / os_i) ** 2)
+        a = a / np.sinh(a)
+        a = a / a[n // 2]
+    return np.nan_to_num(a, nan=1.0)
+
+
+def spread_f64(values, plan):
+    """Float64 spread on a plan's grid: values (F, B, M) -> (F, B, *os) complex128,
+    taps in float64 (orc_grid_f64), not divided by the kernel scale."""
+    F, M, nd = plan.c_os.shape
+    B = values.shape[1]
+    v = np.ascontiguousarray(values, np.complex128).reshape(F, B, M)
+    out = np.zeros((F, B, *plan.os_shape), np.complex128)
+    cxyz = np.ascontiguousarray(plan.c_os, np.float32)
+    w = (ctypes.c_int * nd)(*[int(x) for x in plan.width[::-1]])
+    bt = (ctypes.c_double * nd)(*[float(x) for x in plan.beta[::-1]])
+    no = (ctypes.c_int * nd)(*[int(x) for x in plan.os_shape[::-1]])
+    ca = (ctypes.c_int * nd)(*[int(bool(x)) for x in (plan.is_cart or (False,) * nd)[::-1]])
+    lib().orc_grid_f64(_p(out), _p(v), _p(cxyz), nd, F, B, M, w, bt, no, ca)
+    return out
+
+
+def psf_f64(values, pplan, os_shape, basis=None):
+    """The Toeplitz PSF in float64 (plan time): the adjoint NUFFT of the per-sample
+    values on the PSF plan ``pplan`` (2x coordinates), cropped to ``os_shape``.
+
+    values (L, F, M): per B0 segment l the sample weights (times B_l(t)).  With a
+    basis (F, K) the subspace projection of the reference's PSF
+    (delta[k1, f] = basis[f, k1], spread with conj(basis[f, k2]),
+    _sparsegram/_plan.py:201-208 with _noncart2cart/_2D_subspace.py:49-53) is
+    taken after the per-frame spread, by linearity: P[l, k1, k2] = sum_f
+    basis[f, k1] conj(basis[f, k2]) G[l, f].  The rest of the adjoint (division
+    by the kernel scale, centred inverse FFT with norm None, crop, float64
+    deapodisation) follows _nufft/_nufft.py:254-287.  Returns (L, K, K, *os) or
+    (L, F, *os) complex128."""
+    nd = pplan.ndim
+    Ls, F = values.shape[:2]
+    G = spread_f64(np.moveaxis(values, 0, 1), pplan) / pplan.scale  # (F, L, *os_psf)
+    G = np.moveaxis(G, 1, 0)  # (L, F, ...)
+    if basis is not None:
+        b = np.asarray(basis, np.complex128)
+        G = np.einsum("fa,fb,lf...->lab...", b, b.conj(), G)
+    x = ifft_c(G, nd, None)
+    x = resize(x, os_shape)
+    for n in range(1, nd + 1):
+        ax = -n
+        if int(pplan.width[ax]) != 1:
+            a = apod_vector64(x.shape[ax], pplan.oversamp[ax], pplan.width[ax], pplan.beta[ax])
+            x = x * a.reshape([x.shape[ax]] + [1] * (n - 1))
+    return x
+
+
 def plan_spgram(coord, shape, basis=None, weight=None, width=6, normalize="reference", zmap=None, L=6,
                 nbins=(40, 40), dt=None, T=None):
     """_sparsegram/_plan.py:20-249 with its intent fixes.
 
     PSF = adjoint NUFFT of ``weight * delta`` at 2x coordinates onto the 2N
-    grid (:201-208, with the keyword intent restored), then a centred
+    grid (:201-208, with the keyword intent restored), computed in float64
+    (``psf_f64``; the reference uses its complex64 NUFFT), then a centred
     orthonormal FFT and ifftshift (:211, :226).  With a basis the per-voxel
     matrix is value[v][k2][k1] = T[k1, k2](v) (so out = value[v] @ in, the
     evident intent of _bmatvec/_bdot.py).  ``normalize="reference"`` divides by
@@ -592,29 +652,28 @@ def plan_spgram(coord, shape, basis=None, weight=None, width=6, normalize="refer
     wgt = np.ones(coord.shape[:-1], np.float32) if weight is None else np.asarray(weight, np.float32)
     if basis is not None:
         basis = np.asarray(basis, np.complex64)
-        F, K = basis.shape
-        delta = np.broadcast_to(basis.T.reshape(K, F, *([1] * (coord.ndim - 2))),
-                                (K, *coord.shape[:-1])).astype(np.complex64)
-    else:
-        delta = np.ones(coord.shape[:-1], np.complex64)
     Cl = None
+    vals = wgt.astype(np.complex128)[None]  # (L = 1, F, ...)
     if zmap is not None:
         if T is None:
             T = dt * np.arange(coord.shape[-2], dtype=np.float32)
         Bt, Cl = mri_exp_approx(zmap, T, L, nbins, acorr=True)
         # segment l weights each sample by B_l(t) of its readout position (last axis)
-        Bl = Bt.astype(np.complex64).reshape(L, *([1] * (delta.ndim - 1)), Bt.shape[-1])
-        delta = delta[None] * Bl
+        vals = vals * Bt.astype(np.complex128).reshape(L, *([1] * (vals.ndim - 2)), Bt.shape[-1])
         Cl = Cl.astype(np.complex64)
     pplan = plan_nufft(coord * osf[::-1], os_shape, width=width, oversamp=1.25)
-    psf = nufft_adj((wgt * delta).astype(np.complex64), pplan, basis)
+    # the PSF in float64 at plan time (the reference builds it with its complex64
+    # adjoint NUFFT, _sparsegram/_plan.py:201-208); applies stay complex64
+    Fp = pplan.nframes
+    psf = psf_f64(vals.reshape(vals.shape[0], Fp, -1), pplan, os_shape, basis)
     G_os = float(np.prod(pplan.os_shape))
     if normalize is None:
-        psf = psf * np.float32(G_os)
-        T = fft_c(psf, ndim, norm=None)
+        T = fft_c(psf * G_os, ndim, norm=None)
     else:
         T = fft_c(psf, ndim, norm="ortho")
     nlead = 1 if zmap is not None else 0
+    if not nlead:
+        T = T[0]
     if basis is None and T.ndim > ndim + nlead and T.shape[nlead] == 1:
         T = T[:, 0] if nlead else T[0]
     T = np.fft.ifftshift(T, axes=tuple(range(-ndim, 0)))

@@ -239,3 +239,68 @@ int orc_num_threads(void)
     return 1;
 #endif
 }
+
+/* Float64 spread for the Toeplitz PSF (plan time).  Same tap arithmetic as
+ * orc_prepare_interpolator (x0 = ceil(c - W/2), index (x0 + i) mod n_os,
+ * weight KB(((x0 + i) - c) / (W/2))) with the weights kept in float64 instead of
+ * being rounded to float32 tables; Cartesian axes (cart_xyz[a] != 0) take the
+ * rounded position with weight 1.  coord (F, M, ndim) float32 in (x, y, z)
+ * order; noncart (F, B, M) complex128; cart (F, B, *os) complex128 accumulated.
+ * Parallel over (frame, batch) like orc_grid. */
+void orc_grid_f64(double complex *cart, const double complex *noncart, const float *coord, int ndim,
+                  int64_t nframes, int64_t batch, int64_t npts, const int *width_xyz, const double *beta_xyz,
+                  const int *nos_xyz, const int *cart_xyz)
+{
+    int w[3] = {1, 1, 1}, nos[3] = {1, 1, 1}, ca[3] = {1, 1, 1};
+    double beta[3] = {0, 0, 0};
+    for (int a = 0; a < ndim; ++a) {
+        w[a] = cart_xyz[a] ? 1 : width_xyz[a];
+        nos[a] = nos_xyz[a];
+        beta[a] = beta_xyz[a];
+        ca[a] = cart_xyz[a];
+    }
+    const int64_t plane = (int64_t)nos[0] * nos[1] * nos[2];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t i = 0; i < nframes * batch; ++i) {
+        int64_t frame = i / batch, b = i % batch;
+        double complex *out = cart + (frame * batch + b) * plane;
+        const double complex *in = noncart + (frame * batch + b) * npts;
+        for (int64_t p = 0; p < npts; ++p) {
+            const float *c = coord + (frame * npts + p) * ndim;
+            double wv[3][16];
+            int64_t ix[3][16];
+            for (int a = 0; a < 3; ++a) {
+                if (a >= ndim) {
+                    wv[a][0] = 1.0;
+                    ix[a][0] = 0;
+                    continue;
+                }
+                double cc = (double)c[a];
+                if (ca[a]) {
+                    double m = fmod(rint(cc), (double)nos[a]);
+                    if (m < 0)
+                        m += nos[a];
+                    wv[a][0] = 1.0;
+                    ix[a][0] = (int64_t)m;
+                    continue;
+                }
+                double x0 = ceil(cc - w[a] / 2.0);
+                for (int t = 0; t < w[a]; ++t) {
+                    wv[a][t] = orc_kaiser_bessel(((x0 + t) - cc) / (w[a] / 2.0), beta[a]);
+                    double m = fmod(x0 + t, (double)nos[a]);
+                    if (m < 0)
+                        m += nos[a];
+                    ix[a][t] = (int64_t)m;
+                }
+            }
+            const double complex v = in[p];
+            for (int tz = 0; tz < w[2]; ++tz)
+                for (int ty = 0; ty < w[1]; ++ty) {
+                    const double wzy = wv[2][tz] * wv[1][ty];
+                    const int64_t row = (ix[2][tz] * nos[1] + ix[1][ty]) * nos[0];
+                    for (int tx = 0; tx < w[0]; ++tx)
+                        out[row + ix[0][tx]] += (wzy * wv[0][tx]) * v;
+                }
+        }
+    }
+}

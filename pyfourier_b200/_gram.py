@@ -2,9 +2,11 @@
 
 Mirrors src/pyfourier/_sparsegram/_plan.py:20-270 and
 src/pyfourier/_sparsegram/_fwd.py:17-119.  The point-spread function is built
-at plan time with this package's own adjoint NUFFT at twice the coordinates on
-the 2N grid (as the reference does, _plan.py:201-208), Fourier transformed and
-stored as per-voxel K x K matrices (subspace) or per-frame planes.  The apply
+at plan time in float64 -- the adjoint NUFFT of the sample weights at twice the
+coordinates on the 2N grid (the reference's construction, _plan.py:201-208,
+which runs its complex64 NUFFT) with a float64 spread kernel (pfb_spread_f64)
+and complex128 transforms -- then Fourier transformed and stored as complex64
+per-voxel K x K matrices (subspace) or per-frame planes.  The apply
 (pad -> FFT -> mix -> inverse FFT -> crop) runs in libpfb200.
 
 Intent fixes relative to the shipped reference (whose plan cannot run,
@@ -21,6 +23,7 @@ _plan.py:141-147, :201-208, :229-239):
 from __future__ import annotations
 
 import ctypes
+import math
 from dataclasses import dataclass
 
 import numpy as np
@@ -28,7 +31,6 @@ import torch
 
 from . import _lib
 from ._b0 import mri_exp_approx
-from ._nufft import nufft_adj
 from ._plan import _as_tensor, plan_nufft, resolve_device, to_caller
 
 
@@ -102,6 +104,63 @@ class GramMatrix:
         return self._handle
 
 
+def _apod64(n, oversamp, width, beta, dev):
+    """Deapodisation vector of one axis in float64 (_subroutines/_apod.py:27-41)."""
+    os_i = float(np.ceil(np.float32(oversamp) * np.float32(n)))
+    i = torch.arange(n, dtype=torch.float64, device=dev)
+    a = torch.sqrt(float(beta) ** 2 - (math.pi * int(width) * (i - n // 2) / os_i) ** 2)  # NaN where < 0
+    a = a / torch.sinh(a)
+    a = a / a[n // 2]
+    return torch.nan_to_num(a, nan=1.0)
+
+
+def _centred(x, nd, inverse, norm):
+    axes = tuple(range(-nd, 0))
+    f = torch.fft.ifftn if inverse else torch.fft.fftn
+    return torch.fft.fftshift(f(torch.fft.ifftshift(x, dim=axes), dim=axes, norm=norm), dim=axes)
+
+
+def _psf_f64(vals, pplan, os_shape, basis):
+    """The Toeplitz PSF in float64: adjoint NUFFT of the per-sample values on the
+    PSF plan, cropped to ``os_shape`` (the 2N grid).
+
+    vals (L, total samples) complex128 in the plan's sample order.  The spread
+    runs in libpfb200 in float64 (pfb_spread_f64) into per-frame grids; with a
+    basis (F, K) the subspace projection of the reference (delta[k1, f] =
+    basis[f, k1] spread with conj(basis[f, k2]), _noncart2cart/_2D_subspace.py:49-53)
+    follows by linearity: P[l, k1, k2] = sum_f basis[f, k1] conj(basis[f, k2]) G[l, f].
+    Division by the kernel scale, the centred inverse FFT (norm None), the crop
+    and the deapodisation follow _nufft/_nufft.py:254-287, in complex128.
+    Returns (L, K, K, *os_shape) or (L, F, *os_shape)."""
+    dev = pplan.device
+    nd = pplan.ndim
+    it = pplan.interpolator
+    Ls = vals.shape[0]
+    grid = torch.zeros((Ls, it.nframes, *pplan.os_shape), dtype=torch.complex128, device=dev)
+    v = vals.to(dev, torch.complex128).contiguous()
+    with torch.cuda.device(dev):
+        st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(_lib.load().pfb_spread_f64(it.handle, ctypes.c_void_p(v.data_ptr()), int(Ls),
+                                              ctypes.c_void_p(grid.data_ptr()), st))
+    grid = grid / it.scale
+    if basis is not None:
+        b = basis.to(dev, torch.complex128)
+        grid = torch.einsum("fa,fb,lf...->lab...", b, b.conj(), grid)
+    x = _centred(grid, nd, True, "backward")
+    # centred crop to os_shape (_subroutines/_resize.py:23-42)
+    sl = [slice(None)] * (x.ndim - nd)
+    for i, o in zip(x.shape[-nd:], os_shape):
+        s0 = max(i // 2 - o // 2, 0)
+        sl.append(slice(s0, s0 + min(i, o)))
+    x = x[tuple(sl)]
+    for n in range(1, nd + 1):
+        ax = -n
+        if int(pplan.width[ax]) != 1:
+            a = _apod64(x.shape[ax], pplan.oversamp[ax], pplan.width[ax], pplan.beta[ax], dev)
+            x = x * a.reshape([x.shape[ax]] + [1] * (n - 1))
+    return x
+
+
 def plan_spgram(coord, shape, basis=None, zmap=None, L=6, nbins=(40, 40), dt=None, T=None,
                 L_batch_size=None, weight=None, oversamp=None, width=6, device="cpu",
                 normalize="reference"):
@@ -128,13 +187,8 @@ def plan_spgram(coord, shape, basis=None, zmap=None, L=6, nbins=(40, 40), dt=Non
         wgt = torch.ones(coord_t.shape[:-1], dtype=torch.float32, device=dev)
     else:
         wgt = _as_tensor(weight).to(dev, torch.float32)
-    if basis is not None:
-        basis_t = _as_tensor(basis).to(dev, torch.complex64)
-        F, K = basis_t.shape
-        delta = basis_t.T.reshape(K, F, *([1] * (coord_t.ndim - 2))).expand(K, *coord_t.shape[:-1])
-    else:
-        basis_t = None
-        delta = torch.ones(coord_t.shape[:-1], dtype=torch.complex64, device=dev)
+    basis_t = _as_tensor(basis).to(dev, torch.complex64) if basis is not None else None
+    vals = wgt.to(torch.complex128)[None]  # (L = 1, ...)
     zs = None
     if zmap is not None:
         if T is None:
@@ -143,21 +197,21 @@ def plan_spgram(coord, shape, basis=None, zmap=None, L=6, nbins=(40, 40), dt=Non
             T = dt * np.arange(coord_t.shape[-2], dtype=np.float32)
         bt, zs = mri_exp_approx(_as_tensor(zmap).to(dev), T, L, nbins, acorr=True)
         # segment l weights each sample by B_l(t) of its readout position (last axis)
-        bl = torch.as_tensor(bt, dtype=torch.complex64, device=dev)
-        bl = bl.reshape(L, *([1] * (delta.ndim - 1)), bl.shape[-1])
-        delta = delta[None] * bl
+        bl = torch.as_tensor(bt, dtype=torch.complex128, device=dev)
+        vals = vals * bl.reshape(L, *([1] * (vals.ndim - 2)), bl.shape[-1])
         zs = zs.to(torch.complex64).contiguous()
     scale_xyz = torch.as_tensor(osf[::-1].copy(), device=dev)
     pplan = plan_nufft(coord_t * scale_xyz, os_shape, width=width, oversamp=1.25, device=dev)
-    psf = nufft_adj((wgt * delta).to(torch.complex64), nufft_plan=pplan, basis=basis_t, device=dev)
-    axes = tuple(range(-ndim, 0))
+    psf = _psf_f64(vals.reshape(vals.shape[0], -1), pplan, os_shape, basis_t)
     if normalize is None:
         G_os = float(np.prod(pplan.os_shape))
-        Tk = torch.fft.fftshift(torch.fft.fftn(torch.fft.ifftshift(psf * G_os, dim=axes), dim=axes), dim=axes)
+        Tk = _centred(psf * G_os, ndim, False, "backward")
     else:
-        Tk = torch.fft.fftshift(torch.fft.fftn(torch.fft.ifftshift(psf, dim=axes), dim=axes, norm="ortho"),
-                                dim=axes)
+        Tk = _centred(psf, ndim, False, "ortho")
+    axes = tuple(range(-ndim, 0))
     nlead = 1 if zs is not None else 0
+    if not nlead:
+        Tk = Tk[0]
     if basis_t is None and Tk.ndim > ndim + nlead and Tk.shape[nlead] == 1:
         Tk = Tk[:, 0] if nlead else Tk[0]
     Tk = torch.fft.ifftshift(Tk, dim=axes)

@@ -33,7 +33,8 @@ EXPORTS = (
     "pfb_crop_deapod", "pfb_grid_fft", "pfb_traj_grad", "pfb_gram_create", "pfb_gram_destroy",
     "pfb_gram_workspace_size", "pfb_gram_apply", "pfb_nufft_adj_noalloc",
     "pfb_grog_create", "pfb_grog_destroy", "pfb_grog_workspace_size", "pfb_grog_apply",
-    "pfb_apply_workspace_size", "pfb_nufft_traj_grad", "pfb_nufft_stage",
+    "pfb_apply_workspace_size", "pfb_nufft_traj_grad", "pfb_nufft_stage", "pfb_plan_order", "pfb_spread_f64",
+    "pfb_plan_status",
 )
 
 
@@ -102,6 +103,8 @@ def load(path=LIB_PATH):
         "pfb_plan_set_tuning": (i32, [vp, i32, i32, i32]),
         "pfb_plan_set_chunk": (i32, [vp, i32]),
         "pfb_plan_tables": (i32, [vp, i32, vp, vp, vp]),
+        "pfb_plan_order": (i32, [vp, vp, vp]),
+        "pfb_plan_status": (i32, [vp, P(ctypes.c_int32)]),
         "pfb_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),
         "pfb_nufft_fwd": (i32, [vp, P(ApplyT), vp, vp, vp, ctypes.c_size_t, vp]),
         "pfb_nufft_adj": (i32, [vp, P(ApplyT), vp, vp, vp, ctypes.c_size_t, vp]),
@@ -111,6 +114,7 @@ def load(path=LIB_PATH):
         "pfb_crop_deapod": (i32, [vp, P(ApplyT), vp, vp, f32, vp]),
         "pfb_grid_fft": (i32, [vp, vp, i64, i32, vp, ctypes.c_size_t, vp]),
         "pfb_traj_grad": (i32, [vp, P(ApplyT), vp, vp, vp, i32, vp]),
+        "pfb_spread_f64": (i32, [vp, vp, i32, vp, vp]),
         "pfb_gram_create": (i32, [i32, P(ctypes.c_int), P(ctypes.c_int), i32, i32, i32, vp, i32, vp, P(vp)]),
         "pfb_gram_destroy": (i32, [vp]),
         "pfb_gram_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),

@@ -136,8 +136,9 @@ struct pfb_plan {
     float *d_cos[pfb::kMaxDim] = {nullptr, nullptr, nullptr};  // bin-sorted oversampled coords
     int *d_perm = nullptr;       // sorted position -> global sample index
     int *d_iperm = nullptr;      // global sample index -> sorted position
-    float *d_wtap = nullptr;     // per sorted sample: D x WM kernel weights (WM = 4 for W <= 4, else 8)
-    int *d_xtap = nullptr;       // per sorted sample: D first taps x0 mod n_os
+    float *d_wtap = nullptr;     // per sorted sample a record: D x WM kernel weights (WM = 4 for W <= 4,
+                                 // else 8), the D first taps x0 mod n_os, padded to 16 bytes
+    int *d_xtap = nullptr;       // d_wtap + D * WM (first taps inside the records, not a separate buffer)
     int *d_sframe = nullptr;     // sorted position -> frame
     int *d_bin_start = nullptr;  // (nbins_total * ncode * F + 1) offsets into the sorted order
     int nbins_total = 0;
@@ -166,6 +167,8 @@ struct pfb_plan {
     int fft_fused = -1;          // -1 not decided, 0 not applicable, 1 ready
     pfb::FftAxis fft_ax[pfb::kMaxDim];
     float2 *d_fft_tw = nullptr;  // twiddles of all axes and stages
+    // device status word: kernels whose bounded waits gave up set it (0 = ok)
+    int *d_status = nullptr;
 };
 
 namespace pfb {
@@ -369,6 +372,12 @@ int build_owner_items(pfb_plan *p, int chunk);
 // per-sample kernel weights and first taps of the sorted samples (plan time)
 int build_plan_taps(pfb_plan *p, cudaStream_t s);
 void free_owner_items(pfb_plan *p);
+
+// sort.cu: stable LSD counting sort of (int key, int value) pairs over the low
+// end_bit bits of the keys, keys in [0, 2^31); temp of counting_sort_temp_bytes(n)
+size_t counting_sort_temp_bytes(int64_t n);
+int counting_sort_pairs(const int *keys, const int *vals, int *keys_out, int *vals_out, int64_t n, int end_bit,
+                        void *temp, size_t temp_bytes, cudaStream_t s);
 
 // fused pruned FFT (pfb_fft.cu): 1 when it applies to the plan (tables ready)
 int fft_fused_ready(pfb_plan *p);

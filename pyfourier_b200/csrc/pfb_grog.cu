@@ -17,7 +17,6 @@
 //   3. transposes back to (b, c, m), writing zeros for samples outside the grid.
 // An operator is read from memory once per run of chunks that share it instead
 // of once per sample.
-#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <vector>
@@ -365,10 +364,12 @@ int pfb_grog_create(const int *lut, int64_t nsamples, int ntable, int ncoils, in
         GROG_TRY(cudaGetLastError());
         int end_bit = 1;
         while ((1LL << end_bit) <= (long long)ntable) ++end_bit;
-        size_t tb = 0;
-        GROG_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys_s, idx, perm, (int)M, 0, end_bit, s));
-        GROG_TRY(cudaMalloc(&temp, std::max<size_t>(tb, 1)));
-        GROG_TRY(cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys_s, idx, perm, (int)M, 0, end_bit, s));
+        const size_t tb = counting_sort_temp_bytes(M);
+        GROG_TRY(cudaMalloc(&temp, tb));
+        {
+            const int sst = counting_sort_pairs(keys, idx, keys_s, perm, M, end_bit, temp, tb, s);
+            if (sst) return cleanup(sst);
+        }
         grog_bounds_kernel<<<(unsigned)std::min<int64_t>((M + 256) / 256, 148LL * 32), 256, 0, s>>>(
             keys_s, M, ntable + 1, off);
         GROG_TRY(cudaGetLastError());

@@ -1,5 +1,5 @@
-// Plan construction: coordinate scaling, tile binning and the stable sort of
-// samples by (tile, frame).  Plan-time only; allocations and host syncs here
+// Plan construction: coordinate scaling, tile binning and the stable integer
+// counting sort of samples by (tile, edge code, frame) (pfb_sort.cu).  Plan-time only; allocations and host syncs here
 // are intended.
 //
 // Reference behaviour restated (paths inside the pyfourier project):
@@ -8,8 +8,6 @@
 //   tap index            src/pyfourier/_subroutines/_grid/_plan.py:210 ((x0+i) mod n_os)
 //   kernel scaling       src/pyfourier/_subroutines/_grid/_plan.py:118-141
 //   deapodisation        src/pyfourier/_subroutines/_apod.py:24-44 (here in float64)
-#include <cub/device/device_radix_sort.cuh>
-
 #include <algorithm>
 #include <cmath>
 
@@ -174,6 +172,8 @@ void free_plan_buffers(pfb_plan *p) {
     cudaFree(p->d_items_frame);
     cudaFree(p->d_items_all);
     cudaFree(p->d_frame_off);
+    cudaFree(p->d_status);
+    p->d_status = nullptr;
     p->d_perm = p->d_sframe = p->d_bin_start = nullptr;
     p->d_items_frame = p->d_items_all = nullptr;
     p->d_frame_off = nullptr;
@@ -331,6 +331,8 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
         return cleanup(fail(PFB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e))); } while (0)
 
     PFB_TRY_ST(dev_alloc(&p->d_frame_off, nframes + 1));
+    PFB_TRY_ST(dev_alloc(&p->d_status, 1));
+    PFB_TRY_CU(cudaMemsetAsync(p->d_status, 0, sizeof(int), stream));
     PFB_TRY_CU(cudaMemcpyAsync(p->d_frame_off, frame_offsets, (nframes + 1) * sizeof(int64_t),
                                cudaMemcpyHostToDevice, stream));
     for (int a = 0; a < ndim; ++a) PFB_TRY_ST(dev_alloc(&p->d_cos[a], mtot));
@@ -365,11 +367,10 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
         PFB_TRY_CU(cudaGetLastError());
         int end_bit = 1;
         while ((1LL << end_bit) < (long long)nkeys) ++end_bit;
-        PFB_TRY_CU(cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, d_keys, d_keys_sorted, d_vals,
-                                                   p->d_perm, (int)mtot, 0, end_bit, stream));
-        PFB_TRY_CU(cudaMalloc(&d_temp, std::max<size_t>(temp_bytes, 1)));
-        PFB_TRY_CU(cub::DeviceRadixSort::SortPairs(d_temp, temp_bytes, d_keys, d_keys_sorted, d_vals,
-                                                   p->d_perm, (int)mtot, 0, end_bit, stream));
+        temp_bytes = counting_sort_temp_bytes(mtot);
+        PFB_TRY_CU(cudaMalloc(&d_temp, temp_bytes));
+        PFB_TRY_ST(counting_sort_pairs(d_keys, d_vals, d_keys_sorted, p->d_perm, mtot, end_bit, d_temp, temp_bytes,
+                                       stream));
         gather_sorted_kernel<<<blocks, T, 0, stream>>>(ndim, mtot, nframes, d_cos_tmp, p->d_perm, d_keys_sorted,
                                                        p->d_cos[0], p->d_cos[1], p->d_cos[2], p->d_sframe,
                                                        p->d_iperm);

@@ -51,6 +51,24 @@ def test_gram_subspace_vs_oracle(normalize):
     assert rel(P.sparse_gram(torch.as_tensor(x).cuda(), gg), orc.sparse_gram(x, og)) < 1e-5
 
 
+@pytest.mark.parametrize("zmap", [False, True])
+def test_psf_float64_matches_oracle(zmap):
+    """The Toeplitz kernel is built in float64 at plan time on the GPU (float64
+    spread kernel, complex128 transforms) and by the oracle (float64 C spread,
+    NumPy complex128): both stored as complex64, they agree to 1e-6."""
+    P = pf()
+    rng = np.random.default_rng(20)
+    N, F, K = 24, 8, 4
+    coord = spiral_frames(F, 4, 128, N)
+    basis = np.linalg.qr(crandn(rng, F, K))[0].astype(np.complex64)
+    kw = dict(zmap=_b0_map(N), L=4, nbins=40, dt=5e-3 / 128) if zmap else {}
+    og = orc.plan_spgram(coord, (N, N), basis=basis, normalize=None, **kw)
+    gg = P.plan_spgram(torch.as_tensor(coord), (N, N), basis=torch.as_tensor(basis), device="cuda:0",
+                       normalize=None, **{k: (torch.as_tensor(v) if k == "zmap" else v) for k, v in kw.items()})
+    assert tuple(gg.value.shape) == tuple(og.value.shape)
+    assert rel(gg.value, og.value) < 1e-6
+
+
 def test_gram_exact_equals_ahwa_gpu():
     """normalize=None: sparse_gram(x) == A^H W A x (A = nufft norm None, A^H exact adjoint)."""
     P = pf()

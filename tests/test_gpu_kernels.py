@@ -239,3 +239,55 @@ def test_interleaved_pipeline_matches_planar(case):
         zt = crn(Lseg, 64)
         zs = crn(Lseg, 32 * 32)
         _pipeline_both(plan, crn(6, 1, *N), crn(6, 12 * 64), zs=zs, zt=zt, L=Lseg)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_counting_sort_is_stable_by_bin_key(ndim):
+    """The plan's samples are ordered by the integer bin key
+    ((tile << d | edge code) * F + frame) with the reference's grid-index
+    arithmetic, and equal keys keep the caller's order (a stable sort): the
+    exported order against keys recomputed here from the oracle's tables."""
+    import pyfourier_b200 as pf
+
+    rng = np.random.default_rng(70 + ndim)
+    N = (40,) * ndim
+    F = 3
+    lens = [2500, 700, 4100]
+    frames = [((rng.random((m, ndim)) - 0.5) * N[0]).astype(np.float32) for m in lens]
+    frames[1][:300] *= 0.02  # a crowded bin
+    plan = pf.plan_nufft([torch.as_tensor(c) for c in frames], N, width=4, oversamp=1.25, device="cuda:0")
+    M = plan.interpolator.total_samples
+    order = torch.empty(M, dtype=torch.int32, device="cuda:0")
+    _lib().check(_lib().load().pfb_plan_order(plan.interpolator.handle, ctypes.c_void_p(order.data_ptr()),
+                                              _stream()))
+    order = order.cpu().numpy()
+    assert np.array_equal(np.sort(order), np.arange(M))
+    # keys from the first taps of the oracle's tables (x-first axes)
+    coord = np.concatenate(frames)
+    op = orc.plan_nufft(coord[None], N, width=4, oversamp=1.25)
+    tile = plan.interpolator.tile[::-1]  # (x, y, z)
+    nos = op.os_shape[::-1]
+    frame = np.repeat(np.arange(F), lens)
+    key_bin = np.zeros(M, np.int64)
+    code = np.zeros(M, np.int64)
+    stride = 1
+    for a in range(ndim):
+        x0m = op.index[ndim - 1 - a][0, :, 0].astype(np.int64)
+        nb = -(-nos[a] // tile[a])
+        tb = x0m // tile[a]
+        key_bin += tb * stride
+        stride *= nb
+        text = np.minimum(tile[a], nos[a] - tb * tile[a])
+        if nb > 1:
+            code |= ((x0m - tb * tile[a] + 3 >= text).astype(np.int64) << a)
+    key = ((key_bin << ndim) | code) * F + frame
+    ks = key[order]
+    assert np.all(np.diff(ks) >= 0)
+    same = np.diff(ks) == 0
+    assert np.all(np.diff(order)[same] > 0)
+    # deterministic: a second plan gives the same order
+    plan2 = pf.plan_nufft([torch.as_tensor(c) for c in frames], N, width=4, oversamp=1.25, device="cuda:0")
+    order2 = torch.empty(M, dtype=torch.int32, device="cuda:0")
+    _lib().check(_lib().load().pfb_plan_order(plan2.interpolator.handle, ctypes.c_void_p(order2.data_ptr()),
+                                              _stream()))
+    assert np.array_equal(order2.cpu().numpy(), order)
