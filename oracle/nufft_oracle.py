@@ -594,6 +594,28 @@ def spread_f64(values, plan):
     return out
 
 
+def nufft_adj_f64(kspace, plan):
+    """The adjoint NUFFT of a single-frame plan (norm None) with the reference's
+    taps and kernel but float64 arithmetic throughout: float64 spread
+    (orc_grid_f64), complex128 centred inverse FFT, crop, float64 deapodisation.
+    kspace (B, M) -> (B, *shape) complex128.  A precision reference: the
+    reference's float32 serial sums (_noncart2cart/_3D.py:29-50) drift from it on
+    crowded trajectories (about 7e-4 rel-L2 at the 3D radial 200^3 / 8 M-sample
+    size), an algorithm in float64 does not."""
+    nd = plan.ndim
+    k = np.asarray(kspace, np.complex128)
+    B = k.shape[0]
+    G = spread_f64(k.reshape(1, B, -1), plan)[0] / plan.scale
+    x = ifft_c(G, nd, None)
+    x = resize(x, plan.shape)
+    for n in range(1, nd + 1):
+        ax = -n
+        if int(plan.width[ax]) != 1:
+            a = apod_vector64(x.shape[ax], plan.oversamp[ax], plan.width[ax], plan.beta[ax])
+            x = x * a.reshape([x.shape[ax]] + [1] * (n - 1))
+    return x
+
+
 def psf_f64(values, pplan, os_shape, basis=None):
     """The Toeplitz PSF in float64 (plan time): the adjoint NUFFT of the per-sample
     values on the PSF plan ``pplan`` (2x coordinates), cropped to ``os_shape``.

@@ -1235,11 +1235,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 // of the 8^3 tile x 32 channels in registers, no atomics -- but the samples
 // stream through a ring of kRingStages stages instead of a double buffer
 // between two CTA barriers per batch:
-//   * batches are contiguous runs of kRingBatch visits (pieces of the item's
-//     neighbour ranges), so one bulk copy per piece moves the plan records
-//     (weights + first taps) and, when the apply has exactly 32 channels, the
-//     channel values (otherwise one cp.async per sample), completing on the
-//     stage's transaction barrier;
+//   * a batch holds up to kRingBatch visits: from each of the item's neighbour
+//     ranges a proportional, contiguous piece, so that every batch mixes the
+//     ranges (whose samples hit different blocks) and one bulk copy per piece
+//     moves the plan records (weights + first taps) and, when the apply has
+//     exactly 32 channels, the channel values (otherwise one cp.async per
+//     sample), completing on the stage's transaction barrier;
 //   * batch pb is produced by warp pb % 16: after every warp has released the
 //     stage's previous batch it issues the copies, consumes its current batch
 //     while they land, then turns the records into tile-relative (w, w) weight
@@ -1280,7 +1281,9 @@ __global__ void __launch_bounds__(16 * 32, 1) spread_ring3_kernel(const SpreadIL
     __shared__ int s_beg[NR];
     __shared__ int s_dlt[NR];
     __shared__ __align__(8) unsigned long long bar_raw[NS], bar_full[NS], bar_empty[NS];
-    __shared__ int s_fail;
+    __shared__ int s_fail, s_nbat;
+    __shared__ int s_len[NR], s_vst[NR];  // the item's part of range r: length and first visit
+    __shared__ int s_nb[NS];               // samples of the batch a stage holds
     const OwnerItem it = P.items[blockIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nch = P.ch.nch;
@@ -1304,7 +1307,41 @@ __global__ void __launch_bounds__(16 * 32, 1) spread_ring3_kernel(const SpreadIL
         }
         s_pos[pt] = pos;
     }
-    if (warp == 0) neighbour_ranges<3>(P, it, s_pre, s_beg, s_dlt, lane);
+    if (warp == 0) {
+        neighbour_ranges<3>(P, it, s_pre, s_beg, s_dlt, lane);
+        __syncwarp();
+        // Every batch takes a proportional piece of each neighbour range (the
+        // item's part of it): batch b gets visits [floor(b L / n), floor((b+1) L / n))
+        // of a range of length L, so every batch mixes the ranges (and the blocks
+        // they hit) while each piece stays contiguous for one bulk copy.  n is the
+        // least batch count whose pieces fit a stage: sum_r ceil(L_r / n) <= kRingBatch.
+        int len = 0, vst = 0;
+        if (lane < NR) {
+            vst = max(it.v0, s_pre[lane]);
+            len = max(0, min(it.v1, s_pre[lane + 1]) - vst);
+        }
+        const int nvis = it.v1 - it.v0;
+        int n = (nvis + kRingBatch - 1) / kRingBatch;
+        for (int guard = 0; n > 0 && guard < 64; ++guard) {
+            int need = len > 0 ? (len + n - 1) / n : 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) need += __shfl_xor_sync(0xffffffffu, need, o);
+            if (need <= kRingBatch) break;
+            n = n + (n + 15) / 16;  // grows by about 1/16 per round
+            if (n > nvis) n = nvis;
+        }
+        {
+            int need = (len > 0 && n > 0) ? (len + n - 1) / n : 0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) need += __shfl_xor_sync(0xffffffffu, need, o);
+            if (need > kRingBatch) n = nvis;  // one visit per range and batch: need <= 27 fits
+        }
+        if (lane < NR) {
+            s_len[lane] = len;
+            s_vst[lane] = vst;
+        }
+        if (lane == 0) s_nbat = n;
+    }
     if (threadIdx.x == 0) {
         for (int st = 0; st < NS; ++st) {
             mbar_init(&bar_raw[st], 1);
@@ -1315,10 +1352,8 @@ __global__ void __launch_bounds__(16 * 32, 1) spread_ring3_kernel(const SpreadIL
         mbar_fence_init();
     }
     __syncthreads();
-    const int nvis = it.v1 - it.v0;
-    const int nbat = (nvis + kRingBatch - 1) / kRingBatch;
+    const int nbat = s_nbat;
     auto stage = [&](int bb) { return ring + (bb % NS) * C::Stage; };
-    auto nb_of = [&](int bb) { return min(it.v1 - (it.v0 + bb * kRingBatch), kRingBatch); };
     // copies of batch pb into its stage (this warp produces it; the stage is free)
     auto issue = [&](int pb) {
         unsigned char *S = stage(pb);
@@ -1326,34 +1361,42 @@ __global__ void __launch_bounds__(16 * 32, 1) spread_ring3_kernel(const SpreadIL
         float *rr = reinterpret_cast<float *>(S + C::OffRec);
         int *rd = reinterpret_cast<int *>(S + C::OffRD);
         unsigned long long *br = &bar_raw[pb % NS];
-        const int V0 = it.v0 + pb * kRingBatch, V1 = V0 + nb_of(pb);
-        int lo = 0, hi = 0;  // lane r: the piece of neighbour range r inside [V0, V1)
+        // lane r: the piece of range r in batch pb, visits [vst + a, vst + e)
+        int a = 0, n = 0;
         if (lane < NR) {
-            lo = max(V0, s_pre[lane]);
-            hi = min(V1, s_pre[lane + 1]);
+            const int64_t L = s_len[lane];
+            a = (int)(L * pb / nbat);
+            n = (int)(L * (pb + 1) / nbat) - a;
         }
-        const int n = hi > lo ? hi - lo : 0;
-        unsigned bytes = (unsigned)n * (TS * 4 + (bulk_vals ? 256u : 0u));
+        int q0 = n;  // exclusive prefix of the piece sizes: the piece's first slot
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
-        if (lane == 0) mbar_arrive_tx(br, bytes);
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, q0, o);
+            if (lane >= o) q0 += t;
+        }
+        const int nb = __shfl_sync(0xffffffffu, q0, 31);
+        q0 -= n;
+        unsigned bytes = (unsigned)nb * (TS * 4 + (bulk_vals ? 256u : 0u));
+        if (lane == 0) {
+            s_nb[pb % NS] = nb;
+            mbar_arrive_tx(br, bytes);
+        }
         __syncwarp();
         if (n > 0) {
-            const int64_t j0 = (int64_t)s_beg[lane] + (lo - s_pre[lane]);
-            const int q0 = lo - V0;
+            const int64_t j0 = (int64_t)s_beg[lane] + (s_vst[lane] + a - s_pre[lane]);
             bulk_g2s(rr + q0 * TS, P.wtap + j0 * TS, (unsigned)n * TS * 4, br);
             if (bulk_vals) bulk_g2s(rv + q0 * 32, P.vals + j0 * 32, (unsigned)n * 256, br);
             const int d = s_dlt[lane];
             for (int q = q0; q < q0 + n; ++q) rd[q] = d;
         }
         if (!bulk_vals) {
-            // values one sample at a time (lane = channel), range by range
+            // values one sample at a time (lane = channel), piece by piece
             for (int r = 0; r < NR; ++r) {
-                const int l2 = max(V0, s_pre[r]), h2 = min(V1, s_pre[r + 1]);
-                for (int v = l2; v < h2; ++v) {
-                    const int64_t j = (int64_t)s_beg[r] + (v - s_pre[r]);
-                    cp_async8(rv + (v - V0) * 32 + lane, P.vals + j * nch + (c < nch ? c : 0), c < nch);
-                }
+                const int rn = __shfl_sync(0xffffffffu, n, r), ra = __shfl_sync(0xffffffffu, a, r);
+                const int rq = __shfl_sync(0xffffffffu, q0, r);
+                const int64_t j0 = (int64_t)s_beg[r] + (s_vst[r] + ra - s_pre[r]);
+                for (int k = 0; k < rn; ++k)
+                    cp_async8(rv + (rq + k) * 32 + lane, P.vals + (j0 + k) * nch + (c < nch ? c : 0), c < nch);
             }
             cp_async_commit();
         }
@@ -1370,7 +1413,7 @@ __global__ void __launch_bounds__(16 * 32, 1) spread_ring3_kernel(const SpreadIL
         float4 *tw4 = reinterpret_cast<float4 *>(S + C::OffTW);
         unsigned *tm = reinterpret_cast<unsigned *>(S + C::OffTM);
         const int *rd = reinterpret_cast<const int *>(S + C::OffRD);
-        const int nb = nb_of(pb);
+        const int nb = s_nb[pb % NS];
         for (int qq = 0; qq < nb; qq += 32) {
             const int q = qq + lane;
             if (q < nb) {
@@ -1440,7 +1483,7 @@ __global__ void __launch_bounds__(16 * 32, 1) spread_ring3_kernel(const SpreadIL
         const float2 *rv = reinterpret_cast<const float2 *>(S);
         const float4 *tw4 = reinterpret_cast<const float4 *>(S + C::OffTW);
         const unsigned *tm = reinterpret_cast<const unsigned *>(S + C::OffTM);
-        const int nb = nb_of(b);
+        const int nb = s_nb[b % NS];
         for (int q0 = 0; q0 < nb; q0 += 32) {
             bool hit = false;
             unsigned zl = 0;

@@ -55,9 +55,22 @@ def test_3d_golden_means_radial_32_coils(N, nspokes, nread, tile):
     yg = P.nufft(x, nufft_plan=gplan)
     yr = orc.nufft_fwd(x.cpu().numpy(), oplan)
     assert rel(yg, yr) < TOL
+    # the adjoint of the structured k-space (centre-heavy) against the same algorithm
+    # in float64: the GPU's sums stay within the tolerance of exact arithmetic
+    xa = P.nufft_adj(yg, nufft_plan=gplan)
+    x64 = orc.nufft_adj_f64(yg[:1].reshape(1, -1).cpu().numpy(), oplan)
+    assert rel(xa[:1], x64) < TOL
     yk = crandn(rng, B, nspokes, nread)
     xg = P.nufft_adj(torch.as_tensor(yk).cuda(), nufft_plan=gplan)
     assert rel(xg, orc.nufft_adj(yk, oplan)) < TOL
+    # no bounded wait of the spread gave up
+    import ctypes
+
+    from pyfourier_b200 import _lib
+
+    st = ctypes.c_int32(-1)
+    _lib.check(_lib.load().pfb_plan_status(gplan.interpolator.handle, ctypes.byref(st)))
+    assert st.value == 0
 
 
 def test_toeplitz_gram_subspace_spiral_48_frames_16_coils():

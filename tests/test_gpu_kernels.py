@@ -241,6 +241,53 @@ def test_interleaved_pipeline_matches_planar(case):
         _pipeline_both(plan, crn(6, 1, *N), crn(6, 12 * 64), zs=zs, zt=zt, L=Lseg)
 
 
+def _sorted_order(plan):
+    M = plan.interpolator.total_samples
+    order = torch.empty(M, dtype=torch.int32, device="cuda:0")
+    _lib().check(_lib().load().pfb_plan_order(plan.interpolator.handle, ctypes.c_void_p(order.data_ptr()),
+                                              _stream()))
+    return order.cpu().numpy()
+
+
+def _bin_keys(plan, op, frame, ndim, w=4):
+    """Bin keys ((tile << d | edge code) * F + frame) from the oracle's first taps."""
+    tile = plan.interpolator.tile[::-1]  # (x, y, z)
+    nos = op.os_shape[::-1]
+    M = frame.size
+    key_bin = np.zeros(M, np.int64)
+    code = np.zeros(M, np.int64)
+    stride = 1
+    for a in range(ndim):
+        x0m = op.index[ndim - 1 - a].reshape(-1, op.index[ndim - 1 - a].shape[-1])[:, 0].astype(np.int64)
+        nb = -(-nos[a] // tile[a])
+        tb = x0m // tile[a]
+        key_bin += tb * stride
+        stride *= nb
+        text = np.minimum(tile[a], nos[a] - tb * tile[a])
+        if nb > 1:
+            code |= ((x0m - tb * tile[a] + w - 1 >= text).astype(np.int64) << a)
+    return ((key_bin << ndim) | code) * plan.interpolator.nframes + frame
+
+
+def test_counting_sort_large_3d_radial():
+    """A 3D golden-means radial plan of 2 M samples (500 chunks of the sort, three
+    8-bit passes for its 2^19 keys): sorted by key, stable, a permutation."""
+    import bench
+    import pyfourier_b200 as pf
+
+    N = 160
+    coord = bench.golden_means_radial_3d(8000, 256, N)
+    plan = pf.plan_nufft(torch.as_tensor(coord), (N, N, N), width=4, oversamp=1.25, device="cuda:0")
+    order = _sorted_order(plan)
+    M = order.size
+    assert np.array_equal(np.sort(order), np.arange(M))
+    op = orc.plan_nufft(coord, (N, N, N), width=4, oversamp=1.25)
+    key = _bin_keys(plan, op, np.zeros(M, np.int64), 3)
+    ks = key[order]
+    assert np.all(np.diff(ks) >= 0)
+    assert np.all(np.diff(order)[np.diff(ks) == 0] > 0)
+
+
 @pytest.mark.parametrize("ndim", [2, 3])
 def test_counting_sort_is_stable_by_bin_key(ndim):
     """The plan's samples are ordered by the integer bin key

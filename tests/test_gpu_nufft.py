@@ -118,6 +118,10 @@ def test_crowded_3d_tiles_with_many_channels():
     coord = np.concatenate([hot, edge])[None]
     check_pair(coord, (N, N, N), crandn(rng, 20, N, N, N), crandn(rng, 20, 1, 6500), width=4, oversamp=1.25)
     check_pair(coord, (N, N, N), crandn(rng, 33, N, N, N), crandn(rng, 33, 1, 6500), width=6, oversamp=2.0)
+    # exactly 32 and 64 channels: the ring spread with bulk-copied values (32) and its
+    # per-sample value copies (64), on split crowded tiles
+    check_pair(coord, (N, N, N), crandn(rng, 32, N, N, N), crandn(rng, 32, 1, 6500), width=4, oversamp=1.25)
+    check_pair(coord, (N, N, N), crandn(rng, 64, N, N, N), crandn(rng, 64, 1, 6500), width=4, oversamp=1.25)
 
 
 @pytest.mark.parametrize("nch", [3, 8, 12, 16])
@@ -316,3 +320,48 @@ def test_autotune_keeps_results_and_caches(tmp_path, monkeypatch):
     res2 = P.autotune(plan2, batch=3)
     assert res2["cached"] is True and list(res2["tile"]) == list(res["tile"])
     assert rel(P.nufft(torch.as_tensor(x).cuda(), nufft_plan=plan2), orc.nufft_fwd(x, oplan)) < TOL
+
+
+def test_concurrent_applies_of_one_plan_from_two_threads():
+    """Two host threads apply one plan (and one Gram) on their own streams at the
+    same time: the shared cuFFT handle is used under the plan's lock from
+    set-stream to exec, so each thread's transform runs with its own stream and
+    work area and both results equal the sequential ones."""
+    import threading
+
+    P = pf()
+    rng = np.random.default_rng(30)
+    N = 96
+    coord = ((rng.random((40, 90, 1)) - 0.5) * N).astype(np.float32)  # 1D: library FFT path
+    plan = P.plan_nufft(torch.as_tensor(coord), (N,), width=4, oversamp=2.0, device="cuda:0")
+    gcoord = radial(30, 64, 32)
+    gm = P.plan_spgram(torch.as_tensor(gcoord), (32, 32), device="cuda:0")
+    ys = [torch.as_tensor(crandn(rng, 6, 40, 90)).cuda() for _ in range(2)]
+    xs = [torch.as_tensor(crandn(rng, 5, 32, 32)).cuda() for _ in range(2)]
+    ref_a = [P.nufft_adj(y, nufft_plan=plan) for y in ys]
+    ref_g = [P.sparse_gram(x, gm) for x in xs]
+    torch.cuda.synchronize()
+    out = [[None] * 2 for _ in range(2)]
+    errs = []
+
+    def work(i):
+        try:
+            s = torch.cuda.Stream()
+            with torch.cuda.stream(s):
+                for _ in range(20):
+                    a = P.nufft_adj(ys[i], nufft_plan=plan)
+                    g = P.sparse_gram(xs[i], gm)
+                s.synchronize()
+            out[i] = [a, g]
+        except Exception as e:  # pragma: no cover
+            errs.append(e)
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for i in range(2):
+        assert rel(out[i][0], ref_a[i].cpu().numpy()) < 1e-6
+        assert rel(out[i][1], ref_g[i].cpu().numpy()) < 1e-6

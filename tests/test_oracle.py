@@ -350,3 +350,21 @@ def test_threaded_glue_is_identical_to_per_item_glue():
     assert all(np.array_equal(r[i], orc.resize(x[i:i + 1], (120, 120, 120))[0]) for i in range(5))
     f = orc.fft_c(x, 3)
     assert all(np.array_equal(f[i], orc.fft_c(x[i:i + 1], 3)[0]) for i in range(5))
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_float64_adjoint_restatement(ndim):
+    """nufft_adj_f64 (the reference's adjoint algorithm in float64) agrees with the
+    float32 restatement to float32 rounding and with the direct NUDFT adjoint to the
+    kernel accuracy."""
+    rng = np.random.default_rng(31 + ndim)
+    N = (20,) * ndim
+    coord = ((rng.random((300, ndim)) - 0.5) * N[0]).astype(np.float32)
+    plan = orc.plan_nufft(coord, N, width=6, oversamp=2.0)
+    y = (rng.standard_normal((2, 300)) + 1j * rng.standard_normal((2, 300))).astype(np.complex64)
+    x64 = orc.nufft_adj_f64(y, plan)
+    x32 = orc.nufft_adj(y, plan)
+    assert orc.rel_l2(x32, x64) < 1e-6
+    G = float(np.prod(plan.os_shape))
+    ref = orc.nudft_adj(y, coord, N) / G
+    assert orc.rel_l2(x64, ref) < 1e-4
