@@ -129,13 +129,6 @@ int pfb_plan_set_chunk(pfb_plan *plan, int chunk);
  * Debug / parity aid; not used by the operators. */
 int pfb_plan_tables(const pfb_plan *plan, int axis, int32_t *index, float *value, void *stream);
 
-/* Status of the plan's kernels since the last call: 0, or 1 when a kernel gave up
- * a bounded wait on its own shared-memory barriers (every such wait gives up
- * after about two seconds instead of hanging; the kernel then leaves its tile
- * unwritten).  Synchronises the device, reads and clears the word.  No
- * counterpart in the reference (its kernels have no waits). */
-int pfb_plan_status(pfb_plan *plan, int32_t *status);
-
 /* The plan's sample order after the stable counting sort by bin key: order[j] =
  * the sample (caller's index) at sorted position j, int32 (total samples) on the
  * device.  Equal keys keep the caller's order.  Debug / parity aid; the

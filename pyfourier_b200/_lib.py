@@ -34,7 +34,6 @@ EXPORTS = (
     "pfb_gram_workspace_size", "pfb_gram_apply", "pfb_nufft_adj_noalloc",
     "pfb_grog_create", "pfb_grog_destroy", "pfb_grog_workspace_size", "pfb_grog_apply",
     "pfb_apply_workspace_size", "pfb_nufft_traj_grad", "pfb_nufft_stage", "pfb_plan_order", "pfb_spread_f64",
-    "pfb_plan_status",
 )
 
 
@@ -104,7 +103,6 @@ def load(path=LIB_PATH):
         "pfb_plan_set_chunk": (i32, [vp, i32]),
         "pfb_plan_tables": (i32, [vp, i32, vp, vp, vp]),
         "pfb_plan_order": (i32, [vp, vp, vp]),
-        "pfb_plan_status": (i32, [vp, P(ctypes.c_int32)]),
         "pfb_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),
         "pfb_nufft_fwd": (i32, [vp, P(ApplyT), vp, vp, vp, ctypes.c_size_t, vp]),
         "pfb_nufft_adj": (i32, [vp, P(ApplyT), vp, vp, vp, ctypes.c_size_t, vp]),

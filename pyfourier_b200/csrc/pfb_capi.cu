@@ -236,16 +236,6 @@ int pfb_plan_tables(const pfb_plan *p, int axis, int32_t *index, float *value, v
     return plan_tables(p, axis, index, value, static_cast<cudaStream_t>(stream));
 }
 
-int pfb_plan_status(pfb_plan *p, int32_t *status) {
-    if (!p || !status) return fail(PFB_ERR_INVALID, "NULL argument");
-    DeviceGuard dg(p->device);
-    int v = 0;
-    PFB_CUDA_TRY(cudaMemcpy(&v, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (v) PFB_CUDA_TRY(cudaMemset(p->d_status, 0, sizeof(int)));
-    *status = v;
-    return PFB_OK;
-}
-
 int pfb_plan_order(const pfb_plan *p, int32_t *order, void *stream) {
     if (!p || !order) return fail(PFB_ERR_INVALID, "NULL argument");
     if (p->mtot == 0) return PFB_OK;

@@ -167,8 +167,6 @@ struct pfb_plan {
     int fft_fused = -1;          // -1 not decided, 0 not applicable, 1 ready
     pfb::FftAxis fft_ax[pfb::kMaxDim];
     float2 *d_fft_tw = nullptr;  // twiddles of all axes and stages
-    // device status word: kernels whose bounded waits gave up set it (0 = ok)
-    int *d_status = nullptr;
 };
 
 namespace pfb {

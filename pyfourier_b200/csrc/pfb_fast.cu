@@ -1191,372 +1191,6 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
     }
 }
 
-// ------------------------------------------------------------------------------------
-// mbarrier and bulk-copy helpers (CTA scope; no cluster multicast anywhere)
-// ------------------------------------------------------------------------------------
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
-    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(unsigned long long *b, unsigned bytes) {
-    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(
-                     smem_u32(b)), "r"(bytes) : "memory");
-}
-// Wait for the phase of parity `par` to complete.  Bounded: false after about
-// 2^32 SM cycles (about 2 s), so that a wait that can never end returns.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned par) {
-    const long long t0 = clock64();
-    while (true) {
-        unsigned ok;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                     " selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(ok)
-                     : "r"(smem_u32(b)), "r"(par)
-                     : "memory");
-        if (ok) return true;
-        if (clock64() - t0 > (1ll << 32)) return false;
-    }
-}
-// Global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
-// completing on barrier b's transaction count.
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *b) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(b))
-                 : "memory");
-}
-
-// Ring form of the 32-channel register-tile spread (3D, W <= 4).  Same
-// ownership as spread_reg3_kernel -- 16 warps, each holding one 4 x 4 x 2 block
-// of the 8^3 tile x 32 channels in registers, no atomics -- but the samples
-// stream through a ring of kRingStages stages instead of a double buffer
-// between two CTA barriers per batch:
-//   * a batch holds up to kRingBatch visits: from each of the item's neighbour
-//     ranges a proportional, contiguous piece, so that every batch mixes the
-//     ranges (whose samples hit different blocks) and one bulk copy per piece
-//     moves the plan records (weights + first taps) and, when the apply has
-//     exactly 32 channels, the channel values (otherwise one cp.async per
-//     sample), completing on the stage's transaction barrier;
-//   * batch pb is produced by warp pb % 16: after every warp has released the
-//     stage's previous batch it issues the copies, consumes its current batch
-//     while they land, then turns the records into tile-relative (w, w) weight
-//     pairs and 24-bit occupancy masks (one sample per lane) and marks the
-//     stage full;
-//   * every warp waits only for the stage it consumes and releases it after.
-// Warps drift apart by up to kRingStages - 1 batches instead of meeting at
-// every batch.  Every wait is bounded; a wait that gives up sets the plan's
-// status word and the tile is not written.
-constexpr int kRingStages = 4;
-constexpr int kRingBatch = 96;
-constexpr int kRingRec = 16;  // tap_rec(3, 4)
-struct RingCfg {
-    static constexpr size_t Vals = (size_t)kRingBatch * 32 * sizeof(float2);
-    static constexpr size_t Rec = (size_t)kRingBatch * kRingRec * sizeof(float);
-    static constexpr size_t TW = (size_t)kRingBatch * 16 * sizeof(float4);  // 12 used, 16 slots (swizzle)
-    static constexpr size_t TM = (size_t)kRingBatch * sizeof(unsigned);
-    static constexpr size_t RD = (size_t)kRingBatch * sizeof(int);
-    static constexpr size_t OffRec = Vals, OffTW = OffRec + Rec, OffTM = OffTW + TW, OffRD = OffTM + TM;
-    static constexpr size_t Stage = OffRD + RD;
-    static constexpr size_t Out = (size_t)kRegPts * 33 * sizeof(float2);
-    static constexpr size_t Ring = (size_t)kRingStages * Stage;
-    static constexpr size_t Smem = kRegPts * sizeof(int) + (Ring > Out ? Ring : Out);
-    static_assert(Stage % 16 == 0 && OffRec % 16 == 0 && OffTW % 16 == 0, "16-byte aligned stage arrays");
-    static_assert(Smem + 1024 <= 227 * 1024, "shared memory of one CTA");
-};
-
-template <int WM>
-__global__ void __launch_bounds__(16 * 32, 1) spread_ring3_kernel(const SpreadIL P, int *status) {
-    static_assert(WM == 4, "the ring spread takes kernel widths up to 4");
-    constexpr int NR = 27, TS = kRingRec, NS = kRingStages;
-    using C = RingCfg;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    int *s_pos = reinterpret_cast<int *>(smraw);
-    unsigned char *ring = smraw + kRegPts * sizeof(int);
-    float2 *s_out = reinterpret_cast<float2 *>(ring);  // after the last batch
-    __shared__ int s_pre[NR + 1];
-    __shared__ int s_beg[NR];
-    __shared__ int s_dlt[NR];
-    __shared__ __align__(8) unsigned long long bar_raw[NS], bar_full[NS], bar_empty[NS];
-    __shared__ int s_fail, s_nbat;
-    __shared__ int s_len[NR], s_vst[NR];  // the item's part of range r: length and first visit
-    __shared__ int s_nb[NS];               // samples of the batch a stage holds
-    const OwnerItem it = P.items[blockIdx.x];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nch = P.ch.nch;
-    const int c0 = blockIdx.y * 32, c = c0 + lane;
-    const bool bulk_vals = nch == 32;
-    int org[3], text[3], wrap[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int tc = tile_coord(it.tile, a, P.g);
-        org[a] = tc * P.g.tile[a];
-        text[a] = min(P.g.tile[a], P.g.nos[a] - org[a]);
-        wrap[a] = P.g.nbins[a] == 1 ? text[a] : 0;
-    }
-    for (int pt = threadIdx.x; pt < kRegPts; pt += blockDim.x) {
-        const int t0 = pt & 7, t1 = (pt >> 3) & 7, t2 = pt >> 6;
-        int pos = -1;
-        if (t0 < text[0] && t1 < text[1] && t2 < text[2]) {
-            pos = pmod(org[0] + t0 - P.g.sh[0], P.g.nos[0]) +
-                  pmod(org[1] + t1 - P.g.sh[1], P.g.nos[1]) * P.g.nos[0] +
-                  pmod(org[2] + t2 - P.g.sh[2], P.g.nos[2]) * P.g.nos[0] * P.g.nos[1];
-        }
-        s_pos[pt] = pos;
-    }
-    if (warp == 0) {
-        neighbour_ranges<3>(P, it, s_pre, s_beg, s_dlt, lane);
-        __syncwarp();
-        // Every batch takes a proportional piece of each neighbour range (the
-        // item's part of it): batch b gets visits [floor(b L / n), floor((b+1) L / n))
-        // of a range of length L, so every batch mixes the ranges (and the blocks
-        // they hit) while each piece stays contiguous for one bulk copy.  n is the
-        // least batch count whose pieces fit a stage: sum_r ceil(L_r / n) <= kRingBatch.
-        int len = 0, vst = 0;
-        if (lane < NR) {
-            vst = max(it.v0, s_pre[lane]);
-            len = max(0, min(it.v1, s_pre[lane + 1]) - vst);
-        }
-        const int nvis = it.v1 - it.v0;
-        int n = (nvis + kRingBatch - 1) / kRingBatch;
-        for (int guard = 0; n > 0 && guard < 64; ++guard) {
-            int need = len > 0 ? (len + n - 1) / n : 0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) need += __shfl_xor_sync(0xffffffffu, need, o);
-            if (need <= kRingBatch) break;
-            n = n + (n + 15) / 16;  // grows by about 1/16 per round
-            if (n > nvis) n = nvis;
-        }
-        {
-            int need = (len > 0 && n > 0) ? (len + n - 1) / n : 0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) need += __shfl_xor_sync(0xffffffffu, need, o);
-            if (need > kRingBatch) n = nvis;  // one visit per range and batch: need <= 27 fits
-        }
-        if (lane < NR) {
-            s_len[lane] = len;
-            s_vst[lane] = vst;
-        }
-        if (lane == 0) s_nbat = n;
-    }
-    if (threadIdx.x == 0) {
-        for (int st = 0; st < NS; ++st) {
-            mbar_init(&bar_raw[st], 1);
-            mbar_init(&bar_full[st], 1);
-            mbar_init(&bar_empty[st], 16);
-        }
-        s_fail = 0;
-        mbar_fence_init();
-    }
-    __syncthreads();
-    const int nbat = s_nbat;
-    auto stage = [&](int bb) { return ring + (bb % NS) * C::Stage; };
-    // copies of batch pb into its stage (this warp produces it; the stage is free)
-    auto issue = [&](int pb) {
-        unsigned char *S = stage(pb);
-        float2 *rv = reinterpret_cast<float2 *>(S);
-        float *rr = reinterpret_cast<float *>(S + C::OffRec);
-        int *rd = reinterpret_cast<int *>(S + C::OffRD);
-        unsigned long long *br = &bar_raw[pb % NS];
-        // lane r: the piece of range r in batch pb, visits [vst + a, vst + e)
-        int a = 0, n = 0;
-        if (lane < NR) {
-            const int64_t L = s_len[lane];
-            a = (int)(L * pb / nbat);
-            n = (int)(L * (pb + 1) / nbat) - a;
-        }
-        int q0 = n;  // exclusive prefix of the piece sizes: the piece's first slot
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, q0, o);
-            if (lane >= o) q0 += t;
-        }
-        const int nb = __shfl_sync(0xffffffffu, q0, 31);
-        q0 -= n;
-        unsigned bytes = (unsigned)nb * (TS * 4 + (bulk_vals ? 256u : 0u));
-        if (lane == 0) {
-            s_nb[pb % NS] = nb;
-            mbar_arrive_tx(br, bytes);
-        }
-        __syncwarp();
-        if (n > 0) {
-            const int64_t j0 = (int64_t)s_beg[lane] + (s_vst[lane] + a - s_pre[lane]);
-            bulk_g2s(rr + q0 * TS, P.wtap + j0 * TS, (unsigned)n * TS * 4, br);
-            if (bulk_vals) bulk_g2s(rv + q0 * 32, P.vals + j0 * 32, (unsigned)n * 256, br);
-            const int d = s_dlt[lane];
-            for (int q = q0; q < q0 + n; ++q) rd[q] = d;
-        }
-        if (!bulk_vals) {
-            // values one sample at a time (lane = channel), piece by piece
-            for (int r = 0; r < NR; ++r) {
-                const int rn = __shfl_sync(0xffffffffu, n, r), ra = __shfl_sync(0xffffffffu, a, r);
-                const int rq = __shfl_sync(0xffffffffu, q0, r);
-                const int64_t j0 = (int64_t)s_beg[r] + (s_vst[r] + ra - s_pre[r]);
-                for (int k = 0; k < rn; ++k)
-                    cp_async8(rv + (rq + k) * 32 + lane, P.vals + (j0 + k) * nch + (c < nch ? c : 0), c < nch);
-            }
-            cp_async_commit();
-        }
-    };
-    // tile-relative weights of batch pb, one sample per lane: entry (a, t) = weight of
-    // tile coordinate t on axis a (zero outside the support and the tile), stored as
-    // (w, w) pairs, 2 entries per float4 slot, slot u of sample q at u ^ (q & 15)
-    auto convert = [&](int pb) -> bool {
-        if (!bulk_vals) cp_async_wait_all();
-        if (!mbar_wait(&bar_raw[pb % NS], (pb / NS) & 1)) return false;
-        __syncwarp();
-        unsigned char *S = stage(pb);
-        const float *rr = reinterpret_cast<const float *>(S + C::OffRec);
-        float4 *tw4 = reinterpret_cast<float4 *>(S + C::OffTW);
-        unsigned *tm = reinterpret_cast<unsigned *>(S + C::OffTM);
-        const int *rd = reinterpret_cast<const int *>(S + C::OffRD);
-        const int nb = s_nb[pb % NS];
-        for (int qq = 0; qq < nb; qq += 32) {
-            const int q = qq + lane;
-            if (q < nb) {
-                const float4 *rec = reinterpret_cast<const float4 *>(rr + q * TS);
-                const float4 wxa = rec[0], wya = rec[1], wza = rec[2], xa = rec[3];
-                const int x0[3] = {__float_as_int(xa.x), __float_as_int(xa.y), __float_as_int(xa.z)};
-                const float W[3][4] = {{wxa.x, wxa.y, wxa.z, wxa.w}, {wya.x, wya.y, wya.z, wya.w},
-                                       {wza.x, wza.y, wza.z, wza.w}};
-                const int dl = rd[q];
-                unsigned mask = 0;
-                float4 *t4 = tw4 + q * 16;
-                const int sw = q & 15;
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    int d = x0[a] - org[a];
-                    if (((dl >> a) & 1) && d >= 0) d -= P.g.nos[a];
-                    float wt[8];
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        int i = t - d;
-                        if (wrap[a] && i < 0) i += wrap[a];
-                        const float w = i == 0 ? W[a][0] : (i == 1 ? W[a][1] : (i == 2 ? W[a][2] : W[a][3]));
-                        wt[t] = (t < text[a] && i >= 0 && i < P.g.w[a]) ? w : 0.f;
-                        mask |= (wt[t] != 0.f ? 1u : 0u) << (a * 8 + t);
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        t4[(a * 4 + u) ^ sw] = make_float4(wt[2 * u], wt[2 * u], wt[2 * u + 1], wt[2 * u + 1]);
-                }
-                tm[q] = mask;
-            }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&bar_full[pb % NS]);
-        return true;
-    };
-    bool ok = true;
-    // prologue: batches 0 .. NS - 2 (fresh stages), batch pb by warp pb % 16
-    for (int pb = 0; pb < NS - 1 && pb < nbat; ++pb)
-        if (pb % 16 == warp) {
-            issue(pb);
-            ok = convert(pb);
-        }
-    const int bx0 = (warp & 1) * 4, by0 = ((warp >> 1) & 1) * 4, bz0 = (warp >> 2) * 2;
-    const unsigned bmx = 0xFu << bx0, bmy = 0xFu << (8 + by0), bmz = 0x3u << (16 + bz0);
-    float2 acc[32];
-#pragma unroll
-    for (int q = 0; q < 32; ++q) acc[q] = make_float2(0.f, 0.f);
-    int pending = -1;  // a batch whose copies this warp issued and has not converted yet
-    for (int b = 0; ok && b < nbat; ++b) {
-        const int pb = b + NS - 1;
-        const bool mine = pb < nbat && pb % 16 == warp;
-        if (mine) {
-            // the stage of pb last held batch pb - NS = b - 1: wait until every warp released it
-            // (pb = NS - 1 takes a fresh stage: the wait for parity 1 passes at once)
-            if (!mbar_wait(&bar_empty[pb % NS], ((pb / NS) - 1) & 1)) { ok = false; break; }
-            issue(pb);
-            pending = pb;
-        }
-        // full: converted weights and masks; raw: the bulk-copied values themselves
-        // (already complete once the batch is full; waited on for their visibility)
-        if (!mbar_wait(&bar_full[b % NS], (b / NS) & 1) || !mbar_wait(&bar_raw[b % NS], (b / NS) & 1)) {
-            ok = false;
-            break;
-        }
-        const unsigned char *S = stage(b);
-        const float2 *rv = reinterpret_cast<const float2 *>(S);
-        const float4 *tw4 = reinterpret_cast<const float4 *>(S + C::OffTW);
-        const unsigned *tm = reinterpret_cast<const unsigned *>(S + C::OffTM);
-        const int nb = s_nb[b % NS];
-        for (int q0 = 0; q0 < nb; q0 += 32) {
-            bool hit = false;
-            unsigned zl = 0;
-            if (q0 + lane < nb) {
-                const unsigned m = tm[q0 + lane];
-                zl = (m >> (16 + bz0)) & 3u;
-                hit = (m & bmx) && (m & bmy) && (m & bmz);
-            }
-            unsigned hm = __ballot_sync(0xffffffffu, hit);
-            const unsigned z0 = __ballot_sync(0xffffffffu, zl & 1u), z1 = __ballot_sync(0xffffffffu, zl & 2u);
-            while (hm) {
-                const int k = __ffs(hm) - 1, q = q0 + k;
-                hm &= hm - 1;
-                const float2 v = rv[q * 32 + lane];
-                const float4 *t4 = tw4 + q * 16;
-                const int sw = q & 15;
-                const float4 x01 = t4[(bx0 >> 1) ^ sw], x23 = t4[((bx0 >> 1) + 1) ^ sw];
-                const float4 y01 = t4[((8 + by0) >> 1) ^ sw], y23 = t4[(((8 + by0) >> 1) + 1) ^ sw];
-                const float4 z01 = t4[((16 + bz0) >> 1) ^ sw];
-                const float2 wx2[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
-                                       make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
-                const float2 wy[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w),
-                                      make_float2(y23.x, y23.y), make_float2(y23.z, y23.w)};
-                const float2 wz[2] = {make_float2(z01.x, z01.y), make_float2(z01.z, z01.w)};
-                switch (((z0 >> k) & 1u) | (((z1 >> k) & 1u) << 1)) {
-                    case 1: reg3_rows<0, 3, 0, 0>(acc, wx2, wy, wz, v); break;
-                    case 2: reg3_rows<0, 3, 1, 1>(acc, wx2, wy, wz, v); break;
-                    case 3: reg3_rows<0, 3, 0, 1>(acc, wx2, wy, wz, v); break;
-                    default: break;
-                }
-            }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&bar_empty[b % NS]);
-        if (mine) {
-            if (!convert(pb)) { ok = false; break; }
-            pending = -1;
-        }
-    }
-    if (!ok) {
-        s_fail = 1;
-        // copies still in flight land before the ring is reused or the CTA exits
-        if (!bulk_vals) cp_async_wait_all();
-        if (pending >= 0) mbar_wait(&bar_raw[pending % NS], (pending / NS) & 1);
-    }
-    __syncthreads();  // every stage consumed: reuse the ring for the output tile
-    const bool failed = s_fail != 0;
-    if (!failed) {
-#pragma unroll
-        for (int q = 0; q < 32; ++q) s_out[(warp * 32 + q) * 33 + lane] = acc[q];
-    }
-    __syncthreads();
-    if (failed) {
-        if (threadIdx.x == 0 && status) atomicExch(status, 1);
-        return;
-    }
-    const int grp = P.ch.K ? 0 : (it.frame < 0 ? 0 : it.frame);
-    for (int e = threadIdx.x; e < 32 * kRegPts; e += blockDim.x) {
-        const int ce = e / kRegPts, pt = e - ce * kRegPts;
-        const int ch = c0 + ce;
-        if (ch >= nch) break;
-        const int pos = s_pos[pt];
-        if (pos < 0) continue;
-        const int x = pt & 7, y = (pt >> 3) & 7, z = pt >> 6;
-        const int w = (x >> 2) | ((y >> 2) << 1) | ((z >> 1) << 2);
-        const int q = (x & 3) | ((y & 3) << 2) | ((z & 1) << 4);
-        const float2 vv = s_out[(w * 32 + q) * 33 + ce];
-        float2 *Gp = P.grid + ((int64_t)grp * nch + ch) * P.g.gvol;
-        if (it.atomic) atomicAdd(Gp + pos, vv);
-        else Gp[pos] = vv;
-    }
-}
-
 // Register-tile spread for 2D tiles of up to 16 x 16 points: the 2D form of
 // spread_reg3_kernel.  Eight blocks of 4 (x) x 8 (y) points tile the packed
 // 16 x 16 tile; a lane group of CPW channels owns one block, its 32 points x
@@ -1855,25 +1489,10 @@ int launch_spread_reg2_w(const SpreadIL &P, int nitems, int nch, cudaStream_t s)
 }
 
 template <int WM>
-int launch_spread_ring3_t(const SpreadIL &P, int nitems, int nchunks, int *status, cudaStream_t s) {
-    auto k = spread_ring3_kernel<WM>;
-    PFB_RAISE_SMEM(k, (int)RingCfg::Smem);
-    dim3 grid(nitems, nchunks);
-    k<<<grid, 16 * 32, RingCfg::Smem, s>>>(P, status);
-    PFB_CHECK_LAUNCH();
-    return PFB_OK;
-}
-
-template <int WM>
-int launch_spread_reg3_w(const SpreadIL &P, int nitems, int nch, int *status, cudaStream_t s) {
+int launch_spread_reg3_w(const SpreadIL &P, int nitems, int nch, cudaStream_t s) {
     // channel groups of 8 or 16 keep few-channel spreads on register tiles
     if (nch <= 8) return launch_spread_reg3_t<WM, 8>(P, nitems, 1, s);
     if (nch <= 16) return launch_spread_reg3_t<WM, 16>(P, nitems, 1, s);
-    // 32-channel groups: the ring form (bulk copies need 16-byte aligned sample rows)
-    if constexpr (WM == 4) {
-        if ((reinterpret_cast<uintptr_t>(P.vals) & 15) == 0)
-            return launch_spread_ring3_t<WM>(P, nitems, (nch + 31) / 32, status, s);
-    }
     return launch_spread_reg3_t<WM, 32>(P, nitems, (nch + 31) / 32, s);
 }
 
@@ -2156,9 +1775,9 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
                 p->g.tile[2] <= kRegTile) {
                 // register-tile form: channels in groups of 8, 16 or 32 per block, no
                 // shared atomics
-                return wmv == 1 ? launch_spread_reg3_w<1>(S, nitems, c.nch, p->d_status, s)
-                                : (wmv == 4 ? launch_spread_reg3_w<4>(S, nitems, c.nch, p->d_status, s)
-                                            : launch_spread_reg3_w<8>(S, nitems, c.nch, p->d_status, s));
+                return wmv == 1 ? launch_spread_reg3_w<1>(S, nitems, c.nch, s)
+                                : (wmv == 4 ? launch_spread_reg3_w<4>(S, nitems, c.nch, s)
+                                            : launch_spread_reg3_w<8>(S, nitems, c.nch, s));
             }
             if (p->g.ndim == 2 && p->g.tile[0] <= kReg2Tile && p->g.tile[1] <= kReg2Tile && c.nch > 16) {
                 // 2D register tiles (16 x 16 points), 32 channels per lane group (with

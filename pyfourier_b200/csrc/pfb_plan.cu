@@ -172,8 +172,6 @@ void free_plan_buffers(pfb_plan *p) {
     cudaFree(p->d_items_frame);
     cudaFree(p->d_items_all);
     cudaFree(p->d_frame_off);
-    cudaFree(p->d_status);
-    p->d_status = nullptr;
     p->d_perm = p->d_sframe = p->d_bin_start = nullptr;
     p->d_items_frame = p->d_items_all = nullptr;
     p->d_frame_off = nullptr;
@@ -331,8 +329,6 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
         return cleanup(fail(PFB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e))); } while (0)
 
     PFB_TRY_ST(dev_alloc(&p->d_frame_off, nframes + 1));
-    PFB_TRY_ST(dev_alloc(&p->d_status, 1));
-    PFB_TRY_CU(cudaMemsetAsync(p->d_status, 0, sizeof(int), stream));
     PFB_TRY_CU(cudaMemcpyAsync(p->d_frame_off, frame_offsets, (nframes + 1) * sizeof(int64_t),
                                cudaMemcpyHostToDevice, stream));
     for (int a = 0; a < ndim; ++a) PFB_TRY_ST(dev_alloc(&p->d_cos[a], mtot));

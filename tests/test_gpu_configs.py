@@ -55,22 +55,18 @@ def test_3d_golden_means_radial_32_coils(N, nspokes, nread, tile):
     yg = P.nufft(x, nufft_plan=gplan)
     yr = orc.nufft_fwd(x.cpu().numpy(), oplan)
     assert rel(yg, yr) < TOL
-    # the adjoint of the structured k-space (centre-heavy) against the same algorithm
-    # in float64: the GPU's sums stay within the tolerance of exact arithmetic
+    # the adjoint of the structured (centre-heavy) k-space against the same algorithm
+    # in float64: the reference's float32 serial sums drift from it (1e-4 here), the
+    # GPU's per-block register sums stay close (about 1e-5) and always closer
     xa = P.nufft_adj(yg, nufft_plan=gplan)
-    x64 = orc.nufft_adj_f64(yg[:1].reshape(1, -1).cpu().numpy(), oplan)
-    assert rel(xa[:1], x64) < TOL
+    y0 = yg[:1].reshape(1, -1).cpu().numpy()
+    x64 = orc.nufft_adj_f64(y0, oplan)
+    x32 = orc.nufft_adj(y0.reshape(1, nspokes, nread), oplan)
+    e_gpu, e_orc = rel(xa[:1], x64), rel(x32.reshape(x64.shape), x64)
+    assert e_gpu < 2e-5 and e_gpu < e_orc, (e_gpu, e_orc)
     yk = crandn(rng, B, nspokes, nread)
     xg = P.nufft_adj(torch.as_tensor(yk).cuda(), nufft_plan=gplan)
     assert rel(xg, orc.nufft_adj(yk, oplan)) < TOL
-    # no bounded wait of the spread gave up
-    import ctypes
-
-    from pyfourier_b200 import _lib
-
-    st = ctypes.c_int32(-1)
-    _lib.check(_lib.load().pfb_plan_status(gplan.interpolator.handle, ctypes.byref(st)))
-    assert st.value == 0
 
 
 def test_toeplitz_gram_subspace_spiral_48_frames_16_coils():

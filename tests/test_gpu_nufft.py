@@ -118,8 +118,7 @@ def test_crowded_3d_tiles_with_many_channels():
     coord = np.concatenate([hot, edge])[None]
     check_pair(coord, (N, N, N), crandn(rng, 20, N, N, N), crandn(rng, 20, 1, 6500), width=4, oversamp=1.25)
     check_pair(coord, (N, N, N), crandn(rng, 33, N, N, N), crandn(rng, 33, 1, 6500), width=6, oversamp=2.0)
-    # exactly 32 and 64 channels: the ring spread with bulk-copied values (32) and its
-    # per-sample value copies (64), on split crowded tiles
+    # exactly 32 and 64 channels (one and two full 32-channel groups) on split crowded tiles
     check_pair(coord, (N, N, N), crandn(rng, 32, N, N, N), crandn(rng, 32, 1, 6500), width=4, oversamp=1.25)
     check_pair(coord, (N, N, N), crandn(rng, 64, N, N, N), crandn(rng, 64, 1, 6500), width=4, oversamp=1.25)
 
