@@ -1446,7 +1446,8 @@ int layout_ws(pfb_plan *p, const Chan &c, WsLayout *L, cufftHandle *h, size_t *w
 template <int D, int WM>
 int launch_interp_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
     // element offsets point * nch in 32 bits when the grid allows it
-    if (P.g.gvol * (int64_t)P.ch.nch < (1LL << 31)) interp_il_kernel<D, WM, false><<<blocks, kTileWarps * 32, 0, s>>>(P);
+    const bool wide = P.g.gvol * (int64_t)P.ch.nch >= (1LL << 31);
+    if (!wide) interp_il_kernel<D, WM, false><<<blocks, kTileWarps * 32, 0, s>>>(P);
     else interp_il_kernel<D, WM, true><<<blocks, kTileWarps * 32, 0, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
