@@ -5,7 +5,8 @@
 // (x0 = ceil(c_os - W/2) mod n_os, _grid/_plan.py:192-210).  The sort is a
 // least-significant-digit sequence of counting sorts over 8-bit digits: each
 // pass histograms the digit per chunk of samples, scans the (digit, chunk)
-// counts into output offsets, and scatters every sample to
+// counts into output offsets (a segmented prefix sum over all CTAs), and
+// scatters every sample to
 // offset[digit][chunk] + (its rank among the chunk's samples with the same
 // digit that precede it).  Every pass is stable, so equal keys keep the order
 // of the caller's samples and the result is deterministic (bit for bit the
@@ -65,6 +66,58 @@ __global__ void __launch_bounds__(1024) exclusive_scan_kernel(int *__restrict__ 
     }
 }
 
+// Exclusive prefix sum of a long array in three steps: per-segment sums
+// (kScanSeg elements per CTA), an exclusive scan of the segment sums in one CTA
+// (exclusive_scan_kernel), then each CTA rescans its segment from its offset.
+constexpr int kScanSeg = 4096;
+__global__ void __launch_bounds__(256) segment_sum_kernel(const int *__restrict__ a, int64_t len,
+                                                          int *__restrict__ sums) {
+    __shared__ int s[256];
+    const int64_t b = (int64_t)blockIdx.x * kScanSeg;
+    int v = 0;
+    for (int i = threadIdx.x; i < kScanSeg; i += 256) {
+        const int64_t k = b + i;
+        if (k < len) v += a[k];
+    }
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 128; off > 0; off >>= 1) {
+        if (threadIdx.x < off) s[threadIdx.x] += s[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[blockIdx.x] = s[0];
+}
+
+// segment-local exclusive scan plus the segment's offset; thread t owns the 16
+// consecutive elements t * 16 .. t * 16 + 15 of the segment
+__global__ void __launch_bounds__(256) segment_scan_kernel(int *__restrict__ a, int64_t len,
+                                                           const int *__restrict__ offs) {
+    constexpr int PER = kScanSeg / 256;
+    __shared__ int s[256];
+    const int64_t b = (int64_t)blockIdx.x * kScanSeg + threadIdx.x * PER;
+    int v[PER];
+    int sum = 0;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        v[i] = b + i < len ? a[b + i] : 0;
+        sum += v[i];
+    }
+    s[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {
+        const int t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+        __syncthreads();
+        s[threadIdx.x] += t;
+        __syncthreads();
+    }
+    int run = offs[blockIdx.x] + s[threadIdx.x] - sum;
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        if (b + i < len) a[b + i] = run;
+        run += v[i];
+    }
+}
+
 // Stable scatter of one pass.  A chunk is walked in rounds of 256 samples in
 // sample order (thread t holds sample base + 256 r + t); within a round a
 // sample's rank among equal digits is the count in earlier warps plus the
@@ -113,8 +166,9 @@ __global__ void __launch_bounds__(kSortThreads) digit_scatter_kernel(const int *
 
 size_t counting_sort_temp_bytes(int64_t n) {
     const int64_t nchunks = (n + kSortChunk - 1) / kSortChunk;
-    // two key / value buffers and the (digit, chunk) counts
-    return (size_t)(2 * n + (int64_t)kDigits * nchunks + 64) * sizeof(int);
+    const int64_t nseg = ((int64_t)kDigits * nchunks + kScanSeg - 1) / kScanSeg;
+    // two key / value buffers, the (digit, chunk) counts and their segment sums
+    return (size_t)(2 * n + (int64_t)kDigits * nchunks + nseg + 64) * sizeof(int);
 }
 
 int counting_sort_pairs(const int *keys, const int *vals, int *keys_out, int *vals_out, int64_t n, int end_bit,
@@ -126,6 +180,9 @@ int counting_sort_pairs(const int *keys, const int *vals, int *keys_out, int *va
     int *ka = static_cast<int *>(temp);
     int *va = ka + n;
     int *counts = va + n;
+    const int64_t ncount = (int64_t)kDigits * nchunks;
+    const int nseg = (int)((ncount + kScanSeg - 1) / kScanSeg);
+    int *segs = counts + ncount;
     const int passes = std::max(1, (end_bit + 7) / 8);
     // pass p reads (in) and writes (out); the last pass writes keys_out / vals_out
     const int *kin = keys, *vin = vals;
@@ -136,7 +193,11 @@ int counting_sort_pairs(const int *keys, const int *vals, int *keys_out, int *va
         int *vout = last ? vals_out : (((passes - 1 - p) & 1) ? va : vals_out);
         digit_count_kernel<<<nchunks, kSortThreads, 0, s>>>(kin, (int)n, 8 * p, nchunks, counts);
         PFB_CHECK_LAUNCH();
-        exclusive_scan_kernel<<<1, 1024, 0, s>>>(counts, (int64_t)kDigits * nchunks);
+        segment_sum_kernel<<<nseg, 256, 0, s>>>(counts, ncount, segs);
+        PFB_CHECK_LAUNCH();
+        exclusive_scan_kernel<<<1, 1024, 0, s>>>(segs, nseg);
+        PFB_CHECK_LAUNCH();
+        segment_scan_kernel<<<nseg, 256, 0, s>>>(counts, ncount, segs);
         PFB_CHECK_LAUNCH();
         digit_scatter_kernel<<<nchunks, kSortThreads, 0, s>>>(kin, vin, (int)n, 8 * p, nchunks, counts, kout, vout);
         PFB_CHECK_LAUNCH();
