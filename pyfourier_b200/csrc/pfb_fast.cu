@@ -268,11 +268,11 @@ inline int out_rows(int width) {
 
 // vals[iperm[g]][ch] = y[b][g] * w[g] * conj(B_l(t)) * conj(basis[f, k])
 __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
-    extern __shared__ float2 sm[];  // [rows][B]
+    extern __shared__ float2 sm[];  // [rows][B | 1]
     __shared__ int s_j[kMaxOutRows];
     const int R = P.rows;
     const int64_t g0 = (int64_t)blockIdx.x * R;
-    const int B = P.ch.B;
+    const int B = P.ch.B, SP = B | 1;  // odd row pitch: a warp's column accesses hit distinct banks
     for (int gg = threadIdx.x; gg < R; gg += blockDim.x) s_j[gg] = g0 + gg < P.mtot ? P.iperm[g0 + gg] : 0;
     for (int e = threadIdx.x; e < R * B; e += blockDim.x) {
         const int b = e / R, gg = e - b * R;
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
                 v.y *= w;
             }
         }
-        sm[gg * B + b] = v;
+        sm[gg * SP + b] = v;
     }
     __syncthreads();
     const int nch = P.ch.nch, Kc = P.ch.K ? P.ch.K : 1;
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
         if (g >= P.mtot) continue;
         const int64_t j = s_j[gg];
         const int k = c % Kc, lb = c / Kc, b = lb % B, l = lb / B;
-        float2 v = sm[gg * B + b];
+        float2 v = sm[gg * SP + b];
         if (P.factors && (P.tB || P.ch.K)) {
             const int f = P.sframe[j];
             if (P.tB) {
@@ -311,17 +311,17 @@ __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
 
 // y[b][g] (+)= w[g] * sum_{l,k} B_l(t) basis[f, k] res[iperm[g]][(l, b, k)]
 __global__ void __launch_bounds__(256) out_il_kernel(const SampIL P) {
-    extern __shared__ float2 sm[];  // [rows][nch]
+    extern __shared__ float2 sm[];  // [rows][nch | 1]
     __shared__ int s_j[kMaxOutRows];
     const int R = P.rows;
     const int64_t g0 = (int64_t)blockIdx.x * R;
-    const int nch = P.ch.nch;
+    const int nch = P.ch.nch, SP = nch | 1;  // odd row pitch: a warp's column accesses hit distinct banks
     for (int gg = threadIdx.x; gg < R; gg += blockDim.x) s_j[gg] = g0 + gg < P.mtot ? P.iperm[g0 + gg] : 0;
     __syncthreads();
     for (int e = threadIdx.x; e < R * nch; e += blockDim.x) {
         const int gg = e / nch, c = e - gg * nch;
         const int64_t g = g0 + gg;
-        sm[e] = g < P.mtot ? P.src[(int64_t)s_j[gg] * nch + c] : make_float2(0.f, 0.f);
+        sm[gg * SP + c] = g < P.mtot ? P.src[(int64_t)s_j[gg] * nch + c] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     const int B = P.ch.B, L = P.ch.L, Kc = P.ch.K ? P.ch.K : 1;
@@ -331,14 +331,14 @@ __global__ void __launch_bounds__(256) out_il_kernel(const SampIL P) {
         if (g >= P.mtot) continue;
         float2 acc = make_float2(0.f, 0.f);
         if (L == 1 && !P.ch.K) {
-            acc = sm[gg * nch + b];
+            acc = sm[gg * SP + b];
         } else {
             const int f = P.sframe[s_j[gg]];
             const int t = P.tB ? (int)((g - P.frame_off[f]) % P.readout) : 0;
             for (int l = 0; l < L; ++l) {
                 float2 accl = make_float2(0.f, 0.f);
                 for (int k = 0; k < Kc; ++k) {
-                    float2 v = sm[gg * nch + (l * B + b) * Kc + k];
+                    float2 v = sm[gg * SP + (l * B + b) * Kc + k];
                     if (P.ch.K) v = cmul(v, P.basis[(int64_t)f * P.ch.K + k]);
                     accl.x += v.x;
                     accl.y += v.y;
@@ -1728,14 +1728,14 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             if (stage == PFB_STAGE_OUT) {
                 O.src = samp;
                 O.dst = static_cast<float2 *>(dst);
-                size_t smem = (size_t)O.rows * c.nch * sizeof(float2);
+                size_t smem = (size_t)O.rows * (c.nch | 1) * sizeof(float2);
                 PFB_RAISE_SMEM(out_il_kernel, (int)smem);
                 out_il_kernel<<<blocks, 256, smem, s>>>(O);
             } else {
                 O.src = static_cast<const float2 *>(src);
                 O.dst = samp;
                 O.factors = 1;
-                size_t smem = (size_t)O.rows * c.B * sizeof(float2);
+                size_t smem = (size_t)O.rows * (c.B | 1) * sizeof(float2);
                 PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
                 vals_il_kernel<<<blocks, 256, smem, s>>>(O);
             }
@@ -1854,7 +1854,7 @@ int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const flo
     V.dst = samp;
     V.factors = 0;
     V.rows = out_rows(std::max(c.nch, c.B));
-    size_t smem = (size_t)V.rows * c.B * sizeof(float2);
+    size_t smem = (size_t)V.rows * (c.B | 1) * sizeof(float2);
     PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
     vals_il_kernel<<<(unsigned)((p->mtot + V.rows - 1) / V.rows), 256, smem, s>>>(V);
     PFB_CHECK_LAUNCH();

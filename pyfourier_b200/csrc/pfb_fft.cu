@@ -198,9 +198,102 @@ __device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2
     }
 }
 
+// The stage plan of a transform length known at compile time: the same radix
+// order as make_axis (8, 10, 5, 4, 3, 7, 2, each as often as it divides), so
+// the twiddle table built on the host serves both forms.
+constexpr int kRadixOrder[7] = {8, 10, 5, 4, 3, 7, 2};
+struct StagePlan {
+    int nst = 0;
+    int radix[kFftMaxStages] = {};
+    int ns[kFftMaxStages] = {};
+    int twoff[kFftMaxStages] = {};
+};
+constexpr StagePlan stage_plan(int n) {
+    StagePlan p{};
+    int m = n, ns = 1, off = 0;
+    for (int k = 0; k < 7; ++k) {
+        const int r = kRadixOrder[k];
+        while (m % r == 0 && p.nst < kFftMaxStages) {
+            p.radix[p.nst] = r;
+            p.ns[p.nst] = ns;
+            p.twoff[p.nst] = off;
+            off += ns * (r - 1);
+            ++p.nst;
+            ns *= r;
+            m /= r;
+        }
+    }
+    return p;
+}
+
+// One Stockham stage with the radix, stage extent and butterfly count known at
+// compile time: the loop over butterflies unrolls, j = i mod ns and every
+// shared-memory index reduce to constants plus the thread's stream.
+template <int R, int NS, int M>
+__device__ __forceinline__ void fft_stage_c(const float2 *__restrict__ src, float2 *__restrict__ dst,
+                                            const float2 *__restrict__ tw, int stream, int cp) {
+    constexpr int IT = (M + kPairStreams - 1) / kPairStreams;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int i = stream + it * kPairStreams;
+        if (M % kPairStreams != 0 && i >= M) break;
+        const int j = NS == 1 ? 0 : i % NS;
+        float2 a[R], b[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const float4 v = *reinterpret_cast<const float4 *>(src + (i + q * M) * kPitch + 2 * cp);
+            a[q] = make_float2(v.x, v.y);
+            b[q] = make_float2(v.z, v.w);
+        }
+        if (NS > 1 && j != 0) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                const float2 w = __ldg(tw + j * (R - 1) + (q - 1));
+                a[q] = cmul(a[q], w);
+                b[q] = cmul(b[q], w);
+            }
+        }
+        dft<R>(a);
+        dft<R>(b);
+        const int base = (i - j) * R + j;
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+            *reinterpret_cast<float4 *>(dst + (base + k * NS) * kPitch + 2 * cp) =
+                make_float4(a[k].x, a[k].y, b[k].x, b[k].y);
+    }
+}
+
+template <int N, int S>
+__device__ __forceinline__ void fft_stages_c(float2 *&src, float2 *&dst, const float2 *tw, int stream, int cp) {
+    constexpr StagePlan P = stage_plan(N);
+    if constexpr (S < P.nst) {
+        constexpr int R = P.radix[S], NS = P.ns[S];
+        fft_stage_c<R, NS, N / R>(src, dst, tw + P.twoff[S], stream, cp);
+        __syncthreads();
+        float2 *t = src;
+        src = dst;
+        dst = t;
+        fft_stages_c<N, S + 1>(src, dst, tw, stream, cp);
+    }
+}
+
 // forward FFT of the 16 columns held in A (B is scratch); returns the buffer
-// holding the result.  Ends with the CTA synchronised.
+// holding the result.  Ends with the CTA synchronised.  The transform lengths of
+// the benchmark grids run a compile-time stage plan; other lengths the table-
+// driven loop below (same stages, same twiddles, same results).
 __device__ __forceinline__ const float2 *fft_run(float2 *A, float2 *B, const FftAxis &fa) {
+    {
+        float2 *src = A, *dst = B;
+        const int cp = threadIdx.x & (kCols / 2 - 1), stream = threadIdx.x / (kCols / 2);
+        switch (fa.n) {
+            case 250: fft_stages_c<250, 0>(src, dst, fa.tw, stream, cp); return src;
+            case 240: fft_stages_c<240, 0>(src, dst, fa.tw, stream, cp); return src;
+            case 160: fft_stages_c<160, 0>(src, dst, fa.tw, stream, cp); return src;
+            case 256: fft_stages_c<256, 0>(src, dst, fa.tw, stream, cp); return src;
+            case 512: fft_stages_c<512, 0>(src, dst, fa.tw, stream, cp); return src;
+            default: break;
+        }
+    }
     float2 *src = A, *dst = B;
     const int cp = threadIdx.x & (kCols / 2 - 1), stream = threadIdx.x / (kCols / 2);
     for (int s = 0; s < fa.nst; ++s) {
@@ -254,7 +347,7 @@ struct ColPass {
 // store loops; the host selects it when every base and stride is even in
 // elements (16-byte aligned pairs) and X is even.
 template <bool VEC>
-__global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
+__global__ void __launch_bounds__(kThreads, 3) col_pass_kernel(const ColPass P) {
     extern __shared__ float2 fsm[];
     const int n = P.fa.n;
     float2 *A = fsm, *Bf = fsm + n * kPitch, *Acc = fsm + 2 * n * kPitch;
@@ -300,7 +393,11 @@ __global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
             in_base = (int64_t)plane * P.in_plane + mid * P.in_mid;
         }
         // all copies of the column block in flight at once (C_l into the scratch
-        // buffer); positions without input are zero-filled
+        // buffer); positions without input are zero-filled.  Offsets along the
+        // axis stay in 32 bits (at most 512 x 512^2 elements within a plane).
+        const float2 *srcp = P.src + in_base + xs;
+        const float2 *clp = cl ? cl + xs : nullptr;
+        const int in_ax = (int)P.in_ax;
         for (int p = stream; p < n; p += NS) {
             int i = p;
             if (!P.inv) {
@@ -308,13 +405,13 @@ __global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
                 if (i >= n) i -= n;
             }
             const bool valid = i < P.lin;
-            const int64_t off = (int64_t)(valid ? i : 0) * P.in_ax + xs;
+            const int off = (valid ? i : 0) * in_ax;
             if (VEC) {
-                cp_async16(A + p * kPitch + col, P.src + in_base + off, valid);
-                if (cl) cp_async16(Bf + p * kPitch + col, cl + off, valid);
+                cp_async16(A + p * kPitch + col, srcp + off, valid);
+                if (clp) cp_async16(Bf + p * kPitch + col, clp + off, valid);
             } else {
-                cp_async8(A + p * kPitch + col, P.src + in_base + off, valid);
-                if (cl) cp_async8(Bf + p * kPitch + col, cl + off, valid);
+                cp_async8(A + p * kPitch + col, srcp + off, valid);
+                if (clp) cp_async8(Bf + p * kPitch + col, clp + off, valid);
             }
         }
         cp_async_commit();
@@ -386,14 +483,15 @@ __global__ void __launch_bounds__(kThreads) col_pass_kernel(const ColPass P) {
             }
             if (l + 1 < nl) __syncthreads();  // the next segment reloads A
         } else {
-            const int64_t out_base = (int64_t)plane * P.out_plane + mid * P.out_mid;
+            float2 *dstp = P.dst + (int64_t)plane * P.out_plane + mid * P.out_mid + x;
+            const int out_ax = (int)P.out_ax;
             for (int o = stream; o < P.lout; o += NS) {
                 int pp = o;
                 if (P.inv) {
                     pp = o - hn;
                     if (pp < 0) pp += n;
                 }
-                float2 *d = P.dst + out_base + (int64_t)o * P.out_ax + x;
+                float2 *d = dstp + o * out_ax;
                 if (VEC) {
                     float4 r = *reinterpret_cast<const float4 *>(R + pp * kPitch + col);
                     if (P.inv) {
