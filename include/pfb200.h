@@ -87,6 +87,7 @@ typedef struct {
     double scale;        /* sum of node-centred kernel samples */
     int32_t n_items;     /* spread work items (per-frame binning) */
     int32_t max_bin;     /* largest number of samples starting in one tile */
+    int32_t tile_offset[3]; /* tile t of an axis covers [t*tile - off, (t+1)*tile - off) */
 } pfb_plan_info_t;
 
 const char *pfb_last_error(void);

@@ -71,6 +71,7 @@ class PlanInfoT(ctypes.Structure):
         ("scale", ctypes.c_double),
         ("n_items", ctypes.c_int32),
         ("max_bin", ctypes.c_int32),
+        ("tile_offset", ctypes.c_int32 * 3),
     ]
 
 

@@ -131,6 +131,8 @@ class Interpolator:
         self.n_items = int(info.n_items)
         self.max_bin = int(info.max_bin)
         self.tile = tuple(int(info.tile[i]) for i in range(nd))
+        # tile t of an axis covers [t * tile - offset, (t + 1) * tile - offset) of the grid
+        self.tile_offset = tuple(int(info.tile_offset[i]) for i in range(nd))
 
     @property
     def handle(self):

@@ -201,6 +201,7 @@ int pfb_plan_info(const pfb_plan *p, pfb_plan_info_t *info) {
         info->os_shape[z] = used ? p->g.nos[a] : 1;
         info->width[z] = used ? p->g.w[a] : 1;
         info->tile[z] = used ? p->g.tile[a] : 1;
+        info->tile_offset[z] = used ? p->g.toff[a] : 0;
     }
     info->scale = p->scale;
     info->n_items = p->n_items_frame;

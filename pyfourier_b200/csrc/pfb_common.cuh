@@ -64,11 +64,24 @@ struct Geom {
     int cart[kMaxDim];   // 1 if the axis is Cartesian (integer positions, width 1)
     float beta[kMaxDim]; // Kaiser-Bessel beta
     int tile[kMaxDim];   // bin / tile extent for the spread
-    int nbins[kMaxDim];  // ceil(nos / tile)
+    int toff[kMaxDim];   // tile offset: tile t covers [t * tile - toff, (t + 1) * tile - toff) clipped to the grid
+    int nbins[kMaxDim];  // ceil((nos + toff) / tile)
     int sh[kMaxDim];     // index shift folding fftshift into the grid layout (nos / 2)
     int64_t gvol;        // prod(nos)
     int64_t nvol;        // prod(n)
 };
+
+// First grid index and extent of tile tc along axis a.  Tiles start at
+// tc * tile - toff, so when toff > 0 the first tile is toff points narrower and
+// the remainder of the grid extent goes to the last tile.
+__host__ __device__ __forceinline__ int tile_org(const Geom &g, int a, int tc) {
+    const int o = tc * g.tile[a] - g.toff[a];
+    return o > 0 ? o : 0;
+}
+__host__ __device__ __forceinline__ int tile_extent(const Geom &g, int a, int tc) {
+    const int e = (tc + 1) * g.tile[a] - g.toff[a];
+    return (e < g.nos[a] ? e : g.nos[a]) - tile_org(g, a, tc);
+}
 
 // Work item of the spread: a contiguous run of bin-sorted samples that all
 // start (x0) inside one tile.  frame < 0 means samples of several frames.

@@ -794,8 +794,8 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
     for (int a = 0; a < 3; ++a) {
         if (a < D) {
             int tc = tile_coord(it.tile, a, P.g);
-            org[a] = tc * P.g.tile[a];
-            text[a] = min(P.g.tile[a], P.g.nos[a] - org[a]);
+            org[a] = tile_org(P.g, a, tc);
+            text[a] = tile_extent(P.g, a, tc);
             wrap[a] = P.g.nbins[a] == 1 ? text[a] : 0;
         } else {
             org[a] = 0;
@@ -1034,8 +1034,8 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const int tc = tile_coord(it.tile, a, P.g);
-        org[a] = tc * P.g.tile[a];
-        text[a] = min(P.g.tile[a], P.g.nos[a] - org[a]);
+        org[a] = tile_org(P.g, a, tc);
+        text[a] = tile_extent(P.g, a, tc);
         wrap[a] = P.g.nbins[a] == 1 ? text[a] : 0;
     }
     for (int pt = threadIdx.x; pt < kRegPts; pt += blockDim.x) {
@@ -1243,8 +1243,8 @@ __global__ void __launch_bounds__(Reg2Cfg<CPW>::NW * 32, Reg2Cfg<CPW>::MinBlocks
 #pragma unroll
     for (int a = 0; a < 2; ++a) {
         const int tc = tile_coord(it.tile, a, P.g);
-        org[a] = tc * P.g.tile[a];
-        text[a] = min(P.g.tile[a], P.g.nos[a] - org[a]);
+        org[a] = tile_org(P.g, a, tc);
+        text[a] = tile_extent(P.g, a, tc);
         wrap[a] = P.g.nbins[a] == 1 ? text[a] : 0;
     }
     for (int pt = threadIdx.x; pt < kReg2Pts; pt += blockDim.x) {
@@ -1387,8 +1387,8 @@ __global__ void zero_tiles_kernel(Geom g, const OwnerItem *zero, int nch, float2
         if (a < D) {
             int tc = a == 0 ? it.tile % g.nbins[0]
                             : (a == 1 ? (it.tile / g.nbins[0]) % g.nbins[1] : it.tile / (g.nbins[0] * g.nbins[1]));
-            org[a] = tc * g.tile[a];
-            text[a] = min(g.tile[a], g.nos[a] - org[a]);
+            org[a] = tile_org(g, a, tc);
+            text[a] = tile_extent(g, a, tc);
         } else {
             org[a] = 0;
             text[a] = 1;

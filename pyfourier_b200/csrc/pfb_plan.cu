@@ -27,6 +27,7 @@ struct ScaleParams {
     int w[kMaxDim];
     int cart[kMaxDim];
     int tile[kMaxDim];
+    int toff[kMaxDim];
     int nbins[kMaxDim];
 };
 
@@ -55,12 +56,13 @@ __global__ void scale_and_key_kernel(ScaleParams P, const float *__restrict__ co
         }
         long long x0 = start_index(cos_, P.w[a], P.cart[a]);
         int x0m = pmod(x0, P.nos[a]);
-        const int tb = x0m / P.tile[a];
+        // tile tb covers [tb * tile - toff, (tb + 1) * tile - toff) clipped to the grid
+        const int tb = (x0m + P.toff[a]) / P.tile[a];
         bin += tb * stride;
         stride *= P.nbins[a];
-        const int local = x0m - tb * P.tile[a];
-        const int text = min(P.tile[a], P.nos[a] - tb * P.tile[a]);
-        if (P.nbins[a] > 1 && local + P.w[a] - 1 >= text) code |= 1 << a;
+        const int org = max(tb * P.tile[a] - P.toff[a], 0);
+        const int text = min((tb + 1) * P.tile[a] - P.toff[a], P.nos[a]) - org;
+        if (P.nbins[a] > 1 && x0m - org + P.w[a] - 1 >= text) code |= 1 << a;
     }
     // sort key: (tile, edge code) major, frame minor
     keys[g] = ((bin << P.ndim) | code) * P.nframes + lo;
@@ -126,16 +128,38 @@ double kb_host(double x, double beta) {
             ti * (-0.01647633 + ti * 0.00392377))))))));
 }
 
-// A tile must be at least W - 1 wide, and so must the last (partial) tile, so
-// that a kernel footprint spans at most two consecutive tiles per axis (the
-// owner-computes spread gathers from the tile and its lower neighbour only).
-int fit_tile(int t, int w, int nos) {
+// Every tile must be at least W - 1 wide, the first and the last (partial) one
+// included, so that a kernel footprint spans at most two consecutive tiles per
+// axis (the owner-computes spread gathers from the tile and its lower neighbour
+// only).  When the grid extent leaves a last tile narrower than that, the tiles
+// are shifted by an offset toff (tile t starts at t * tile - toff) that moves
+// part of the remainder into a narrower first tile, so the requested extent is
+// kept: 250 = 7 + 30 x 8 + 3 for tile 8, W 4 (toff 1).  Only when no offset
+// works does the extent change (the nearest one that fits, smaller first).
+int fit_tile(int t, int w, int nos, int *toff) {
     t = std::max(1, std::min(t, nos));
-    if (w <= 1) return t;
-    auto ok = [&](int tt) { int r = nos % tt; return tt >= w - 1 && (r == 0 || r >= w - 1); };
+    *toff = 0;
+    if (w <= 1 || nos <= t) return t;
+    // smallest offset o for which extent tt fits, -1 if none
+    auto fit = [&](int tt) {
+        if (tt < w - 1) return -1;
+        if (nos <= tt) return 0;  // one tile: the footprints wrap inside it
+        for (int o = 0; o < tt && tt - o >= w - 1; ++o) {
+            const int r = (nos + o) % tt;  // width of the last tile (0: full)
+            if (r == 0 || r >= w - 1) return o;
+        }
+        return -1;
+    };
     for (int d = 0; d < nos; ++d) {
-        if (t - d >= 1 && ok(t - d)) return t - d;
-        if (t + d <= nos && ok(t + d)) return t + d;
+        int o;
+        if (t - d >= 1 && (o = fit(t - d)) >= 0) {
+            *toff = o;
+            return t - d;
+        }
+        if (t + d <= nos && (o = fit(t + d)) >= 0) {
+            *toff = o;
+            return t + d;
+        }
     }
     return nos;
 }
@@ -260,9 +284,11 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
             g.cart[a] = (is_cart && is_cart[z] != 0) || width[z] == 1;
             g.w[a] = g.cart[a] ? 1 : width[z];
             g.beta[a] = beta[z];
-            g.tile[a] = fit_tile(tile && tile[z] > 0 ? tile[z] : default_tile(ndim, g.nos[a]), g.w[a], g.nos[a]);
+            g.tile[a] = fit_tile(tile && tile[z] > 0 ? tile[z] : default_tile(ndim, g.nos[a]), g.w[a], g.nos[a],
+                                 &g.toff[a]);
         } else {
             g.n[a] = g.nos[a] = g.w[a] = g.tile[a] = 1;
+            g.toff[a] = 0;
             g.cart[a] = 1;
             g.beta[a] = 0.f;
         }
@@ -278,7 +304,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
             delete p;
             return fail(PFB_ERR_INVALID, "kernel width larger than the oversampled grid");
         }
-        g.nbins[a] = (g.nos[a] + g.tile[a] - 1) / g.tile[a];
+        g.nbins[a] = (g.nos[a] + g.toff[a] + g.tile[a] - 1) / g.tile[a];
         g.sh[a] = g.nos[a] / 2;
         g.gvol *= g.nos[a];
         g.nvol *= g.n[a];
@@ -355,6 +381,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
         sp.w[a] = g.w[a];
         sp.cart[a] = g.cart[a];
         sp.tile[a] = g.tile[a];
+        sp.toff[a] = g.toff[a];
         sp.nbins[a] = g.nbins[a];
     }
     if (mtot > 0) {

@@ -59,9 +59,9 @@ __global__ void __launch_bounds__(256) spread_kernel(const SpreadParams P) {
     int org[kMaxDim] = {0, 0, 0};
     {
         int b = it.bin;
-        org[0] = (b % P.g.nbins[0]) * P.g.tile[0];
-        if (D > 1) { b /= P.g.nbins[0]; org[1] = (b % P.g.nbins[1]) * P.g.tile[1]; }
-        if (D > 2) { b /= P.g.nbins[1]; org[2] = b * P.g.tile[2]; }
+        org[0] = tile_org(P.g, 0, b % P.g.nbins[0]);
+        if (D > 1) { b /= P.g.nbins[0]; org[1] = tile_org(P.g, 1, b % P.g.nbins[1]); }
+        if (D > 2) { b /= P.g.nbins[1]; org[2] = tile_org(P.g, 2, b); }
     }
     __syncthreads();
 

@@ -52,12 +52,35 @@ def test_status_mapping_without_gpu():
     assert L.pfb_plan_info(None, ctypes.byref(info)) == _lib.PFB_ERR_INVALID
 
 
-def test_apply_struct_layout_matches_header():
+def test_apply_struct_layout_matches_header(tmp_path):
+    """The ctypes mirrors have the size and field offsets the C compiler gives the
+    header's structs."""
+    import shutil
+
     from pyfourier_b200 import _lib
 
     # int64 + 2*int32 + 4 pointers + 2*int32 = 8 + 8 + 32 + 8 = 56 bytes on LP64
     assert ctypes.sizeof(_lib.ApplyT) == 56
-    assert ctypes.sizeof(_lib.PlanInfoT) == 4 + 4 + 8 + 4 * 12 + 8 + 4 + 4
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lines = []
+    for cname, mirror in (("pfb_apply_t", _lib.ApplyT), ("pfb_plan_info_t", _lib.PlanInfoT)):
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in mirror._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "pfb200.h"\nint main(void) {\n'
+                   + "\n".join(lines) + "\nreturn 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, mirror in (("pfb_apply_t", _lib.ApplyT), ("pfb_plan_info_t", _lib.PlanInfoT)):
+        assert got[(cname, "size")] == ctypes.sizeof(mirror), cname
+        for f, _ in mirror._fields_:
+            assert got[(cname, f)] == getattr(mirror, f).offset, (cname, f)
 
 
 def test_host_parameter_math_matches_oracle():

@@ -2,8 +2,9 @@
 oracle finishes in seconds, with the benchmark's own trajectory generators.
 
 * 3D golden-means radial (osf 1.25, W 4, 32 coils): the 32-channel register-tile
-  spread and the 32-channel interp, on 8^3 tiles and on 7^3 tiles with a partial
-  last tile (the tile fit of the 250^3 grid);
+  spread and the 32-channel interp, on 8^3 tiles of an 80^3 grid and on 8^3 tiles
+  of a 90^3 grid shifted by one point (first tile 7, last tile 3 wide: the tile
+  fit of the 250^3 benchmark grid, 7 + 30 x 8 + 3);
 * Toeplitz Gram with a K = 4 exponential-recovery subspace over 48 rotated
   variable-density spiral frames, 16 coils;
 * B0 time-segmented (L = 8) dynamic radial with 12 coils and frames of uneven
@@ -41,15 +42,16 @@ def rel(a, b):
     return orc.rel_l2(a, b)
 
 
-@pytest.mark.parametrize("N, nspokes, nread, tile", [(64, 2000, 128, 8), (72, 1500, 144, 7)])
-def test_3d_golden_means_radial_32_coils(N, nspokes, nread, tile):
+@pytest.mark.parametrize("N, nspokes, nread, offset", [(64, 2000, 128, 0), (72, 1500, 144, 1)])
+def test_3d_golden_means_radial_32_coils(N, nspokes, nread, offset):
     P = pf()
     rng = np.random.default_rng(N)
     coord = bench.golden_means_radial_3d(nspokes, nread, N)
     B = 32
     oplan = orc.plan_nufft(coord, (N, N, N), width=4, oversamp=1.25)
     gplan = P.plan_nufft(torch.as_tensor(coord), (N, N, N), width=4, oversamp=1.25, device="cuda:0")
-    assert gplan.interpolator.tile == (tile, tile, tile)
+    assert gplan.interpolator.tile == (8, 8, 8)
+    assert gplan.interpolator.tile_offset == (offset,) * 3
     ph = bench.phantom_3d(torch, N, 20, "cuda:0", seed=1)
     x = (bench.coil_maps_3d(torch, N, B, "cuda:0") * ph[None]).contiguous()
     yg = P.nufft(x, nufft_plan=gplan)

@@ -250,8 +250,10 @@ def _sorted_order(plan):
 
 
 def _bin_keys(plan, op, frame, ndim, w=4):
-    """Bin keys ((tile << d | edge code) * F + frame) from the oracle's first taps."""
+    """Bin keys ((tile << d | edge code) * F + frame) from the oracle's first taps;
+    tile t of an axis covers [t * tile - offset, (t + 1) * tile - offset) of the grid."""
     tile = plan.interpolator.tile[::-1]  # (x, y, z)
+    off = plan.interpolator.tile_offset[::-1]
     nos = op.os_shape[::-1]
     M = frame.size
     key_bin = np.zeros(M, np.int64)
@@ -259,13 +261,14 @@ def _bin_keys(plan, op, frame, ndim, w=4):
     stride = 1
     for a in range(ndim):
         x0m = op.index[ndim - 1 - a].reshape(-1, op.index[ndim - 1 - a].shape[-1])[:, 0].astype(np.int64)
-        nb = -(-nos[a] // tile[a])
-        tb = x0m // tile[a]
+        nb = -(-(nos[a] + off[a]) // tile[a])
+        tb = (x0m + off[a]) // tile[a]
         key_bin += tb * stride
         stride *= nb
-        text = np.minimum(tile[a], nos[a] - tb * tile[a])
+        org = np.maximum(tb * tile[a] - off[a], 0)
+        text = np.minimum((tb + 1) * tile[a] - off[a], nos[a]) - org
         if nb > 1:
-            code |= ((x0m - tb * tile[a] + w - 1 >= text).astype(np.int64) << a)
+            code |= ((x0m - org + w - 1 >= text).astype(np.int64) << a)
     return ((key_bin << ndim) | code) * plan.interpolator.nframes + frame
 
 
@@ -312,22 +315,9 @@ def test_counting_sort_is_stable_by_bin_key(ndim):
     # keys from the first taps of the oracle's tables (x-first axes)
     coord = np.concatenate(frames)
     op = orc.plan_nufft(coord[None], N, width=4, oversamp=1.25)
-    tile = plan.interpolator.tile[::-1]  # (x, y, z)
-    nos = op.os_shape[::-1]
-    frame = np.repeat(np.arange(F), lens)
-    key_bin = np.zeros(M, np.int64)
-    code = np.zeros(M, np.int64)
-    stride = 1
-    for a in range(ndim):
-        x0m = op.index[ndim - 1 - a][0, :, 0].astype(np.int64)
-        nb = -(-nos[a] // tile[a])
-        tb = x0m // tile[a]
-        key_bin += tb * stride
-        stride *= nb
-        text = np.minimum(tile[a], nos[a] - tb * tile[a])
-        if nb > 1:
-            code |= ((x0m - tb * tile[a] + 3 >= text).astype(np.int64) << a)
-    key = ((key_bin << ndim) | code) * F + frame
+    # a 50-point grid axis: tiles shifted by one point (first tile one narrower, last 3 wide)
+    assert plan.interpolator.tile_offset == (1,) * ndim
+    key = _bin_keys(plan, op, np.repeat(np.arange(F), lens), ndim)
     ks = key[order]
     assert np.all(np.diff(ks) >= 0)
     same = np.diff(ks) == 0
