@@ -39,6 +39,7 @@ extern "C" {
 #define PFB_ERR_NOMEM 4       /* device allocation failed */
 #define PFB_ERR_UNSUPPORTED 5 /* valid request this build does not implement */
 #define PFB_ERR_WORKSPACE 6   /* workspace too small */
+#define PFB_ERR_DEVICE 7      /* a kernel's bounded wait gave up; see pfb_plan_check */
 
 #define PFB_NORM_NONE 0  /* forward unscaled, adjoint scaled by 1/prod(os_shape) */
 #define PFB_NORM_ORTHO 1 /* both scaled by 1/sqrt(prod(os_shape)) */
@@ -136,6 +137,12 @@ int pfb_plan_tables(const pfb_plan *plan, int axis, int32_t *index, float *value
  * reference has no sorted order (its kernels walk the samples as given,
  * src/pyfourier/_subroutines/_grid/_noncart2cart/_3D.py:29-50). */
 int pfb_plan_order(const pfb_plan *plan, int32_t *order, void *stream);
+
+/* Device-side status of the plan's applies: PFB_ERR_DEVICE if a kernel gave up
+ * a bounded wait since the last check (its results are invalid; the flag is
+ * cleared), else PFB_OK.  Synchronises `stream`.  The reference has no
+ * counterpart (its kernels never wait on asynchronous copies). */
+int pfb_plan_check(pfb_plan *plan, void *stream);
 
 /* Workspace bytes for an apply over `nplanes` oversampled grid planes
  * (nplanes = nseg * batch * ncoeff).  May create the cuFFT plan. */

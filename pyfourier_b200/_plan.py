@@ -148,6 +148,13 @@ class Interpolator:
             self._build()
         return self
 
+    def check(self):
+        """Raise RuntimeError if a kernel of this plan's applies gave up a bounded
+        wait since the last check (those results are invalid).  Synchronises the
+        device's current stream."""
+        s = torch.cuda.current_stream(self.device)
+        _lib.check(_lib.load().pfb_plan_check(self._handle, ctypes.c_void_p(s.cuda_stream)))
+
     def retile(self, tile):
         """Rebuild the device plan with another tile extent ((z, y, x) order)."""
         tile = tuple(int(t) for t in tile)

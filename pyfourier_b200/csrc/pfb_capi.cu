@@ -246,6 +246,22 @@ int pfb_plan_order(const pfb_plan *p, int32_t *order, void *stream) {
     return PFB_OK;
 }
 
+int pfb_plan_check(pfb_plan *p, void *stream) {
+    if (!p) return fail(PFB_ERR_INVALID, "NULL plan");
+    if (!p->d_fft_err) return PFB_OK;
+    DeviceGuard dg(p->device);
+    int v = 0;
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    PFB_CUDA_TRY(cudaMemcpyAsync(&v, p->d_fft_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PFB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (v) {
+        PFB_CUDA_TRY(cudaMemsetAsync(p->d_fft_err, 0, sizeof(int), s));
+        return fail(PFB_ERR_DEVICE, "a fused-FFT pass gave up waiting for its tile loads: "
+                                    "results since the last check are invalid");
+    }
+    return PFB_OK;
+}
+
 int pfb_workspace_size(pfb_plan *p, int64_t nplanes, size_t *bytes) {
     if (!p || !bytes || nplanes < 1) return fail(PFB_ERR_INVALID, "bad argument");
     DeviceGuard dg(p->device);

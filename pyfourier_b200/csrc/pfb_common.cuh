@@ -180,6 +180,8 @@ struct pfb_plan {
     int fft_fused = -1;          // -1 not decided, 0 not applicable, 1 ready
     pfb::FftAxis fft_ax[pfb::kMaxDim];
     float2 *d_fft_tw = nullptr;  // twiddles of all axes and stages
+    int *d_fft_err = nullptr;    // set by a fused-FFT kernel whose bounded wait gave up
+    int fft_nsm = 0;             // SMs of the plan's device (persistent grids)
 };
 
 namespace pfb {

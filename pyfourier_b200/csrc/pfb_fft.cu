@@ -28,6 +28,9 @@
 // butterflies run over them.  The inverse transform conjugates on load and store.
 // Twiddles are computed in double precision on the host.
 
+#include <cuda.h>
+
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -167,9 +170,9 @@ __device__ __forceinline__ void dft<10>(float2 *a) {
     }
 }
 
-// One Stockham stage over the CTA's 16 columns; a thread takes two adjacent
-// columns (one float4) of each of its butterflies.
-template <int R>
+// One Stockham stage over the CTA's 16 columns (rows PITCH float2 apart); a
+// thread takes two adjacent columns (one float4) of each of its butterflies.
+template <int R, int PITCH>
 __device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2 *__restrict__ dst, int m, int ns,
                                           unsigned magic, const float2 *__restrict__ tw, int stream, int cp) {
     for (int i = stream; i < m; i += kPairStreams) {
@@ -177,7 +180,7 @@ __device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2
         float2 a[R], b[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) {
-            const float4 v = *reinterpret_cast<const float4 *>(src + (i + q * m) * kPitch + 2 * cp);
+            const float4 v = *reinterpret_cast<const float4 *>(src + (i + q * m) * PITCH + 2 * cp);
             a[q] = make_float2(v.x, v.y);
             b[q] = make_float2(v.z, v.w);
         }
@@ -194,7 +197,7 @@ __device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2
         const int base = (i - j) * R + j;
 #pragma unroll
         for (int k = 0; k < R; ++k)
-            *reinterpret_cast<float4 *>(dst + (base + k * ns) * kPitch + 2 * cp) = make_float4(a[k].x, a[k].y, b[k].x, b[k].y);
+            *reinterpret_cast<float4 *>(dst + (base + k * ns) * PITCH + 2 * cp) = make_float4(a[k].x, a[k].y, b[k].x, b[k].y);
     }
 }
 
@@ -229,7 +232,7 @@ constexpr StagePlan stage_plan(int n) {
 // One Stockham stage with the radix, stage extent and butterfly count known at
 // compile time: the loop over butterflies unrolls, j = i mod ns and every
 // shared-memory index reduce to constants plus the thread's stream.
-template <int R, int NS, int M>
+template <int R, int NS, int M, int PITCH>
 __device__ __forceinline__ void fft_stage_c(const float2 *__restrict__ src, float2 *__restrict__ dst,
                                             const float2 *__restrict__ tw, int stream, int cp) {
     constexpr int IT = (M + kPairStreams - 1) / kPairStreams;
@@ -241,7 +244,7 @@ __device__ __forceinline__ void fft_stage_c(const float2 *__restrict__ src, floa
         float2 a[R], b[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) {
-            const float4 v = *reinterpret_cast<const float4 *>(src + (i + q * M) * kPitch + 2 * cp);
+            const float4 v = *reinterpret_cast<const float4 *>(src + (i + q * M) * PITCH + 2 * cp);
             a[q] = make_float2(v.x, v.y);
             b[q] = make_float2(v.z, v.w);
         }
@@ -258,39 +261,41 @@ __device__ __forceinline__ void fft_stage_c(const float2 *__restrict__ src, floa
         const int base = (i - j) * R + j;
 #pragma unroll
         for (int k = 0; k < R; ++k)
-            *reinterpret_cast<float4 *>(dst + (base + k * NS) * kPitch + 2 * cp) =
+            *reinterpret_cast<float4 *>(dst + (base + k * NS) * PITCH + 2 * cp) =
                 make_float4(a[k].x, a[k].y, b[k].x, b[k].y);
     }
 }
 
-template <int N, int S>
+template <int N, int S, int PITCH>
 __device__ __forceinline__ void fft_stages_c(float2 *&src, float2 *&dst, const float2 *tw, int stream, int cp) {
     constexpr StagePlan P = stage_plan(N);
     if constexpr (S < P.nst) {
         constexpr int R = P.radix[S], NS = P.ns[S];
-        fft_stage_c<R, NS, N / R>(src, dst, tw + P.twoff[S], stream, cp);
+        fft_stage_c<R, NS, N / R, PITCH>(src, dst, tw + P.twoff[S], stream, cp);
         __syncthreads();
         float2 *t = src;
         src = dst;
         dst = t;
-        fft_stages_c<N, S + 1>(src, dst, tw, stream, cp);
+        fft_stages_c<N, S + 1, PITCH>(src, dst, tw, stream, cp);
     }
 }
 
-// forward FFT of the 16 columns held in A (B is scratch); returns the buffer
-// holding the result.  Ends with the CTA synchronised.  The transform lengths of
-// the benchmark grids run a compile-time stage plan; other lengths the table-
-// driven loop below (same stages, same twiddles, same results).
-__device__ __forceinline__ const float2 *fft_run(float2 *A, float2 *B, const FftAxis &fa) {
+// forward FFT of the 16 columns held in A (B is scratch; rows PITCH float2
+// apart); returns the buffer holding the result.  Ends with the CTA
+// synchronised.  The transform lengths of the benchmark grids run a compile-time
+// stage plan; other lengths the table-driven loop below (same stages, same
+// twiddles, same results).
+template <int PITCH = kPitch>
+__device__ __forceinline__ float2 *fft_run(float2 *A, float2 *B, const FftAxis &fa) {
     {
         float2 *src = A, *dst = B;
         const int cp = threadIdx.x & (kCols / 2 - 1), stream = threadIdx.x / (kCols / 2);
         switch (fa.n) {
-            case 250: fft_stages_c<250, 0>(src, dst, fa.tw, stream, cp); return src;
-            case 240: fft_stages_c<240, 0>(src, dst, fa.tw, stream, cp); return src;
-            case 160: fft_stages_c<160, 0>(src, dst, fa.tw, stream, cp); return src;
-            case 256: fft_stages_c<256, 0>(src, dst, fa.tw, stream, cp); return src;
-            case 512: fft_stages_c<512, 0>(src, dst, fa.tw, stream, cp); return src;
+            case 250: fft_stages_c<250, 0, PITCH>(src, dst, fa.tw, stream, cp); return src;
+            case 240: fft_stages_c<240, 0, PITCH>(src, dst, fa.tw, stream, cp); return src;
+            case 160: fft_stages_c<160, 0, PITCH>(src, dst, fa.tw, stream, cp); return src;
+            case 256: fft_stages_c<256, 0, PITCH>(src, dst, fa.tw, stream, cp); return src;
+            case 512: fft_stages_c<512, 0, PITCH>(src, dst, fa.tw, stream, cp); return src;
             default: break;
         }
     }
@@ -301,13 +306,13 @@ __device__ __forceinline__ const float2 *fft_run(float2 *A, float2 *B, const Fft
         const unsigned mg = fa.magic[s];
         const float2 *tw = fa.tw + fa.twoff[s];
         switch (r) {
-            case 2: fft_stage<2>(src, dst, m, ns, mg, tw, stream, cp); break;
-            case 3: fft_stage<3>(src, dst, m, ns, mg, tw, stream, cp); break;
-            case 4: fft_stage<4>(src, dst, m, ns, mg, tw, stream, cp); break;
-            case 5: fft_stage<5>(src, dst, m, ns, mg, tw, stream, cp); break;
-            case 7: fft_stage<7>(src, dst, m, ns, mg, tw, stream, cp); break;
-            case 10: fft_stage<10>(src, dst, m, ns, mg, tw, stream, cp); break;
-            default: fft_stage<8>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 2: fft_stage<2, PITCH>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 3: fft_stage<3, PITCH>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 4: fft_stage<4, PITCH>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 5: fft_stage<5, PITCH>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 7: fft_stage<7, PITCH>(src, dst, m, ns, mg, tw, stream, cp); break;
+            case 10: fft_stage<10, PITCH>(src, dst, m, ns, mg, tw, stream, cp); break;
+            default: fft_stage<8, PITCH>(src, dst, m, ns, mg, tw, stream, cp); break;
         }
         __syncthreads();
         float2 *t = src;
@@ -341,6 +346,8 @@ struct ColPass {
     const float2 *Cl;
     float factor;
     int accumulate;
+    int *err;   // device flag of the plan (TMA form: a wait that gave up)
+    int nsm;    // SMs of the device (TMA form: persistent grid)
 };
 
 // VEC: a thread moves two adjacent columns (16 bytes) in the copy, finish and
@@ -509,6 +516,240 @@ __global__ void __launch_bounds__(kThreads, 3) col_pass_kernel(const ColPass P) 
     }
 }
 
+// ------------------------------------------------------------------------------------
+// Column pass on the tensor memory accelerator: a persistent CTA walks column
+// tiles (16 adjacent x positions x the whole axis, one (mid, plane)), each loaded
+// by TMA into one slot of a two-slot ring while the previous tile transforms.
+// Rows are dense in shared memory (16 float2 = 128 bytes, the box layout), so
+// forward passes also leave by TMA store.  Inverse passes run the forward
+// transform and read its output reversed, IDFT(x)[k] = DFT(x)[(n - k) mod n],
+// which needs no conjugation of the input or output.
+// ------------------------------------------------------------------------------------
+constexpr int kTmaPitch = kCols;        // float2 per shared row: one 128-byte TMA box row
+constexpr int kTmaMaxBoxes = 8;         // load boxes per tile
+constexpr int kWaitLimit = 1 << 20;     // mbarrier polls before a wait gives up
+
+struct ColTma {
+    FftAxis fa;
+    int inv, mode;          // as ColPass: 0 buffer -> buffer, 1 image -> buffer, 2 buffer -> image
+    int lin, lout, hn;      // rows read / written; hn: rotation of the fftshift (nax / 2)
+    int X, nxc, nmid, nplanes;
+    int64_t ntiles;
+    int nbox;               // load boxes per tile: smem row, source row (before the +hn rotation fold)
+    int box_smem[kTmaMaxBoxes], box_src[kTmaMaxBoxes];
+    int br;                 // rows per load box
+    int nsbox, sbr;         // forward stores: boxes and rows per box (overlapping last box)
+    int64_t out_plane, out_mid, out_ax;  // plain stores (inverse passes)
+    float2 *dst;
+    Chan ch;
+    int C;
+    int64_t nvol;
+    const float *apod_ax, *apod_mid, *apod_x;
+    float factor;
+    int accumulate;
+    int *err;               // set to 1 when a wait gives up (the results are then invalid)
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// bounded wait for the phase with the given parity to complete
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    const unsigned a = smem_u32(bar);
+    for (int it = 0; it < kWaitLimit; ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// 4D tiled TMA load into this CTA's shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                          uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+// 4D tiled TMA store from shared memory (bulk-group completion)
+__device__ __forceinline__ void tma_store4(const CUtensorMap *map, int c0, int c1, int c2, int c3, const void *src) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(map),
+                 "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+struct TileInfo {
+    int xc, mid, plane;
+};
+
+// src_map: the pass's source as 4D (2X floats, rows, mid, source plane); dst_map:
+// the destination of forward passes (2X floats, n rows, mid, plane).
+__global__ void __launch_bounds__(kThreads, 2)
+    col_tma_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
+                   const ColTma P) {
+    extern __shared__ __align__(128) float2 tsm[];
+    __shared__ __align__(8) uint64_t full[2];
+    __shared__ TileInfo info[2];
+    const int n = P.fa.n;
+    // slot s of the ring at tsm + s * n rows, the transform's scratch buffer after them
+    float2 *scr = tsm + 2 * n * kTmaPitch;
+    const int col = (threadIdx.x % (kCols / 2)) * 2, stream = threadIdx.x / (kCols / 2);
+    constexpr int NS = kThreads * 2 / kCols;  // row streams: a thread moves two adjacent columns
+    const unsigned box_bytes = (unsigned)P.br * kTmaPitch * sizeof(float2);
+    const bool fwd_store = P.mode != 2 && !P.inv;
+    // thread 0: load tile t into slot s (tile coordinates go with it through shared memory)
+    auto issue = [&](int64_t t, int s) {
+        const int xc = (int)(t % P.nxc);
+        const int64_t r = t / P.nxc;
+        const int mid = (int)(r % P.nmid), plane = (int)(r / P.nmid);
+        int sp = plane;  // source plane
+        if (P.mode == 1) {  // grid plane (grp, ch) <- image plane (b, c)
+            const int Kc = P.ch.K ? P.ch.K : 1;
+            const int grp = plane / P.ch.nch, chn = plane - grp * P.ch.nch;
+            const int k = chn % Kc, b = (chn / Kc) % P.ch.B;
+            sp = b * P.C + (P.ch.K ? k : grp);
+        } else if (P.mode == 2) {  // image plane (b, c) <- grid plane (grp, chn) of the only segment
+            const int b = plane / P.C, c = plane - b * P.C;
+            const int Kc = P.ch.K ? P.ch.K : 1;
+            sp = (P.ch.K ? 0 : c) * P.ch.nch + (P.ch.K ? b * Kc + c : b);
+        }
+        info[s] = TileInfo{xc, mid, plane};
+        mbar_expect_tx(&full[s], box_bytes * P.nbox);
+        for (int b = 0; b < P.nbox; ++b)
+            tma_load4(tsm + (s * n + P.box_smem[b]) * kTmaPitch, &src_map, xc * 2 * kCols, P.box_src[b], mid, sp,
+                      &full[s]);
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s) {
+            const int64_t t = blockIdx.x + (int64_t)s * gridDim.x;
+            if (t < P.ntiles) issue(t, s);
+        }
+    }
+    int k = 0;
+    for (int64_t t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++k) {
+        const int s = k & 1;
+        bool ok = mbar_wait(&full[s], (k >> 1) & 1);
+        const TileInfo ti = info[s];
+        float2 *A = tsm + s * n * kTmaPitch;
+        const int x = ti.xc * kCols + col;
+        const bool xin = x < P.X;
+        const int xs = xin ? x : P.X - 2;
+        float amid0 = P.factor, amid1 = P.factor;
+        if (P.mode != 0) {
+            if (P.apod_mid) {
+                amid0 *= P.apod_mid[ti.mid];
+                amid1 *= P.apod_mid[ti.mid];
+            }
+            if (P.apod_x) {
+                amid0 *= P.apod_x[xs];
+                amid1 *= P.apod_x[xs + 1];
+            }
+        }
+        if (ok && P.mode == 1) {
+            // deapodise the rows that hold image data (the others were filled with zeros)
+            for (int p = stream; p < n; p += NS) {
+                int i = p + P.hn;
+                if (i >= n) i -= n;
+                if (i >= P.lin) continue;
+                const float a = P.apod_ax ? P.apod_ax[i] : 1.f;
+                float4 *q = reinterpret_cast<float4 *>(A + p * kTmaPitch + col);
+                float4 v = *q;
+                const float a0 = a * amid0, a1 = a * amid1;
+                v.x *= a0;
+                v.y *= a0;
+                v.z *= a1;
+                v.w *= a1;
+                *q = v;
+            }
+        }
+        // every thread agrees on the wait's outcome; the previous tile's TMA store has
+        // read the scratch buffer (thread 0 waited on it before this barrier)
+        ok = __syncthreads_and(ok);
+        if (!ok) {
+            if (threadIdx.x == 0) {
+                atomicExch(P.err, 1);
+                // the other slot's load, if one is in flight
+                if (t + gridDim.x < P.ntiles) mbar_wait(&full[s ^ 1], ((k + 1) >> 1) & 1);
+            }
+            return;
+        }
+        const float2 *R = fft_run<kTmaPitch>(A, scr, P.fa);
+        if (fwd_store) {
+            // rows 0..n-1 of the result are the output rows: TMA store from shared memory
+            fence_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int b = 0; b < P.nsbox; ++b) {
+                    const int r0 = b + 1 < P.nsbox ? b * P.sbr : n - P.sbr;
+                    tma_store4(&dst_map, ti.xc * 2 * kCols, r0, ti.mid, ti.plane, R + r0 * kTmaPitch);
+                }
+                bulk_commit();
+                bulk_wait_read0();
+            }
+        } else {
+            // output row o holds inverse-transform position pp = (o - hn) mod n, i.e. the
+            // forward transform's position (n - pp) mod n
+            const int64_t obase = P.mode == 2 ? (int64_t)ti.plane * P.nvol + (int64_t)ti.mid * P.out_mid
+                                              : (int64_t)ti.plane * P.out_plane + (int64_t)ti.mid * P.out_mid;
+            for (int o = stream; o < P.lout; o += NS) {
+                int pp = o - P.hn;
+                if (pp < 0) pp += n;
+                const int q = pp == 0 ? 0 : n - pp;
+                float4 v = *reinterpret_cast<const float4 *>(R + q * kTmaPitch + col);
+                if (!xin) continue;
+                float4 *d = reinterpret_cast<float4 *>(P.dst + obase + (int64_t)o * P.out_ax + x);
+                if (P.mode == 2) {
+                    const float a = P.apod_ax ? P.apod_ax[o] : 1.f;
+                    const float a0 = a * amid0, a1 = a * amid1;
+                    v.x *= a0;
+                    v.y *= a0;
+                    v.z *= a1;
+                    v.w *= a1;
+                    if (P.accumulate) {
+                        const float4 old = *d;
+                        v.x += old.x;
+                        v.y += old.y;
+                        v.z += old.z;
+                        v.w += old.w;
+                    }
+                }
+                *d = v;
+            }
+            // the slot and the scratch buffer are read; the generic accesses are ordered
+            // before the slot's next TMA load
+            fence_async_smem();
+            __syncthreads();
+        }
+        // refill this slot with the tile after next
+        if (threadIdx.x == 0) {
+            const int64_t tn = t + 2 * (int64_t)gridDim.x;
+            if (tn < P.ntiles) issue(tn, s);
+        }
+    }
+}
+
 // Transform along x.  Forward: rows of T (N0 long, [plane][kz][ky][x]) -> the
 // interleaved grid [grp][point][ch]; the 16 vectors of a CTA are consecutive
 // (grp, kz, ky, ch) with ch fastest, so a half-warp stores 16 channels of one
@@ -650,9 +891,143 @@ size_t col_smem(int n, int mode, int nseg) {
 }
 size_t row_smem(int n) { return (size_t)2 * n * kPitch * sizeof(float2); }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the driver
+// library itself is not linked)
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+
+// 4D map over complex64 data seen as float32 pairs: (2 X floats, rows, mid,
+// planes) with the given element strides, boxes of 16 complex x br rows.  Rows
+// past `rows` read as zeros.  Strides of unit extents are unused: any legal value.
+bool encode_col_map(CUtensorMap *m, const void *base, int X, int rows, int nmid, int64_t nplanes, int64_t s_row,
+                    int64_t s_mid, int64_t s_plane, int br) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    if (nmid == 1) s_mid = s_row;
+    if (nplanes == 1) s_plane = s_row;
+    const cuuint64_t dim[4] = {(cuuint64_t)2 * X, (cuuint64_t)rows, (cuuint64_t)nmid, (cuuint64_t)nplanes};
+    const cuuint64_t str[3] = {(cuuint64_t)s_row * 8, (cuuint64_t)s_mid * 8, (cuuint64_t)s_plane * 8};
+    for (cuuint64_t v : str)
+        if (v == 0 || v % 16 != 0 || v >= (1ull << 40)) return false;
+    const cuuint32_t box[4] = {2 * kCols, (cuuint32_t)br, 1, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(base), dim, str, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// rows per box for segments of lengths a and b (b may be 0): the largest common
+// divisor <= 256 when it is at least 32 rows, else the shortest segment (<= 256)
+// with the last box of a segment overlapping the one before it
+int box_rows(int a, int b) {
+    const int m = std::min(256, b > 0 ? std::min(a, b) : a);
+    for (int d = m; d >= 32; --d)
+        if (a % d == 0 && (b == 0 || b % d == 0)) return d;
+    return m;
+}
+
+// The column pass on TMA when its layout allows it (every stride and base
+// 16-byte aligned, even X, no B0 factors, one segment); returns 1 if launched,
+// 0 to take the copy-based kernel, or an error.
+int launch_col_tma(const ColPass &P, int64_t ntiles, cudaStream_t s) {
+    const int n = P.fa.n;
+    if (!P.err || P.nsm <= 0 || P.Cl || (P.mode == 2 && P.ch.L != 1) || P.X % 2 != 0 || n > kMaxN) return 0;
+    auto a16 = [](const void *q) { return ((uintptr_t)q & 15u) == 0; };
+    if (!a16(P.src) || !a16(P.dst)) return 0;
+    const int64_t src_plane = P.mode == 1 ? P.nvol : P.in_plane;
+    const int64_t dst_plane = P.mode == 2 ? P.nvol : P.out_plane;
+    for (int64_t v : {P.in_ax, P.in_mid, src_plane, P.out_ax, P.out_mid, dst_plane})
+        if (v % 2 != 0) return 0;
+    ColTma T{};
+    T.fa = P.fa;
+    T.inv = P.inv;
+    T.mode = P.mode;
+    T.lin = P.lin;
+    T.lout = P.lout;
+    T.hn = P.nax / 2;
+    T.X = P.X;
+    T.nxc = (P.X + kCols - 1) / kCols;
+    T.nmid = P.nmid;
+    T.nplanes = P.nplanes;
+    T.ntiles = ntiles;
+    // load boxes: forward passes rotate (smem row p <- source row (p + hn) mod n),
+    // inverse passes read the rows in order
+    const int seg0 = P.inv ? n : n - T.hn, seg1 = P.inv ? 0 : T.hn;
+    T.br = box_rows(seg0, seg1);
+    if (T.br > P.lin) return 0;
+    int nb = 0;
+    for (int sg = 0; sg < 2; ++sg) {
+        const int len = sg == 0 ? seg0 : seg1;
+        const int s0 = sg == 0 ? 0 : seg0, r0 = sg == 0 ? (P.inv ? 0 : T.hn) : 0;
+        for (int r = 0; r < len; r += T.br) {
+            if (nb >= kTmaMaxBoxes) return 0;
+            const int o = std::min(r, len - T.br);
+            T.box_smem[nb] = s0 + o;
+            T.box_src[nb] = r0 + o;
+            ++nb;
+        }
+    }
+    T.nbox = nb;
+    if (!P.inv && P.mode != 2) {
+        if (P.lout != n) return 0;
+        T.sbr = box_rows(n, 0);
+        T.nsbox = (n + T.sbr - 1) / T.sbr;
+    }
+    T.out_plane = P.out_plane;
+    T.out_mid = P.out_mid;
+    T.out_ax = P.out_ax;
+    T.dst = P.dst;
+    T.ch = P.ch;
+    T.C = P.C;
+    T.nvol = P.nvol;
+    T.apod_ax = P.apod_ax;
+    T.apod_mid = P.apod_mid;
+    T.apod_x = P.apod_x;
+    T.factor = P.factor;
+    T.accumulate = P.accumulate;
+    T.err = P.err;
+    const int64_t src_planes = P.mode == 1 ? (int64_t)P.ch.B * P.C
+                                           : (P.mode == 2 ? (int64_t)P.ch.ngrp * P.ch.nch : P.nplanes);
+    CUtensorMap smap, dmap;
+    if (!encode_col_map(&smap, P.src, P.X, P.lin, P.nmid, src_planes, P.in_ax, P.in_mid, src_plane, T.br)) return 0;
+    if (T.nsbox > 0) {
+        if (!encode_col_map(&dmap, P.dst, P.X, n, P.nmid, P.nplanes, P.out_ax, P.out_mid, P.out_plane, T.sbr))
+            return 0;
+    } else {
+        dmap = smap;  // not read
+    }
+    const size_t smem = (size_t)3 * n * kTmaPitch * sizeof(float2);
+    PFB_RAISE_SMEM(col_tma_kernel, (int)smem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_tma_kernel, kThreads, smem) != cudaSuccess ||
+        per_sm < 1)
+        return 0;
+    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)P.nsm * per_sm);
+    col_tma_kernel<<<(unsigned)grid, kThreads, smem, s>>>(smap, dmap, T);
+    PFB_CHECK_LAUNCH();
+    return 1;
+}
+
 int launch_col(const ColPass &P, cudaStream_t s) {
     const int64_t blocks = (int64_t)P.nplanes * P.nmid * ((P.X + kCols - 1) / kCols);
     if (blocks == 0) return PFB_OK;
+    {
+        const int st = launch_col_tma(P, blocks, s);
+        if (st == 1) return PFB_OK;
+        if (st != 0) return st;
+    }
     if (blocks >= (1LL << 31)) return fail(PFB_ERR_UNSUPPORTED, "too many vectors for the fused FFT");
     const size_t smem = col_smem(P.fa.n, P.mode, P.ch.L);
     // two-column moves when every base and stride keeps the pairs 16-byte aligned
@@ -703,6 +1078,18 @@ int fft_fused_ready(pfb_plan *p) {
         return 0;
     }
     for (int a = 0; a < D; ++a) p->fft_ax[a].tw = p->d_fft_tw;
+    // the TMA column pass's flag and persistent grid (optional: without them the
+    // copy-based column pass runs)
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&p->fft_nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        p->fft_nsm = 0;
+    if (cudaMalloc(&p->d_fft_err, sizeof(int)) != cudaSuccess) {
+        p->d_fft_err = nullptr;
+    } else if (cudaMemset(p->d_fft_err, 0, sizeof(int)) != cudaSuccess) {
+        cudaFree(p->d_fft_err);
+        p->d_fft_err = nullptr;
+    }
     p->fft_fused = 1;
     return 1;
 }
@@ -711,6 +1098,8 @@ void fft_fused_free(pfb_plan *p) {
     std::lock_guard<std::mutex> lk(p->fft_mu);
     cudaFree(p->d_fft_tw);
     p->d_fft_tw = nullptr;
+    cudaFree(p->d_fft_err);
+    p->d_fft_err = nullptr;
     p->fft_fused = -1;
 }
 
@@ -722,6 +1111,8 @@ int fft_fused_fwd(pfb_plan *p, int pass, const Chan &c, int C, const float2 *img
     const int64_t N0 = g.n[0], N1 = g.n[1], n1 = g.nos[1], n2 = g.nos[2];
     if (pass == 0) {  // image -> first intermediate: z pass (3D) into gridi, or y pass (2D) into gridp
         ColPass Q{};
+        Q.err = p->d_fft_err;
+        Q.nsm = p->fft_nsm;
         Q.inv = 0;
         Q.mode = 1;
         Q.X = (int)N0;
@@ -765,6 +1156,8 @@ int fft_fused_fwd(pfb_plan *p, int pass, const Chan &c, int C, const float2 *img
     if (pass == 1) {  // 3D: y pass, gridi -> gridp
         if (D != 3) return PFB_OK;
         ColPass Q{};
+        Q.err = p->d_fft_err;
+        Q.nsm = p->fft_nsm;
         Q.fa = p->fft_ax[1];
         Q.inv = 0;
         Q.mode = 0;
@@ -817,6 +1210,8 @@ int fft_fused_adj(pfb_plan *p, int pass, const Chan &c, int C, float2 *img, cons
         if (st || D != 3) return st;
         // 3D: y pass, gridi -> gridp, cropped to N1
         ColPass Q{};
+        Q.err = p->d_fft_err;
+        Q.nsm = p->fft_nsm;
         Q.fa = p->fft_ax[1];
         Q.inv = 1;
         Q.mode = 0;
@@ -837,6 +1232,8 @@ int fft_fused_adj(pfb_plan *p, int pass, const Chan &c, int C, float2 *img, cons
     }
     // last pass -> image: z pass (3D, from gridp) or y pass (2D, from gridi)
     ColPass Q{};
+    Q.err = p->d_fft_err;
+    Q.nsm = p->fft_nsm;
     Q.inv = 1;
     Q.mode = 2;
     Q.X = (int)N0;
