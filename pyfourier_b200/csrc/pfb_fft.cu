@@ -534,7 +534,7 @@ struct ColTma {
     int inv, mode;          // as ColPass: 0 buffer -> buffer, 1 image -> buffer, 2 buffer -> image
     int lin, lout, hn;      // rows read / written; hn: rotation of the fftshift (nax / 2)
     int X, nxc, nmid, nplanes;
-    int64_t ntiles;
+    int ntiles;
     int nbox;               // load boxes per tile: smem row, source row (before the +hn rotation fold)
     int box_smem[kTmaMaxBoxes], box_src[kTmaMaxBoxes];
     int br;                 // rows per load box
@@ -614,10 +614,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     const unsigned box_bytes = (unsigned)P.br * kTmaPitch * sizeof(float2);
     const bool fwd_store = P.mode != 2 && !P.inv;
     // thread 0: load tile t into slot s (tile coordinates go with it through shared memory)
-    auto issue = [&](int64_t t, int s) {
-        const int xc = (int)(t % P.nxc);
-        const int64_t r = t / P.nxc;
-        const int mid = (int)(r % P.nmid), plane = (int)(r / P.nmid);
+    auto issue = [&](int t, int s) {
+        const int r = t / P.nxc, xc = t - r * P.nxc;
+        const int plane = r / P.nmid, mid = r - plane * P.nmid;
         int sp = plane;  // source plane
         if (P.mode == 1) {  // grid plane (grp, ch) <- image plane (b, c)
             const int Kc = P.ch.K ? P.ch.K : 1;
@@ -643,12 +642,13 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int s = 0; s < 2; ++s) {
-            const int64_t t = blockIdx.x + (int64_t)s * gridDim.x;
+            const int t = blockIdx.x + s * gridDim.x;
             if (t < P.ntiles) issue(t, s);
         }
     }
     int k = 0;
-    for (int64_t t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++k) {
+    bool store_pending = false;  // thread 0: a TMA store of the scratch buffer may still be reading it
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++k) {
         const int s = k & 1;
         bool ok = mbar_wait(&full[s], (k >> 1) & 1);
         const TileInfo ti = info[s];
@@ -684,18 +684,24 @@ __global__ void __launch_bounds__(kThreads, 2)
                 *q = v;
             }
         }
-        // every thread agrees on the wait's outcome; the previous tile's TMA store has
-        // read the scratch buffer (thread 0 waited on it before this barrier)
+        // the previous tile's TMA store has read the scratch buffer before the
+        // transform below writes it; every thread agrees on the wait's outcome
+        if (threadIdx.x == 0 && store_pending) {
+            bulk_wait_read0();
+            store_pending = false;
+        }
         ok = __syncthreads_and(ok);
         if (!ok) {
             if (threadIdx.x == 0) {
                 atomicExch(P.err, 1);
                 // the other slot's load, if one is in flight
-                if (t + gridDim.x < P.ntiles) mbar_wait(&full[s ^ 1], ((k + 1) >> 1) & 1);
+                if (t + (int)gridDim.x < P.ntiles) mbar_wait(&full[s ^ 1], ((k + 1) >> 1) & 1);
+                if (store_pending) bulk_wait_read0();
             }
             return;
         }
         const float2 *R = fft_run<kTmaPitch>(A, scr, P.fa);
+        const int tn = t + 2 * gridDim.x;  // the tile after next, for this slot
         if (fwd_store) {
             // rows 0..n-1 of the result are the output rows: TMA store from shared memory
             fence_async_smem();
@@ -706,8 +712,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                     tma_store4(&dst_map, ti.xc * 2 * kCols, r0, ti.mid, ti.plane, R + r0 * kTmaPitch);
                 }
                 bulk_commit();
-                bulk_wait_read0();
+                // refill the slot now unless the store reads it; a store of the scratch
+                // buffer is waited for before the next transform
+                if (R == A) bulk_wait_read0();
+                else store_pending = true;
+                if (tn < P.ntiles) issue(tn, s);
             }
+            continue;
         } else {
             // output row o holds inverse-transform position pp = (o - hn) mod n, i.e. the
             // forward transform's position (n - pp) mod n
@@ -743,11 +754,9 @@ __global__ void __launch_bounds__(kThreads, 2)
             __syncthreads();
         }
         // refill this slot with the tile after next
-        if (threadIdx.x == 0) {
-            const int64_t tn = t + 2 * (int64_t)gridDim.x;
-            if (tn < P.ntiles) issue(tn, s);
-        }
+        if (threadIdx.x == 0 && tn < P.ntiles) issue(tn, s);
     }
+    if (threadIdx.x == 0 && store_pending) bulk_wait_read0();
 }
 
 // Transform along x.  Forward: rows of T (N0 long, [plane][kz][ky][x]) -> the
@@ -961,7 +970,8 @@ int launch_col_tma(const ColPass &P, int64_t ntiles, cudaStream_t s) {
     T.nxc = (P.X + kCols - 1) / kCols;
     T.nmid = P.nmid;
     T.nplanes = P.nplanes;
-    T.ntiles = ntiles;
+    if (ntiles >= (1LL << 31) - 2LL * P.nsm * 4) return 0;
+    T.ntiles = (int)ntiles;
     // load boxes: forward passes rotate (smem row p <- source row (p + hn) mod n),
     // inverse passes read the rows in order
     const int seg0 = P.inv ? n : n - T.hn, seg1 = P.inv ? 0 : T.hn;

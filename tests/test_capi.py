@@ -50,6 +50,7 @@ def test_status_mapping_without_gpu():
     assert L.pfb_gram_destroy(None) == 0
     info = _lib.PlanInfoT()
     assert L.pfb_plan_info(None, ctypes.byref(info)) == _lib.PFB_ERR_INVALID
+    assert L.pfb_plan_check(None, None) == _lib.PFB_ERR_INVALID
 
 
 def test_apply_struct_layout_matches_header(tmp_path):
