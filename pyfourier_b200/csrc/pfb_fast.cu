@@ -964,21 +964,21 @@ constexpr int kRegPts = kRegTile * kRegTile * kRegTile;
 // Launch shape of the register spread for CPW channels per lane group: the 32
 // lanes of a warp are G = 32 / CPW groups of CPW channels, each group owning one
 // of the 16 blocks of 4 x 4 x 2 points, so a CTA has 16 / G warps.
-// Staging: two raw buffers (values [B][CPW] f2, weights [B][24] f, first taps
-// [B][4] i, neighbour bits [B] i), filled by cp.async one batch ahead, then one
-// set of derived arrays (tile weights [B][24] f2, each weight held twice as the
-// broadcast operand of a packed FFMA2; masks [B] u), written and read within one
-// batch.  With 32 channels one CTA fills an SM (registers); smaller groups use
-// smaller batches so that 2 (16 channels) or 4 (8) CTAs share an SM.
-template <int CPW>
+// Staging: two raw buffers (values [B][CPW] f2, plan records [B][REC] words
+// (the kernel weights, then the first taps), neighbour bits [B] i), filled by
+// cp.async one batch ahead, then one set of derived arrays (tile weights [B][24]
+// f2, each weight held twice as the broadcast operand of a packed FFMA2; masks
+// [B] u), written and read within one batch.  With 32 channels one CTA fills an
+// SM (registers); smaller groups use smaller batches so that 2 (16 channels) or
+// 4 (8) CTAs share an SM.
+template <int CPW, int REC>
 struct RegCfg {
     static constexpr int G = 32 / CPW;
     static constexpr int NW = 16 / G;
     static constexpr int Batch = CPW == 32 ? 224 : (CPW == 16 ? 128 : 80);
     static constexpr int MinBlocks = CPW == 32 ? 1 : (CPW == 16 ? 2 : 4);
-    static constexpr size_t OffW = (size_t)Batch * CPW * sizeof(float2);
-    static constexpr size_t OffX = OffW + (size_t)Batch * 24 * sizeof(float);
-    static constexpr size_t OffD = OffX + (size_t)Batch * 4 * sizeof(int);
+    static constexpr size_t OffR = (size_t)Batch * CPW * sizeof(float2);
+    static constexpr size_t OffD = OffR + (size_t)Batch * REC * sizeof(int);
     static constexpr size_t Buf = OffD + (size_t)Batch * sizeof(int);
     static constexpr size_t OffTW = 2 * Buf;
     static constexpr size_t OffM = OffTW + (size_t)Batch * 24 * sizeof(float2);
@@ -1012,11 +1012,11 @@ __device__ __forceinline__ void reg3_rows(float2 (&acc)[32], const float2 (&wx2)
 }
 
 template <int WM, int CPW>
-__global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
+__global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<CPW, tap_rec(3, WM)>::MinBlocks)
     spread_reg3_kernel(const SpreadIL P) {
-    using C = RegCfg<CPW>;
+    constexpr int D = 3, DW = D * WM, REC = tap_rec(D, WM);
+    using C = RegCfg<CPW, REC>;
     constexpr int G = C::G, NW = C::NW;
-    constexpr int D = 3, DW = D * WM;
     extern __shared__ __align__(16) unsigned char smraw[];
     int *s_pos = reinterpret_cast<int *>(smraw);
     unsigned char *ub = smraw + kRegPts * sizeof(int);
@@ -1053,27 +1053,65 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
     const int nvis = it.v1 - it.v0;
     const int nbat = (nvis + C::Batch - 1) / C::Batch;
     auto batch_size = [&](int bb) { return (nvis - bb + nbat - 1) / nbat; };
-    // issue the copies of batch bb into buffer buf (warps take samples warp, warp + NW, ...)
+    // issue the copies of batch bb into buffer buf.  A warp takes rounds of 32
+    // samples (warp, warp + NW, ... in units of 32): lane l resolves sample q0 + l
+    // (its sorted position and neighbour delta), then the warp copies the round's
+    // plan records and value rows in 16-byte pieces, consecutive lanes on
+    // consecutive pieces of a row
     auto issue = [&](int bb, int buf) {
         unsigned char *B = ub + buf * C::Buf;
         float2 *rv = reinterpret_cast<float2 *>(B);
-        float *rw = reinterpret_cast<float *>(B + C::OffW);
-        int *rx = reinterpret_cast<int *>(B + C::OffX);
+        int *rr = reinterpret_cast<int *>(B + C::OffR);
         int *rd = reinterpret_cast<int *>(B + C::OffD);
         const int nb = batch_size(bb);
-        for (int q = warp; q < nb; q += NW) {
-            // batch bb takes visits bb, bb + nbat, bb + 2 nbat, ...: every batch
-            // mixes the neighbour ranges, so all warps find work in it
-            const int v = it.v0 + bb + q * nbat;
-            // range: the last one whose prefix is <= v (empty ranges share the
-            // prefix of the next one and are skipped)
-            const unsigned le = __ballot_sync(0xffffffffu, lane < NR && s_pre[lane] <= v);
-            const int r = 31 - __clz(le);
-            const int64_t j = (int64_t)s_beg[r] + (v - s_pre[r]);
-            if (lane < CPW) cp_async8(rv + q * CPW + lane, P.vals + j * nch + (c < nch ? c : 0), c < nch);
-            if (lane < DW) cp_async4(rw + q * 24 + lane, P.wtap + j * tap_rec(D, WM) + lane);
-            if (lane < D) cp_async4(rx + q * 4 + lane, P.xtap + j * tap_rec(D, WM) + lane);
-            if (lane == 0) rd[q] = s_dlt[r];
+        for (int q0 = warp * 32; q0 < nb; q0 += NW * 32) {
+            const int q = q0 + lane, nq = min(32, nb - q0);
+            int j = 0;
+            if (q < nb) {
+                // batch bb takes visits bb, bb + nbat, bb + 2 nbat, ...: every batch
+                // mixes the neighbour ranges, so all warps find work in it
+                const int v = it.v0 + bb + q * nbat;
+                // range: the last one whose prefix is <= v (empty ranges share the
+                // prefix of the next one and are skipped)
+                int lo = 0, hi = NR;
+                while (hi - lo > 1) {
+                    const int m = (lo + hi) >> 1;
+                    if (s_pre[m] <= v) lo = m;
+                    else hi = m;
+                }
+                j = s_beg[lo] + (v - s_pre[lo]);
+                rd[q] = s_dlt[lo];
+            }
+            // plan records: REC / 4 pieces per sample
+            constexpr int RP = REC / 4;
+            for (int e0 = 0; e0 < nq * RP; e0 += 32) {
+                const int e = e0 + lane;
+                const bool in = e < nq * RP;
+                const int sq = in ? e / RP : 0, part = e - sq * RP;
+                const int js = __shfl_sync(0xffffffffu, j, sq);
+                cp_async16(rr + (q0 + sq) * REC + 4 * part, P.wtap + (in ? (int64_t)js * REC + 4 * part : 0), in);
+            }
+            // value rows: channels c0 .. c0 + CPW - 1, zeros past nch
+            if (nch % 2 == 0) {
+                constexpr int VP = CPW / 2;  // 16-byte pieces (two channels) per row
+                for (int e0 = 0; e0 < nq * VP; e0 += 32) {
+                    const int e = e0 + lane;
+                    const int sq = e < nq * VP ? e / VP : 0, part = e - sq * VP;
+                    const int js = __shfl_sync(0xffffffffu, j, sq);
+                    const int ch = c0 + 2 * part;
+                    const bool ok = e < nq * VP && ch < nch;
+                    cp_async16(rv + (q0 + sq) * CPW + 2 * part, P.vals + (ok ? (int64_t)js * nch + ch : 0), ok);
+                }
+            } else {
+                for (int e0 = 0; e0 < nq * CPW; e0 += 32) {
+                    const int e = e0 + lane;
+                    const int sq = e < nq * CPW ? e / CPW : 0, part = e - sq * CPW;
+                    const int js = __shfl_sync(0xffffffffu, j, sq);
+                    const int ch = c0 + part;
+                    const bool ok = e < nq * CPW && ch < nch;
+                    cp_async8(rv + (q0 + sq) * CPW + part, P.vals + (ok ? (int64_t)js * nch + ch : 0), ok);
+                }
+            }
         }
     };
     // this lane's block (block id warp * G + group) and the warp's blocks' bits in the
@@ -1108,8 +1146,8 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
         cp_async_commit();
         unsigned char *B = ub + cur * C::Buf;
         const float2 *rv = reinterpret_cast<const float2 *>(B);
-        const float *rw = reinterpret_cast<const float *>(B + C::OffW);
-        const int *rx = reinterpret_cast<const int *>(B + C::OffX);
+        const float *rw = reinterpret_cast<const float *>(B + C::OffR);  // records: weights, then first taps
+        const int *rx = reinterpret_cast<const int *>(B + C::OffR) + DW;
         const int *rd = reinterpret_cast<const int *>(B + C::OffD);
         float2 *tw = reinterpret_cast<float2 *>(ub + C::OffTW);
         unsigned *tm = reinterpret_cast<unsigned *>(ub + C::OffM);
@@ -1117,11 +1155,11 @@ __global__ void __launch_bounds__(RegCfg<CPW>::NW * 32, RegCfg<CPW>::MinBlocks)
         for (int q = warp; q < nb; q += NW) {
             float wv = 0.f;
             if (lane < 24) {
-                int d = rx[q * 4 + la] - orga;
+                int d = rx[q * REC + la] - orga;
                 if (((rd[q] >> la) & 1) && d >= 0) d -= nosa;
                 int i = lt - d;
                 if (wrapa && i < 0) i += wrapa;
-                if (lt < texta && i >= 0 && i < wa) wv = rw[q * 24 + la * WM + i];
+                if (lt < texta && i >= 0 && i < wa) wv = rw[q * REC + la * WM + i];
                 tw[q * 24 + lane] = make_float2(wv, wv);
             }
             const unsigned m = __ballot_sync(0xffffffffu, wv != 0.f);
@@ -1462,7 +1500,7 @@ int launch_traj_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
 
 template <int WM, int CPW>
 int launch_spread_reg3_t(const SpreadIL &P, int nitems, int nchunks, cudaStream_t s) {
-    using C = RegCfg<CPW>;
+    using C = RegCfg<CPW, tap_rec(3, WM)>;
     auto k = spread_reg3_kernel<WM, CPW>;
     PFB_RAISE_SMEM(k, (int)C::Smem);
     dim3 grid(nitems, nchunks);
