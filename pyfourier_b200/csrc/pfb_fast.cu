@@ -1029,7 +1029,7 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nch = P.ch.nch;
     const int cl = lane % CPW, grpl = lane / CPW;  // channel and block group of this lane
-    const int c0 = blockIdx.y * CPW, c = c0 + cl;
+    const int c0 = blockIdx.y * CPW;
     int org[3], text[3], wrap[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -1126,13 +1126,9 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
         bmy[g] = 0xFu << (8 + ((b2 >> 1) & 1) * 4);
         bmz[g] = 0x3u << (16 + (b2 >> 2) * 2);
     }
-    // lane (a, t): tile coordinate t on axis a (lanes 0..23)
-    const int la = lane >> 3, lt = lane & 7;
-    const int orga = la == 0 ? org[0] : (la == 1 ? org[1] : org[2]);
-    const int texta = la == 0 ? text[0] : (la == 1 ? text[1] : text[2]);
-    const int wrapa = la == 0 ? wrap[0] : (la == 1 ? wrap[1] : wrap[2]);
-    const int nosa = la == 0 ? P.g.nos[0] : (la == 1 ? P.g.nos[1] : P.g.nos[2]);
-    const int wa = la == 0 ? P.g.w[0] : (la == 1 ? P.g.w[1] : P.g.w[2]);
+    // tile weights: lane (slot, t) builds tile coordinate t of every axis for sample
+    // slot (lanes 8 slot .. 8 slot + 7), four samples per warp pass
+    const int lt = lane & 7, lslot = lane >> 3;
     float2 acc[32];
 #pragma unroll
     for (int q = 0; q < 32; ++q) acc[q] = make_float2(0.f, 0.f);
@@ -1152,18 +1148,38 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
         float2 *tw = reinterpret_cast<float2 *>(ub + C::OffTW);
         unsigned *tm = reinterpret_cast<unsigned *>(ub + C::OffM);
         const int nb = batch_size(b);
-        for (int q = warp; q < nb; q += NW) {
-            float wv = 0.f;
-            if (lane < 24) {
-                int d = rx[q * REC + la] - orga;
-                if (((rd[q] >> la) & 1) && d >= 0) d -= nosa;
-                int i = lt - d;
-                if (wrapa && i < 0) i += wrapa;
-                if (lt < texta && i >= 0 && i < wa) wv = rw[q * REC + la * WM + i];
-                tw[q * 24 + lane] = make_float2(wv, wv);
+        for (int q0 = warp * 4; q0 < nb; q0 += NW * 4) {
+            const int q = q0 + lslot;
+            const bool qv = q < nb;
+            int4 x0 = make_int4(0, 0, 0, 0);
+            int dl = 0;
+            if (qv) {
+                // first taps mod n_os (x, y, z); one 16-byte load when they start 16-byte aligned
+                if constexpr (DW % 4 == 0) {
+                    x0 = *reinterpret_cast<const int4 *>(rx + q * REC);
+                } else {
+                    x0.x = rx[q * REC];
+                    x0.y = rx[q * REC + 1];
+                    x0.z = rx[q * REC + 2];
+                }
+                dl = rd[q];
             }
-            const unsigned m = __ballot_sync(0xffffffffu, wv != 0.f);
-            if (lane == 0) tm[q] = m;
+            unsigned m = 0;  // the sample's 24-bit mask of non-zero tile weights
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                float wv = 0.f;
+                if (qv) {
+                    int d = (a == 0 ? x0.x : (a == 1 ? x0.y : x0.z)) - org[a];
+                    if (((dl >> a) & 1) && d >= 0) d -= P.g.nos[a];
+                    int i = lt - d;
+                    if (wrap[a] && i < 0) i += wrap[a];
+                    if (lt < text[a] && i >= 0 && i < P.g.w[a]) wv = rw[q * REC + a * WM + i];
+                    tw[q * 24 + a * 8 + lt] = make_float2(wv, wv);
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, wv != 0.f);
+                m |= ((bal >> (8 * lslot)) & 0xffu) << (8 * a);
+            }
+            if (qv && lt == 0) tm[q] = m;
         }
         __syncthreads();  // tile weights and masks of batch b ready
         for (int q0 = 0; q0 < nb; q0 += 32) {
