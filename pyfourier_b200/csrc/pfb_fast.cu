@@ -960,7 +960,6 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
 // samples that touch its block.  The tile leaves through shared memory,
 // coalesced along x.
 constexpr int kRegTile = 8;                   // packed tile extent per axis
-constexpr int kRegPts = kRegTile * kRegTile * kRegTile;
 // Launch shape of the register spread for CPW channels per lane group: the 32
 // lanes of a warp are G = 32 / CPW groups of CPW channels, each group owning one
 // of the 16 blocks of 4 x 4 x 2 points, so a CTA has 16 / G warps.
@@ -983,8 +982,8 @@ struct RegCfg {
     static constexpr size_t OffTW = 2 * Buf;
     static constexpr size_t OffM = OffTW + (size_t)Batch * 24 * sizeof(float2);
     static constexpr size_t Stage = OffM + (size_t)Batch * sizeof(unsigned);
-    static constexpr size_t Out = (size_t)kRegPts * (CPW + 1) * sizeof(float2);
-    static constexpr size_t Smem = kRegPts * sizeof(int) + (Out > Stage ? Out : Stage);
+    static constexpr size_t Out = (size_t)kRegTile * kRegTile * kRegTile * (CPW + 1) * sizeof(float2);
+    static constexpr size_t Smem = Out > Stage ? Out : Stage;
     static_assert(Buf % 16 == 0 && OffTW % 16 == 0, "16-byte aligned staging arrays");
     static_assert(Smem * MinBlocks + MinBlocks * 1024 <= 228 * 1024, "shared memory of the CTAs of one SM");
 };
@@ -1017,10 +1016,7 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
     constexpr int D = 3, DW = D * WM, REC = tap_rec(D, WM);
     using C = RegCfg<CPW, REC>;
     constexpr int G = C::G, NW = C::NW;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    int *s_pos = reinterpret_cast<int *>(smraw);
-    unsigned char *ub = smraw + kRegPts * sizeof(int);
-    float2 *s_out = reinterpret_cast<float2 *>(ub);  // [16 blocks x 32 points][CPW + 1], after the last batch
+    extern __shared__ __align__(16) unsigned char ub[];
     constexpr int NR = 27;
     __shared__ int s_pre[NR + 1];
     __shared__ int s_beg[NR];
@@ -1037,16 +1033,6 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
         org[a] = tile_org(P.g, a, tc);
         text[a] = tile_extent(P.g, a, tc);
         wrap[a] = P.g.nbins[a] == 1 ? text[a] : 0;
-    }
-    for (int pt = threadIdx.x; pt < kRegPts; pt += blockDim.x) {
-        const int t0 = pt & 7, t1 = (pt >> 3) & 7, t2 = pt >> 6;
-        int pos = -1;
-        if (t0 < text[0] && t1 < text[1] && t2 < text[2]) {
-            pos = pmod(org[0] + t0 - P.g.sh[0], P.g.nos[0]) +
-                  pmod(org[1] + t1 - P.g.sh[1], P.g.nos[1]) * P.g.nos[0] +
-                  pmod(org[2] + t2 - P.g.sh[2], P.g.nos[2]) * P.g.nos[0] * P.g.nos[1];
-        }
-        s_pos[pt] = pos;
     }
     if (warp == 0) neighbour_ranges<3>(P, it, s_pre, s_beg, s_dlt, lane);
     __syncthreads();
@@ -1224,24 +1210,31 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
             }
         }
     }
-    __syncthreads();  // staging no longer read: reuse it for the output tile
+    // the tile leaves through shared memory: [16 blocks x 32 points][CPW + 1]
+    // (odd pitch), then thread pt writes tile point pt of every channel (the points
+    // of a warp are 4 rows of 8 x positions, contiguous in the grid between wraps)
+    float2 *s_out = reinterpret_cast<float2 *>(ub);
+    __syncthreads();  // staging no longer read
 #pragma unroll
     for (int q = 0; q < 32; ++q) s_out[(bid * 32 + q) * (CPW + 1) + cl] = acc[q];
     __syncthreads();
     const int grp = P.ch.K ? 0 : (it.frame < 0 ? 0 : it.frame);
-    for (int e = threadIdx.x; e < CPW * kRegPts; e += blockDim.x) {
-        const int ce = e / kRegPts, pt = e - ce * kRegPts;
-        const int ch = c0 + ce;
-        if (ch >= nch) break;
-        const int pos = s_pos[pt];
-        if (pos < 0) continue;
+    const int nce = min(CPW, nch - c0);
+    for (int pt = threadIdx.x; pt < kRegTile * kRegTile * kRegTile; pt += blockDim.x) {
         const int x = pt & 7, y = (pt >> 3) & 7, z = pt >> 6;
+        if (x >= text[0] || y >= text[1] || z >= text[2]) continue;
+        const int pos = pmod(org[0] + x - P.g.sh[0], P.g.nos[0]) +
+                        pmod(org[1] + y - P.g.sh[1], P.g.nos[1]) * P.g.nos[0] +
+                        pmod(org[2] + z - P.g.sh[2], P.g.nos[2]) * P.g.nos[0] * P.g.nos[1];
         const int w = (x >> 2) | ((y >> 2) << 1) | ((z >> 1) << 2);
         const int q = (x & 3) | ((y & 3) << 2) | ((z & 1) << 4);
-        const float2 vv = s_out[(w * 32 + q) * (CPW + 1) + ce];
-        float2 *Gp = P.grid + ((int64_t)grp * nch + ch) * P.g.gvol;
-        if (it.atomic) atomicAdd(Gp + pos, vv);
-        else Gp[pos] = vv;
+        const float2 *src = s_out + (w * 32 + q) * (CPW + 1);
+        float2 *dst = P.grid + ((int64_t)grp * nch + c0) * P.g.gvol + pos;
+        if (it.atomic) {
+            for (int ce = 0; ce < nce; ++ce, dst += P.g.gvol) atomicAdd(dst, src[ce]);
+        } else {
+            for (int ce = 0; ce < nce; ++ce, dst += P.g.gvol) *dst = src[ce];
+        }
     }
 }
 
