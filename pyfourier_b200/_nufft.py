@@ -263,12 +263,26 @@ def _finish(out, dtype, idevice, as_numpy):
 _HOST_PIPELINE_MIN_BYTES = 64 << 20
 _HOST_PIPELINE_CHUNKS_FWD = 8
 _HOST_PIPELINE_CHUNKS_ADJ = 4
+_HOST_PIPELINE_SHIFT = True
 
 
 def _host_pipelined(t, grad_coord):
     """A CPU complex64 input without autograd history takes the chunked host path."""
     return (t.device.type == "cpu" and t.dtype == torch.complex64 and not t.requires_grad and grad_coord is None
             and t.numel() * 8 >= _HOST_PIPELINE_MIN_BYTES)
+
+
+def _chunk_bounds(B, chunks):
+    """Batch ranges of the host pipeline: ``chunks`` chunks of about B / chunks items
+    with the boundaries shifted by half a chunk when _HOST_PIPELINE_SHIFT is set, so
+    that the first and the last chunk are half as large (their host->device copy and
+    read-back are the ones that run alone): 32 in 4 gives 4, 8, 8, 8, 4."""
+    n = max(1, min(B, chunks))
+    if _HOST_PIPELINE_SHIFT and n >= 2 and B >= 2 * n:
+        edges = sorted({0, B} | {(B * (2 * k + 1)) // (2 * n) for k in range(n)})
+    else:
+        edges = [B * j // n for j in range(n + 1)]
+    return [(a, b) for a, b in zip(edges[:-1], edges[1:]) if b > a]
 
 
 def _pipeline(xh, run, out_tail, dev, chunks):
@@ -279,8 +293,7 @@ def _pipeline(xh, run, out_tail, dev, chunks):
     page-locked buffers.  Returns a page-locked CPU tensor (B, *out_tail)."""
     B = xh.shape[0]
     out = torch.empty((B, *out_tail), dtype=torch.complex64, pin_memory=True)
-    n = max(1, min(B, chunks))
-    bounds = [(B * j // n, B * (j + 1) // n) for j in range(n)]
+    bounds = _chunk_bounds(B, chunks)
     pinned = xh.is_pinned()
     with torch.cuda.device(dev):
         comp = torch.cuda.current_stream(dev)
