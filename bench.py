@@ -1163,10 +1163,10 @@ def extra_workload(args):
 
 
 # DRAM bytes (read + write) per launch of the dominant kernel: the ncu capture of
-# the 128^3 / 32-coil variant (0.945 + 1.001 GB for 32 x 2.048 M samples) scaled by
+# the 128^3 / 32-coil variant (0.947 + 1.001 GB for 32 x 2.048 M samples) scaled by
 # the samples processed (x 3.906) to the 200^3 / 8 M-sample workload; the capture
 # and its command are summarised under profiles/.
-NCU_TRAFFIC = {("cfg2", "spread"): int(1.946e9 * 3.906)}
+NCU_TRAFFIC = {("cfg2", "spread"): int(1.948e9 * 3.906)}
 
 
 def main():
