@@ -1068,34 +1068,38 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
                 j = s_beg[lo] + (v - s_pre[lo]);
                 rd[q] = s_dlt[lo];
             }
-            // plan records: REC / 4 pieces per sample
+            // plan records: REC / 4 pieces per sample.  Lanes past the round's last
+            // piece copy nothing (a zero-size copy still writes its destination)
             constexpr int RP = REC / 4;
             for (int e0 = 0; e0 < nq * RP; e0 += 32) {
                 const int e = e0 + lane;
                 const bool in = e < nq * RP;
                 const int sq = in ? e / RP : 0, part = e - sq * RP;
                 const int js = __shfl_sync(0xffffffffu, j, sq);
-                cp_async16(rr + (q0 + sq) * REC + 4 * part, P.wtap + (in ? (int64_t)js * REC + 4 * part : 0), in);
+                if (in) cp_async16(rr + (q0 + sq) * REC + 4 * part, P.wtap + (int64_t)js * REC + 4 * part, true);
             }
-            // value rows: channels c0 .. c0 + CPW - 1, zeros past nch
+            // value rows: channels c0 .. c0 + CPW - 1, zero-filled past nch; lanes past
+            // the round's last piece copy nothing
             if (nch % 2 == 0) {
                 constexpr int VP = CPW / 2;  // 16-byte pieces (two channels) per row
                 for (int e0 = 0; e0 < nq * VP; e0 += 32) {
                     const int e = e0 + lane;
-                    const int sq = e < nq * VP ? e / VP : 0, part = e - sq * VP;
+                    const bool in = e < nq * VP;
+                    const int sq = in ? e / VP : 0, part = e - sq * VP;
                     const int js = __shfl_sync(0xffffffffu, j, sq);
                     const int ch = c0 + 2 * part;
-                    const bool ok = e < nq * VP && ch < nch;
-                    cp_async16(rv + (q0 + sq) * CPW + 2 * part, P.vals + (ok ? (int64_t)js * nch + ch : 0), ok);
+                    const bool ok = ch < nch;
+                    if (in) cp_async16(rv + (q0 + sq) * CPW + 2 * part, P.vals + (ok ? (int64_t)js * nch + ch : 0), ok);
                 }
             } else {
                 for (int e0 = 0; e0 < nq * CPW; e0 += 32) {
                     const int e = e0 + lane;
-                    const int sq = e < nq * CPW ? e / CPW : 0, part = e - sq * CPW;
+                    const bool in = e < nq * CPW;
+                    const int sq = in ? e / CPW : 0, part = e - sq * CPW;
                     const int js = __shfl_sync(0xffffffffu, j, sq);
                     const int ch = c0 + part;
-                    const bool ok = e < nq * CPW && ch < nch;
-                    cp_async8(rv + (q0 + sq) * CPW + part, P.vals + (ok ? (int64_t)js * nch + ch : 0), ok);
+                    const bool ok = ch < nch;
+                    if (in) cp_async8(rv + (q0 + sq) * CPW + part, P.vals + (ok ? (int64_t)js * nch + ch : 0), ok);
                 }
             }
         }
@@ -1980,11 +1984,13 @@ void owner_items_for(const pfb_plan *p, bool per_frame, int chunk, std::vector<O
 
 template <typename T>
 int upload(const std::vector<T> &h, T **d) {
-    cudaFree(*d);
-    *d = nullptr;
-    size_t n = std::max<size_t>(h.size(), 1);
-    cudaError_t e = cudaMalloc((void **)d, n * sizeof(T));
-    if (e != cudaSuccess) return fail(PFB_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    if (*d) {
+        cudaDeviceSynchronize();  // applies in flight may read the old table
+        pool_free(*d, 0);
+        *d = nullptr;
+    }
+    const int st = pool_alloc(reinterpret_cast<void **>(d), std::max<size_t>(h.size(), 1) * sizeof(T));
+    if (st) return st;
     if (!h.empty()) PFB_CUDA_TRY(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
     return PFB_OK;
 }
@@ -2009,13 +2015,17 @@ int build_owner_items(pfb_plan *p, int chunk) {
 }
 
 int build_plan_taps(pfb_plan *p, cudaStream_t s) {
-    cudaFree(p->d_wtap);
+    if (p->d_wtap) {
+        cudaDeviceSynchronize();  // applies in flight may read the old records
+        pool_free(p->d_wtap, 0);
+    }
     p->d_wtap = nullptr;
     p->d_xtap = nullptr;
     const int D = p->g.ndim, WM = wm_of(p->g);
     const size_t n = (size_t)std::max<int64_t>(p->mtot, 1);
     // one record per sorted sample: weights, then first taps (d_xtap points into it)
-    PFB_CUDA_TRY(cudaMalloc(&p->d_wtap, n * tap_rec(D, WM) * sizeof(float)));
+    const int st = pool_alloc(reinterpret_cast<void **>(&p->d_wtap), n * tap_rec(D, WM) * sizeof(float));
+    if (st) return st;
     p->d_xtap = reinterpret_cast<int *>(p->d_wtap + D * WM);
     if (p->mtot == 0) return PFB_OK;
     const int tb = flat_blocks(p->mtot);
@@ -2037,13 +2047,14 @@ int build_plan_taps(pfb_plan *p, cudaStream_t s) {
 }
 
 void free_owner_items(pfb_plan *p) {
-    cudaFree(p->d_wtap);  // d_xtap points into the same records
+    cudaDeviceSynchronize();  // every apply of the plan has finished
+    pool_free(p->d_wtap, 0);  // d_xtap points into the same records
     p->d_wtap = nullptr;
     p->d_xtap = nullptr;
-    cudaFree(p->d_own_frame);
-    cudaFree(p->d_zero_frame);
-    cudaFree(p->d_own_all);
-    cudaFree(p->d_zero_all);
+    pool_free(p->d_own_frame, 0);
+    pool_free(p->d_zero_frame, 0);
+    pool_free(p->d_own_all, 0);
+    pool_free(p->d_zero_all, 0);
     p->d_own_frame = p->d_zero_frame = p->d_own_all = p->d_zero_all = nullptr;
     fft_fused_free(p);
 }

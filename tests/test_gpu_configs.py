@@ -139,3 +139,22 @@ def test_differentiable_spiral_8_coils_ortho():
     assert rel(yg, yr) < TOL
     xg = P.nufft_adj(yg, nufft_plan=gplan, norm="ortho")
     assert rel(xg, orc.nufft_adj(yr, oplan, norm="ortho")) < TOL
+
+
+@pytest.mark.parametrize("B", [1, 8, 16])
+def test_3d_w6_few_channel_spread_is_deterministic(B):
+    """Width 6 (8-tap register blocks) with 8- and 16-channel groups on a crowded 3D
+    radial plan: full batches whose last staging round is partial.  Two applies give
+    the same image, and it matches the reference's adjoint in float64."""
+    P = pf()
+    N = 48
+    coord = bench.golden_means_radial_3d(2000, 96, N)
+    gplan = P.plan_nufft(torch.as_tensor(coord), (N, N, N), width=6, oversamp=1.5, device="cuda:0")
+    oplan = orc.plan_nufft(coord, (N, N, N), width=6, oversamp=1.5)
+    yk = crandn(np.random.default_rng(B), B, 2000, 96)
+    yt = torch.as_tensor(yk).cuda()
+    x1 = P.nufft_adj(yt, nufft_plan=gplan)
+    x2 = P.nufft_adj(yt, nufft_plan=gplan)
+    assert rel(x2, x1.cpu().numpy()) < 1e-6
+    x64 = orc.nufft_adj_f64(yk[:1].reshape(1, -1), oplan)
+    assert rel(x1[:1], x64) < 2e-5
