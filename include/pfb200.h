@@ -144,6 +144,13 @@ int pfb_plan_order(const pfb_plan *plan, int32_t *order, void *stream);
  * counterpart (its kernels never wait on asynchronous copies). */
 int pfb_plan_check(pfb_plan *plan, void *stream);
 
+/* Plans take their device memory from a library-owned pool per device that keeps
+ * the blocks destroyed plans give back (repeated plan builds, e.g. one per
+ * Pipe-Menon call, then allocate nothing from the driver).  Hand the kept blocks
+ * of `device` back to the driver; synchronises the device.  The reference has no
+ * counterpart (its plans are NumPy / CuPy arrays). */
+int pfb_release_cached_memory(int device);
+
 /* Workspace bytes for an apply over `nplanes` oversampled grid planes
  * (nplanes = nseg * batch * ncoeff).  May create the cuFFT plan. */
 int pfb_workspace_size(pfb_plan *plan, int64_t nplanes, size_t *bytes);

@@ -19,7 +19,7 @@ from ._dcf import pipe_menon_dcf
 from ._gram import GramMatrix, plan_spgram, sparse_gram
 from ._nufft import nufft, nufft_adj
 from ._preinterp import GrogPlan, grog_interp
-from ._plan import Interpolator, NUFFTPlan, plan_nufft
+from ._plan import Interpolator, NUFFTPlan, plan_nufft, release_cached_memory
 from ._sparsefft import FFTPlan, plan_spfft, sparse_fftn, sparse_ifftn
 from . import pipemenon  # noqa: E402  (module path of the reference: pyfourier.pipemenon)
 
@@ -29,5 +29,5 @@ __all__ = [
     "nufft", "nufft_adj", "plan_nufft", "NUFFTPlan", "Interpolator",
     "plan_spgram", "sparse_gram", "GramMatrix", "mri_exp_approx", "autotune", "pipe_menon_dcf",
     "pipemenon", "plan_spfft", "sparse_fftn", "sparse_ifftn", "FFTPlan", "plan_gram", "gram",
-    "grog_interp", "GrogPlan",
+    "grog_interp", "GrogPlan", "release_cached_memory",
 ]

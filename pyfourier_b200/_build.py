@@ -10,7 +10,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpfb200.so")
 SOURCES = ["pfb_capi.cu", "pfb_plan.cu", "pfb_spread.cu", "pfb_interp.cu", "pfb_glue.cu", "pfb_noalloc.cu", "pfb_fast.cu",
-           "pfb_fft.cu", "pfb_dcf.cu", "pfb_grog.cu", "pfb_psf.cu", "pfb_sort.cu"]
+           "pfb_fft.cu", "pfb_dcf.cu", "pfb_grog.cu", "pfb_psf.cu", "pfb_sort.cu", "pfb_pool.cu"]
 
 
 def nvcc_path():

@@ -35,7 +35,7 @@ EXPORTS = (
     "pfb_gram_workspace_size", "pfb_gram_apply", "pfb_nufft_adj_noalloc",
     "pfb_grog_create", "pfb_grog_destroy", "pfb_grog_workspace_size", "pfb_grog_apply",
     "pfb_apply_workspace_size", "pfb_nufft_traj_grad", "pfb_nufft_stage", "pfb_plan_order", "pfb_spread_f64",
-    "pfb_plan_check",
+    "pfb_plan_check", "pfb_release_cached_memory",
 )
 
 
@@ -107,6 +107,7 @@ def load(path=LIB_PATH):
         "pfb_plan_tables": (i32, [vp, i32, vp, vp, vp]),
         "pfb_plan_order": (i32, [vp, vp, vp]),
         "pfb_plan_check": (i32, [vp, vp]),
+        "pfb_release_cached_memory": (i32, [i32]),
         "pfb_workspace_size": (i32, [vp, i64, P(ctypes.c_size_t)]),
         "pfb_nufft_fwd": (i32, [vp, P(ApplyT), vp, vp, vp, ctypes.c_size_t, vp]),
         "pfb_nufft_adj": (i32, [vp, P(ApplyT), vp, vp, vp, ctypes.c_size_t, vp]),

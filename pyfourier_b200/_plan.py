@@ -27,6 +27,13 @@ def _as_tensor(x, dtype=None):
     return torch.as_tensor(np.asarray(x), dtype=dtype)
 
 
+def release_cached_memory(device=None):
+    """Hand the device memory kept from destroyed plans back to the driver (plans
+    allocate from a pool that keeps it for the next plan); synchronises the device."""
+    dev = resolve_device(device)
+    _lib.check(_lib.load().pfb_release_cached_memory(int(dev.index)))
+
+
 def resolve_device(device, fallback=None):
     """Map the reference's device argument ("cpu", "cuda:n", -1, n, None) to a CUDA device.
 

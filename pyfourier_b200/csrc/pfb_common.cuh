@@ -389,6 +389,13 @@ void free_owner_items(pfb_plan *p);
 // sort.cu: stable LSD counting sort of (int key, int value) pairs over the low
 // end_bit bits of the keys, keys in [0, 2^31); temp of counting_sort_temp_bytes(n)
 size_t counting_sort_temp_bytes(int64_t n);
+
+// Plan memory (pfb_pool.cu): blocks from a library-owned pool per device that keeps
+// what destroyed plans give back.  pool_alloc's block is usable on every stream when
+// it returns; pool_free is ordered on stream s (the caller orders s after the last
+// use, or synchronises the device first).
+int pool_alloc(void **p, size_t bytes);
+void pool_free(void *p, cudaStream_t s);
 int counting_sort_pairs(const int *keys, const int *vals, int *keys_out, int *vals_out, int64_t n, int end_bit,
                         void *temp, size_t temp_bytes, cudaStream_t s);
 

@@ -1078,12 +1078,9 @@ int fft_fused_ready(pfb_plan *p) {
     for (int a = 0; a < D; ++a)
         if (!make_axis(p->g.nos[a], &p->fft_ax[a], tw)) return 0;
     if (tw.empty()) tw.push_back(make_float2(1.f, 0.f));
-    if (cudaMalloc(&p->d_fft_tw, tw.size() * sizeof(float2)) != cudaSuccess) {
-        p->d_fft_tw = nullptr;
-        return 0;
-    }
+    if (pool_alloc(reinterpret_cast<void **>(&p->d_fft_tw), tw.size() * sizeof(float2)) != PFB_OK) return 0;
     if (cudaMemcpy(p->d_fft_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
-        cudaFree(p->d_fft_tw);
+        pool_free(p->d_fft_tw, 0);
         p->d_fft_tw = nullptr;
         return 0;
     }
@@ -1094,10 +1091,10 @@ int fft_fused_ready(pfb_plan *p) {
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&p->fft_nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         p->fft_nsm = 0;
-    if (cudaMalloc(&p->d_fft_err, sizeof(int)) != cudaSuccess) {
+    if (pool_alloc(reinterpret_cast<void **>(&p->d_fft_err), sizeof(int)) != PFB_OK) {
         p->d_fft_err = nullptr;
     } else if (cudaMemset(p->d_fft_err, 0, sizeof(int)) != cudaSuccess) {
-        cudaFree(p->d_fft_err);
+        pool_free(p->d_fft_err, 0);
         p->d_fft_err = nullptr;
     }
     p->fft_fused = 1;
@@ -1106,9 +1103,10 @@ int fft_fused_ready(pfb_plan *p) {
 
 void fft_fused_free(pfb_plan *p) {
     std::lock_guard<std::mutex> lk(p->fft_mu);
-    cudaFree(p->d_fft_tw);
+    // called with the device synchronised (plan destruction)
+    pool_free(p->d_fft_tw, 0);
     p->d_fft_tw = nullptr;
-    cudaFree(p->d_fft_err);
+    pool_free(p->d_fft_err, 0);
     p->d_fft_err = nullptr;
     p->fft_fused = -1;
 }

@@ -172,30 +172,26 @@ int default_tile(int ndim, int nos) {
 
 template <typename T>
 int dev_alloc(T **p, size_t count) {
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
-    if (e != cudaSuccess) {
-        *p = nullptr;
-        return fail(e == cudaErrorMemoryAllocation ? PFB_ERR_NOMEM : PFB_ERR_CUDA,
-                    std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    }
-    return PFB_OK;
+    return pool_alloc(reinterpret_cast<void **>(p), (count == 0 ? 1 : count) * sizeof(T));
 }
 
+// every apply of the plan has finished first (the device is synchronised, as
+// cudaFree would)
 void free_plan_buffers(pfb_plan *p) {
+    cudaDeviceSynchronize();
     for (int a = 0; a < kMaxDim; ++a) {
-        cudaFree(p->d_cos[a]);
-        cudaFree(p->d_apod[a]);
+        pool_free(p->d_cos[a], 0);
+        pool_free(p->d_apod[a], 0);
         p->d_cos[a] = p->d_apod[a] = nullptr;
     }
-    cudaFree(p->d_perm);
-    cudaFree(p->d_iperm);
+    pool_free(p->d_perm, 0);
+    pool_free(p->d_iperm, 0);
     p->d_iperm = nullptr;
-    cudaFree(p->d_sframe);
-    cudaFree(p->d_bin_start);
-    cudaFree(p->d_items_frame);
-    cudaFree(p->d_items_all);
-    cudaFree(p->d_frame_off);
+    pool_free(p->d_sframe, 0);
+    pool_free(p->d_bin_start, 0);
+    pool_free(p->d_items_frame, 0);
+    pool_free(p->d_items_all, 0);
+    pool_free(p->d_frame_off, 0);
     p->d_perm = p->d_sframe = p->d_bin_start = nullptr;
     p->d_items_frame = p->d_items_all = nullptr;
     p->d_frame_off = nullptr;
@@ -230,8 +226,9 @@ int rebuild_items(pfb_plan *p, int chunk) {
     std::vector<SpreadItem> a, b;
     build_items(p->bin_start, p->nbins_total, p->ncode, p->nframes, chunk, true, a);
     build_items(p->bin_start, p->nbins_total, p->ncode, p->nframes, chunk, false, b);
-    cudaFree(p->d_items_frame);
-    cudaFree(p->d_items_all);
+    if (p->d_items_frame || p->d_items_all) cudaDeviceSynchronize();  // applies in flight may read them
+    pool_free(p->d_items_frame, 0);
+    pool_free(p->d_items_all, 0);
     p->d_items_frame = p->d_items_all = nullptr;
     int st;
     if ((st = dev_alloc(&p->d_items_frame, a.size()))) return st;
@@ -335,13 +332,14 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
     int nkeys = (int)(nbins_total * p->ncode * nframes);
     const int T = 256;
 
+    // the temporaries go back in the order of the plan stream's work
     auto cleanup = [&](int code) {
-        cudaFree(d_cos_tmp);
-        cudaFree(d_keys);
-        cudaFree(d_vals);
-        cudaFree(d_keys_sorted);
-        cudaFree(d_bad);
-        cudaFree(d_temp);
+        pool_free(d_cos_tmp, stream);
+        pool_free(d_keys, stream);
+        pool_free(d_vals, stream);
+        pool_free(d_keys_sorted, stream);
+        pool_free(d_bad, stream);
+        pool_free(d_temp, stream);
         if (code != PFB_OK) {
             free_owner_items(p);
             free_plan_buffers(p);
@@ -391,7 +389,7 @@ int plan_create(const float *coord, int ndim, int nframes, const int64_t *frame_
         int end_bit = 1;
         while ((1LL << end_bit) < (long long)nkeys) ++end_bit;
         temp_bytes = counting_sort_temp_bytes(mtot);
-        PFB_TRY_CU(cudaMalloc(&d_temp, temp_bytes));
+        PFB_TRY_ST(pool_alloc(&d_temp, temp_bytes));
         PFB_TRY_ST(counting_sort_pairs(d_keys, d_vals, d_keys_sorted, p->d_perm, mtot, end_bit, d_temp, temp_bytes,
                                        stream));
         gather_sorted_kernel<<<blocks, T, 0, stream>>>(ndim, mtot, nframes, d_cos_tmp, p->d_perm, d_keys_sorted,

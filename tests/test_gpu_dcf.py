@@ -115,3 +115,25 @@ def test_dcf_multiframe_and_zero_iterations():
                        w4.cpu().numpy().reshape(coord.shape[:-1])) < TOL
     w0 = pf().pipe_menon_dcf(torch.as_tensor(coord), N, niter=0)
     assert torch.equal(w0, torch.ones_like(w0))
+
+
+def test_repeated_calls_reuse_pooled_plan_memory():
+    """Each call builds and destroys a plan; its device memory comes back from the
+    library's pool, so back-to-back calls do not grow the device's footprint, give
+    the same weights, and the kept blocks can be handed back.  One iteration: the
+    chaotic iteration amplifies the float-atomic ordering of the crowded tiles
+    (about 1e-3 after three iterations on this trajectory)."""
+    P = pf()
+    bench = pytest.importorskip("bench")
+    coord = bench.golden_means_radial_3d(3000, 128, 64)
+    w0 = P.pipe_menon_dcf(coord, 64, niter=1, device="cuda:0")
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    for _ in range(3):
+        w = P.pipe_menon_dcf(coord, 64, niter=1, device="cuda:0")
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info(0)[0]
+    assert abs(free1 - free0) < (32 << 20), (free0, free1)
+    assert rel(w, w0) < TOL
+    P.release_cached_memory("cuda:0")
+    assert torch.cuda.mem_get_info(0)[0] >= free1
