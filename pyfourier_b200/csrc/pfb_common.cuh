@@ -91,12 +91,22 @@ struct SpreadItem {
 
 // Work item of the owner-computes spread: output tile `tile` (of frame
 // `frame`, or all frames when < 0) gathers the samples of its 2^d lower
-// neighbour bins, virtual positions [v0, v1) of their concatenation.
-// atomic = 1 when the tile is split over several items (combined with
-// float2 atomics after the tile was zeroed).
+// neighbour bins, virtual positions of their concatenation (item_stride /
+// item_visits below).  atomic = the number of items when the tile is split
+// over several (combined with float2 atomics after the tile was zeroed), else 0.
 struct OwnerItem {
     int tile, frame, v0, v1, atomic;
 };
+
+// The visits of an owner item: v0, v0 + s, v0 + 2 s, ... below v1 with stride
+// s = atomic when the tile is split over atomic > 1 items (item r of a split tile
+// has v0 = r and v1 = the tile's visit count, so every item mixes all neighbour
+// ranges and all blocks of the tile get work), else s = 1.
+__host__ __device__ __forceinline__ int item_stride(const OwnerItem &it) { return it.atomic > 1 ? it.atomic : 1; }
+__host__ __device__ __forceinline__ int item_visits(const OwnerItem &it) {
+    const int s = item_stride(it);
+    return it.v1 > it.v0 ? (it.v1 - it.v0 + s - 1) / s : 0;
+}
 
 // Arguments describing the "channels" of an apply: coils (B), subspace
 // coefficients / frames (C), B0 segments (L).

@@ -827,8 +827,9 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) spread_il_kernel(const Spre
     if (warp == 0) neighbour_ranges<D>(P, it, s_pre, s_beg, s_dlt, lane);
     __syncthreads();
     constexpr int DW = D * WM;
-    // virtual index v in [it.v0, it.v1) over the concatenated neighbour ranges
-    for (int v = it.v0 + warp; v < it.v1; v += kSpreadWarps) {
+    // virtual index v over the concatenated neighbour ranges: it.v0, it.v0 + s, ...
+    const int vs = item_stride(it);
+    for (int v = it.v0 + warp * vs; v < it.v1; v += kSpreadWarps * vs) {
         // range r: the last one whose prefix is <= v (binary search; empty
         // ranges share their prefix with the next one and are skipped)
         int lo_r = 0, hi_r = NR;  // s_pre[lo_r] <= v < s_pre[hi_r]
@@ -1036,7 +1037,7 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
     }
     if (warp == 0) neighbour_ranges<3>(P, it, s_pre, s_beg, s_dlt, lane);
     __syncthreads();
-    const int nvis = it.v1 - it.v0;
+    const int nvis = item_visits(it), vs = item_stride(it);
     const int nbat = (nvis + C::Batch - 1) / C::Batch;
     auto batch_size = [&](int bb) { return (nvis - bb + nbat - 1) / nbat; };
     // issue the copies of batch bb into buffer buf.  A warp takes rounds of 32
@@ -1056,7 +1057,7 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
             if (q < nb) {
                 // batch bb takes visits bb, bb + nbat, bb + 2 nbat, ...: every batch
                 // mixes the neighbour ranges, so all warps find work in it
-                const int v = it.v0 + bb + q * nbat;
+                const int v = it.v0 + (bb + q * nbat) * vs;
                 // range: the last one whose prefix is <= v (empty ranges share the
                 // prefix of the next one and are skipped)
                 int lo = 0, hi = NR;
@@ -1307,7 +1308,7 @@ __global__ void __launch_bounds__(Reg2Cfg<CPW>::NW * 32, Reg2Cfg<CPW>::MinBlocks
     }
     if (warp == 0) neighbour_ranges<2>(P, it, s_pre, s_beg, s_dlt, lane);
     __syncthreads();
-    const int nvis = it.v1 - it.v0;
+    const int nvis = item_visits(it), vs = item_stride(it);
     const int nbat = (nvis + C::Batch - 1) / C::Batch;
     auto batch_size = [&](int bb) { return (nvis - bb + nbat - 1) / nbat; };
     auto issue = [&](int bb, int buf) {
@@ -1318,7 +1319,7 @@ __global__ void __launch_bounds__(Reg2Cfg<CPW>::NW * 32, Reg2Cfg<CPW>::MinBlocks
         int *rd = reinterpret_cast<int *>(B + C::OffD);
         const int nb = batch_size(bb);
         for (int q = warp; q < nb; q += NW) {
-            const int v = it.v0 + bb + q * nbat;  // batches mix the neighbour ranges
+            const int v = it.v0 + (bb + q * nbat) * vs;  // batches mix the neighbour ranges
             const unsigned le = __ballot_sync(0xffffffffu, lane < NR && s_pre[lane] <= v);
             const int r = 31 - __clz(le);
             const int64_t j = (int64_t)s_beg[r] + (v - s_pre[r]);
@@ -1974,8 +1975,11 @@ void owner_items_for(const pfb_plan *p, bool per_frame, int chunk, std::vector<O
             if (total <= chunk) {
                 items.push_back({t, fr, 0, (int)total, 0});
             } else {
-                for (long long v = 0; v < total; v += chunk)
-                    items.push_back({t, fr, (int)v, (int)std::min<long long>(total, v + chunk), 1});
+                // a crowded tile: S items, item r taking visits r, r + S, r + 2 S, ... (a
+                // contiguous piece would mostly be one neighbour range, whose samples
+                // reach only the blocks on that side of the tile)
+                const int S = (int)((total + chunk - 1) / chunk);
+                for (int r = 0; r < S; ++r) items.push_back({t, fr, r, (int)total, S});
                 zero.push_back({t, fr, 0, 0, 1});
             }
         }
