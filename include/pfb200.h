@@ -121,7 +121,7 @@ int pfb_plan_set_tuning(pfb_plan *plan, int spread_threads, int interp_threads,
                         int spread_channels);
 
 /* Maximum number of samples per spread work item (the split of crowded tiles),
- * in [1, 4096]. */
+ * in [1, 16384]. */
 int pfb_plan_set_chunk(pfb_plan *plan, int chunk);
 
 /* Materialise the reference's interpolator tables for one axis (0 = z ... in

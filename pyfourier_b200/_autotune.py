@@ -64,7 +64,8 @@ def default_candidates(ndim):
         tiles = [(16, 16), (24, 24), (32, 32), (16, 64)]
     else:
         tiles = [(64,), (256,), (1024,)]
-    return tiles, [1024, 2048, 4096]
+    # visits per spread work item (a crowded tile is split over interleaved items)
+    return tiles, ([2048, 4096, 8192] if ndim == 3 else [1024, 2048, 4096])
 
 
 def _time_pair(fwd, adj, iters):

@@ -224,7 +224,7 @@ int pfb_plan_set_tuning(pfb_plan *p, int spread_threads, int interp_threads, int
 }
 
 int pfb_plan_set_chunk(pfb_plan *p, int chunk) {
-    if (!p || chunk < 1 || chunk > 4096) return fail(PFB_ERR_INVALID, "chunk must be in [1, 4096]");
+    if (!p || chunk < 1 || chunk > 16384) return fail(PFB_ERR_INVALID, "chunk must be in [1, 16384]");
     DeviceGuard dg(p->device);
     int st = rebuild_items(p, chunk);
     if (st) return st;

@@ -40,4 +40,4 @@ def test_default_candidates():
     for ndim in (1, 2, 3):
         tiles, chunks = _autotune.default_candidates(ndim)
         assert tiles and all(len(t) == ndim and all(e >= 1 for e in t) for t in tiles)
-        assert chunks and all(1 <= c <= 4096 for c in chunks)  # pfb_plan_set_chunk's range
+        assert chunks and all(1 <= c <= 16384 for c in chunks)  # pfb_plan_set_chunk's range
