@@ -232,9 +232,34 @@ constexpr StagePlan stage_plan(int n) {
 // One Stockham stage with the radix, stage extent and butterfly count known at
 // compile time: the loop over butterflies unrolls, j = i mod ns and every
 // shared-memory index reduce to constants plus the thread's stream.
-template <int R, int NS, int M, int PITCH>
-__device__ __forceinline__ void fft_stage_c(const float2 *__restrict__ src, float2 *__restrict__ dst,
-                                            const float2 *__restrict__ tw, int stream, int cp) {
+// Source of a stage: position pos of the column pair cp as (col 2cp, col 2cp + 1).
+// Rows of PITCH float2, position-major (the layout every stage writes).
+template <int PITCH>
+struct PitchLoad {
+    const float2 *src;
+    __device__ __forceinline__ float4 operator()(int pos, int cp) const {
+        return *reinterpret_cast<const float4 *>(src + pos * PITCH + 2 * cp);
+    }
+};
+
+// Source of the first stage of an x pass: 16 rows (one per vector) of `pitch`
+// float2 as loaded from global memory (row-major); position pos holds element
+// x = (pos + rot) mod n of its row, zero where x >= len (the pruned input)
+struct RowMajorLoad {
+    const float2 *src;
+    int pitch, n, rot, len;
+    __device__ __forceinline__ float4 operator()(int pos, int cp) const {
+        int x = pos + rot;
+        if (x >= n) x -= n;
+        if (x >= len) return make_float4(0.f, 0.f, 0.f, 0.f);
+        const float2 a = src[(2 * cp) * pitch + x], b = src[(2 * cp + 1) * pitch + x];
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+};
+
+template <int R, int NS, int M, int PITCH, class L>
+__device__ __forceinline__ void fft_stage_cl(const L &ld, float2 *__restrict__ dst, const float2 *__restrict__ tw,
+                                             int stream, int cp) {
     constexpr int IT = (M + kPairStreams - 1) / kPairStreams;
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
@@ -244,7 +269,7 @@ __device__ __forceinline__ void fft_stage_c(const float2 *__restrict__ src, floa
         float2 a[R], b[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) {
-            const float4 v = *reinterpret_cast<const float4 *>(src + (i + q * M) * PITCH + 2 * cp);
+            const float4 v = ld(i + q * M, cp);
             a[q] = make_float2(v.x, v.y);
             b[q] = make_float2(v.z, v.w);
         }
@@ -264,6 +289,12 @@ __device__ __forceinline__ void fft_stage_c(const float2 *__restrict__ src, floa
             *reinterpret_cast<float4 *>(dst + (base + k * NS) * PITCH + 2 * cp) =
                 make_float4(a[k].x, a[k].y, b[k].x, b[k].y);
     }
+}
+
+template <int R, int NS, int M, int PITCH>
+__device__ __forceinline__ void fft_stage_c(const float2 *__restrict__ src, float2 *__restrict__ dst,
+                                            const float2 *__restrict__ tw, int stream, int cp) {
+    fft_stage_cl<R, NS, M, PITCH>(PitchLoad<PITCH>{src}, dst, tw, stream, cp);
 }
 
 template <int N, int S, int PITCH>
@@ -321,6 +352,35 @@ __device__ __forceinline__ float2 *fft_run(float2 *A, float2 *B, const FftAxis &
     }
     return src;
 }
+
+// Forward FFT of length N whose first stage reads its input through `ld` and
+// writes B; the later stages ping-pong between B and A (rows PITCH float2 apart).
+// Returns the buffer holding the result; ends with the CTA synchronised.
+template <int N, int PITCH, class L>
+__device__ __forceinline__ float2 *fft_run_first_n(const L &ld, float2 *A, float2 *B, const float2 *tw) {
+    constexpr StagePlan SP = stage_plan(N);
+    const int cp = threadIdx.x & (kCols / 2 - 1), stream = threadIdx.x / (kCols / 2);
+    fft_stage_cl<SP.radix[0], SP.ns[0], N / SP.radix[0], PITCH>(ld, B, tw + SP.twoff[0], stream, cp);
+    __syncthreads();
+    float2 *src = B, *dst = A;
+    fft_stages_c<N, 1, PITCH>(src, dst, tw, stream, cp);
+    return src;
+}
+
+// The same for the transform lengths with a compile-time stage plan; nullptr for
+// any other length (the caller only launches with those)
+template <int PITCH, class L>
+__device__ __forceinline__ float2 *fft_run_first(const L &ld, float2 *A, float2 *B, const FftAxis &fa) {
+    switch (fa.n) {
+        case 250: return fft_run_first_n<250, PITCH>(ld, A, B, fa.tw);
+        case 240: return fft_run_first_n<240, PITCH>(ld, A, B, fa.tw);
+        case 160: return fft_run_first_n<160, PITCH>(ld, A, B, fa.tw);
+        case 256: return fft_run_first_n<256, PITCH>(ld, A, B, fa.tw);
+        case 512: return fft_run_first_n<512, PITCH>(ld, A, B, fa.tw);
+        default: return nullptr;
+    }
+}
+bool first_stage_length(int n) { return n == 250 || n == 240 || n == 160 || n == 256 || n == 512; }
 
 // Transform along an outer axis (y or z) of 16 adjacent x positions.
 //   mode 0: buffer -> buffer; 1: image -> buffer (forward first pass: deapodisation,
@@ -759,6 +819,164 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (threadIdx.x == 0 && store_pending) bulk_wait_read0();
 }
 
+// ------------------------------------------------------------------------------------
+// x passes on TMA (row_tma_kernel).  A tile is 16 consecutive vectors (rows along x);
+// each row arrives by 2D tensor-map boxes, `pitch` float2 apart in shared memory, into
+// one slot of a two-slot ring while the previous tile transforms.  The first radix
+// stage reads that row-major layout (RowMajorLoad: the fftshift rotation and the zero
+// padding fold into its index) and writes the position-major layout of the later
+// stages.  Forward: rows of T (N0 long, [plane][kz][ky][x]) -> the interleaved grid,
+// the 16 vectors being 16 consecutive channels of one (group, kz, ky), stored by TMA
+// as boxes of 16 channels x kx (rows 16 float2 wide).  Adjoint: rows of the planar
+// grid (n long) -> rows of T cropped to N0, read back reversed (IDFT(x)[k] =
+// DFT(x)[(n - k) mod n], no conjugation) from rows of 18 float2 (conflict-free column
+// reads) and stored coalesced along x.
+// ------------------------------------------------------------------------------------
+struct RowTma {
+    FftAxis fa;
+    int N0, len, rot;   // input row length; first-stage rotation (forward N0 / 2, adjoint 0)
+    int hn;             // adjoint crop rotation (N0 / 2)
+    int nvec, ntiles;
+    int nch, nos1, nos2;
+    int pitch;          // x extent of the load box = float2 between the loaded rows (>= len;
+                        // the columns past len are zero-filled)
+    int nsbox, sbr;     // forward stores: boxes along kx and rows per box (last box overlapping)
+    int slot;           // float2 per ring slot
+    float2 *dst;        // adjoint output
+    int *err;
+};
+
+__device__ __forceinline__ void tma_load2(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(kThreads, 2)
+    row_tma_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
+                   const RowTma P) {
+    constexpr int PITCH = INV ? kPitch : kTmaPitch;
+    extern __shared__ __align__(128) float2 tsm[];
+    __shared__ __align__(8) uint64_t full[2];
+    const int n = P.fa.n;
+    float2 *scr = tsm + 2 * P.slot;
+    // thread 0: load tile t into slot s as one box of 16 rows of P.pitch (rows past the
+    // last vector and columns past the row length are zero-filled).  A tensor copy's
+    // shared-memory destination must be 128-byte aligned: the slots are; a slot that
+    // is not (never by construction) sets the error flag and is not loaded
+    auto issue = [&](int t, int s) {
+        float2 *dst = tsm + s * P.slot;
+        const int u0 = t * kCols;
+        if (smem_u32(dst) & 127u) {
+            atomicExch(P.err, 1);
+            mbar_expect_tx(&full[s], 0);
+            return;
+        }
+        mbar_expect_tx(&full[s], (unsigned)(kCols * P.pitch * sizeof(float2)));
+        if (INV) {
+            tma_load2(dst, &src_map, 0, u0, &full[s]);  // 16 consecutive rows of the planar grid
+        } else {
+            // 16 consecutive channels of one (group, kz, ky): planes grp nch + chn0 ..
+            const int chn0 = u0 % P.nch;
+            int r = u0 / P.nch;
+            const int ky = r % P.nos1;
+            r /= P.nos1;
+            const int kz = r % P.nos2, grp = r / P.nos2;
+            tma_load3(dst, &src_map, 0, kz * P.nos1 + ky, grp * P.nch + chn0, &full[s]);
+        }
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; ++s) {
+            const int t = blockIdx.x + s * gridDim.x;
+            if (t < P.ntiles) issue(t, s);
+        }
+    }
+    int k = 0;
+    bool store_pending = false;  // thread 0: a TMA store of the scratch buffer may still be reading it
+    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++k) {
+        const int s = k & 1;
+        bool ok = mbar_wait(&full[s], (k >> 1) & 1);
+        float2 *S = tsm + s * P.slot;
+        if (threadIdx.x == 0 && store_pending) {
+            bulk_wait_read0();
+            store_pending = false;
+        }
+        ok = __syncthreads_and(ok);
+        if (!ok) {
+            if (threadIdx.x == 0) {
+                atomicExch(P.err, 1);
+                if (t + (int)gridDim.x < P.ntiles) mbar_wait(&full[s ^ 1], ((k + 1) >> 1) & 1);
+                if (store_pending) bulk_wait_read0();
+            }
+            return;
+        }
+        const RowMajorLoad ld{S, P.pitch, n, P.rot, P.len};
+        const float2 *R = fft_run_first<PITCH>(ld, S, scr, P.fa);
+        const int u0 = t * kCols;
+        const int tn = t + 2 * gridDim.x;
+        if (!INV) {
+            // rows kx of the result are 16 channels of point (kz, ky, kx): TMA store
+            fence_async_smem();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                const int chn0 = u0 % P.nch;
+                int r = u0 / P.nch;
+                const int ky = r % P.nos1;
+                r /= P.nos1;
+                const int kz = r % P.nos2, grp = r / P.nos2;
+                for (int b = 0; b < P.nsbox; ++b) {
+                    const int r0 = b + 1 < P.nsbox ? b * P.sbr : n - P.sbr;
+                    tma_store4(&dst_map, chn0, r0, kz * P.nos1 + ky, grp, R + r0 * PITCH);
+                }
+                bulk_commit();
+                // refill the slot now unless the store reads it; a store of the scratch
+                // buffer is waited for before the next transform
+                if (R == S) bulk_wait_read0();
+                else store_pending = true;
+                if (tn < P.ntiles) issue(tn, s);
+            }
+            continue;
+        }
+        // adjoint: element x < N0 of vector v is inverse-transform position
+        // pp = (x - hn) mod n, i.e. forward position (n - pp) mod n
+        {
+            const int v = threadIdx.x >> 4, lx = threadIdx.x & 15;
+            const int u = u0 + v;
+            if (u < P.nvec) {
+                float2 *d = P.dst + (int64_t)u * P.N0;
+                for (int x = lx; x < P.N0; x += 16) {
+                    int pp = x - P.hn;
+                    if (pp < 0) pp += n;
+                    const int q = pp == 0 ? 0 : n - pp;
+                    d[x] = R[q * PITCH + v];
+                }
+            }
+        }
+        // the slot and the scratch buffer are read; the generic accesses are ordered
+        // before the slot's next TMA load
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0 && tn < P.ntiles) issue(tn, s);
+    }
+    if (threadIdx.x == 0 && store_pending) bulk_wait_read0();
+}
+
 // Transform along x.  Forward: rows of T (N0 long, [plane][kz][ky][x]) -> the
 // interleaved grid [grp][point][ch]; the 16 vectors of a CTA are consecutive
 // (grp, kz, ky, ch) with ch fastest, so a half-warp stores 16 channels of one
@@ -772,6 +990,8 @@ struct RowPass {
     int64_t gvol;
     const float2 *src;
     float2 *dst;
+    int *err;  // device flag of the plan (TMA form: a wait that gave up)
+    int nsm;   // SMs of the device (TMA form: persistent grid)
 };
 
 __global__ void __launch_bounds__(kThreads) row_fwd_kernel(const RowPass P) {
@@ -1054,9 +1274,103 @@ int launch_col(const ColPass &P, cudaStream_t s) {
     return PFB_OK;
 }
 
+// Tiled tensor map over 8-byte elements (complex64 as one element): rank dims
+// (innermost first), rank - 1 byte strides, a box per dimension.  Rows past an
+// extent read as zeros.
+bool encode_map8(CUtensorMap *m, const void *base, int rank, const cuuint64_t *dim, const cuuint64_t *stride,
+                 const cuuint32_t *box) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn || rank < 1 || rank > 5) return false;
+    for (int i = 0; i < rank - 1; ++i)
+        if (stride[i] == 0 || stride[i] % 16 != 0 || stride[i] >= (1ull << 40)) return false;
+    for (int i = 0; i < rank; ++i)
+        if (dim[i] == 0 || box[i] == 0 || box[i] > 256) return false;
+    if ((box[0] * 8) % 16 != 0) return false;
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_INT64, (cuuint32_t)rank, const_cast<void *>(base), dim, stride, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The x pass on TMA when the layout allows it (a transform length with a
+// compile-time stage plan, even row lengths, 16-byte aligned bases, 32-bit vector
+// indices; forward: a multiple of 16 channels); returns 1 if launched, 0 to take
+// the copy-based kernel, or an error.
+int launch_row_tma(const RowPass &P, bool inv, cudaStream_t s) {
+    const int n = P.fa.n;
+    if (!P.err || P.nsm <= 0 || !first_stage_length(n) || P.N0 % 2 != 0 || n % 2 != 0) return 0;
+    if (P.nvec <= 0 || P.nvec >= (1LL << 31) - (int64_t)kCols * 4 * P.nsm) return 0;
+    if (!inv && (P.nch % kCols != 0)) return 0;
+    auto a16 = [](const void *q) { return ((uintptr_t)q & 15u) == 0; };
+    if (!a16(P.src) || !a16(P.dst)) return 0;
+    RowTma T{};
+    T.fa = P.fa;
+    T.N0 = P.N0;
+    T.len = inv ? n : P.N0;
+    T.rot = inv ? 0 : P.N0 / 2;
+    T.hn = P.N0 / 2;
+    T.nvec = (int)P.nvec;
+    T.ntiles = (int)((P.nvec + kCols - 1) / kCols);
+    T.nch = P.nch;
+    T.nos1 = P.nos1;
+    T.nos2 = P.nos2;
+    // one box per tile, x extent = row pitch >= the row length with pitch = 2 (mod 8):
+    // the first stage's column reads (8 column pairs x 4 positions per warp) then touch
+    // each bank at most twice; a box is at most 256 wide
+    T.pitch = T.len;
+    while (T.pitch % 8 != 2) ++T.pitch;
+    if (T.pitch > 256) return 0;
+    const int pitch_out = inv ? kPitch : kTmaPitch;
+    T.slot = std::max(kCols * T.pitch, n * pitch_out);
+    T.slot = (T.slot + 15) / 16 * 16;  // 128-byte aligned slots
+    T.dst = P.dst;
+    T.err = P.err;
+    CUtensorMap smap, dmap;
+    if (inv) {
+        // rows of the planar grid, 16 consecutive ones per tile
+        const cuuint64_t dim[2] = {(cuuint64_t)n, (cuuint64_t)P.nvec};
+        const cuuint64_t str[1] = {(cuuint64_t)n * 8};
+        const cuuint32_t box[2] = {(cuuint32_t)T.pitch, (cuuint32_t)kCols};
+        if (!encode_map8(&smap, P.src, 2, dim, str, box)) return 0;
+    } else {
+        // rows of T: x, row (kz, ky) of a plane, plane (group, channel); 16 planes per tile
+        const int64_t planes = P.nvec / ((int64_t)P.nos1 * P.nos2);
+        const cuuint64_t dim[3] = {(cuuint64_t)P.N0, (cuuint64_t)P.nos2 * P.nos1, (cuuint64_t)planes};
+        const cuuint64_t str[2] = {(cuuint64_t)P.N0 * 8, (cuuint64_t)P.N0 * P.nos2 * P.nos1 * 8};
+        const cuuint32_t box[3] = {(cuuint32_t)T.pitch, 1, (cuuint32_t)kCols};
+        if (!encode_map8(&smap, P.src, 3, dim, str, box)) return 0;
+    }
+    if (!inv) {
+        T.sbr = n <= 256 ? n : 256;
+        T.nsbox = (n + T.sbr - 1) / T.sbr;
+        const int64_t ngrp = P.nvec / ((int64_t)P.nch * P.nos1 * P.nos2);
+        const cuuint64_t dim[4] = {(cuuint64_t)P.nch, (cuuint64_t)n, (cuuint64_t)P.nos2 * P.nos1, (cuuint64_t)ngrp};
+        const cuuint64_t str[3] = {(cuuint64_t)P.nch * 8, (cuuint64_t)n * P.nch * 8, (cuuint64_t)P.gvol * P.nch * 8};
+        const cuuint32_t box[4] = {(cuuint32_t)kCols, (cuuint32_t)T.sbr, 1, 1};
+        if (!encode_map8(&dmap, P.dst, 4, dim, str, box)) return 0;
+    } else {
+        dmap = smap;  // not read
+    }
+    const size_t smem = (size_t)3 * T.slot * sizeof(float2);
+    auto k = inv ? row_tma_kernel<true> : row_tma_kernel<false>;
+    PFB_RAISE_SMEM(k, (int)smem);
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem) != cudaSuccess || per_sm < 1)
+        return 0;
+    const int grid = (int)std::min<int64_t>(T.ntiles, (int64_t)P.nsm * per_sm);
+    k<<<grid, kThreads, smem, s>>>(smap, dmap, T);
+    PFB_CHECK_LAUNCH();
+    return 1;
+}
+
 int launch_row(const RowPass &P, bool inv, cudaStream_t s) {
     const int64_t blocks = (P.nvec + kCols - 1) / kCols;
     if (blocks == 0) return PFB_OK;
+    {
+        const int st = launch_row_tma(P, inv, s);
+        if (st == 1) return PFB_OK;
+        if (st != 0) return st;
+    }
     if (blocks >= (1LL << 31)) return fail(PFB_ERR_UNSUPPORTED, "too many vectors for the fused FFT");
     const size_t smem = row_smem(P.fa.n);
     auto k = inv ? row_inv_kernel : row_fwd_kernel;
@@ -1186,6 +1500,8 @@ int fft_fused_fwd(pfb_plan *p, int pass, const Chan &c, int C, const float2 *img
     }
     // x pass: gridp rows -> interleaved grid
     RowPass R{};
+    R.err = p->d_fft_err;
+    R.nsm = p->fft_nsm;
     R.fa = p->fft_ax[0];
     R.N0 = (int)N0;
     R.nch = c.nch;
@@ -1207,6 +1523,8 @@ int fft_fused_adj(pfb_plan *p, int pass, const Chan &c, int C, float2 *img, cons
     if (pass == 0) {
         // x pass: planar grid rows -> gridi, cropped to N0
         RowPass R{};
+        R.err = p->d_fft_err;
+        R.nsm = p->fft_nsm;
         R.fa = p->fft_ax[0];
         R.N0 = (int)N0;
         R.nos1 = (int)n1;
