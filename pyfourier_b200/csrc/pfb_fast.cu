@@ -249,8 +249,16 @@ struct SampIL {
     float2 *dst;        // vals_il: vals [M][nch];   out_il: k-space (B, M)
     int factors;        // vals_il: apply conj(tB) conj(basis) (1) or only the weight (0)
     int accumulate;
-    int rows;           // samples per CTA (kOutRows .. kMaxOutRows)
+    int rows;           // samples per CTA (kOutRows .. kMaxOutRows, a power of two)
+    int lrows;          // log2(rows)
+    unsigned m_nch, m_kc, m_b;  // reciprocals for fdiv by nch, K (or 1) and B
 };
+
+// floor(e / d) for 0 <= e < 2^32 / d as a multiply-high by M = ceil(2^32 / d)
+// (magic_of(d); M = 0 stands for d = 1): the index splits of the transposes need no
+// integer division
+__device__ __forceinline__ int fdiv(int e, unsigned M) { return M ? (int)__umulhi((unsigned)e, M) : e; }
+inline unsigned magic_of(int d) { return d <= 1 ? 0u : (unsigned)((0x100000000ull + (unsigned)d - 1) / (unsigned)d); }
 
 constexpr int kMaxOutRows = 128;
 
@@ -260,6 +268,16 @@ inline int out_rows(int width) {
     int r = kOutRows;
     while (r < kMaxOutRows && (size_t)(2 * r) * width * sizeof(float2) <= 32 * 1024) r *= 2;
     return r;
+}
+
+// the rows and reciprocals of a transpose of `width` float2 per sample (O.ch set)
+inline void set_samp_rows(SampIL &O, int width) {
+    O.rows = out_rows(width);
+    O.lrows = 0;
+    while ((1 << O.lrows) < O.rows) ++O.lrows;
+    O.m_nch = magic_of(O.ch.nch);
+    O.m_kc = magic_of(O.ch.K ? O.ch.K : 1);
+    O.m_b = magic_of(O.ch.B);
 }
 
 // Both transposes walk the samples in their original order, P.rows per CTA, so
@@ -275,7 +293,7 @@ __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
     const int B = P.ch.B, SP = B | 1;  // odd row pitch: a warp's column accesses hit distinct banks
     for (int gg = threadIdx.x; gg < R; gg += blockDim.x) s_j[gg] = g0 + gg < P.mtot ? P.iperm[g0 + gg] : 0;
     for (int e = threadIdx.x; e < R * B; e += blockDim.x) {
-        const int b = e / R, gg = e - b * R;
+        const int b = e >> P.lrows, gg = e & (R - 1);
         const int64_t g = g0 + gg;
         float2 v = make_float2(0.f, 0.f);
         if (g < P.mtot) {
@@ -291,11 +309,11 @@ __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
     __syncthreads();
     const int nch = P.ch.nch, Kc = P.ch.K ? P.ch.K : 1;
     for (int e = threadIdx.x; e < R * nch; e += blockDim.x) {
-        const int gg = e / nch, c = e - gg * nch;
+        const int gg = fdiv(e, P.m_nch), c = e - gg * nch;
         const int64_t g = g0 + gg;
         if (g >= P.mtot) continue;
         const int64_t j = s_j[gg];
-        const int k = c % Kc, lb = c / Kc, b = lb % B, l = lb / B;
+        const int lb = fdiv(c, P.m_kc), k = c - lb * Kc, l = fdiv(lb, P.m_b), b = lb - l * B;
         float2 v = sm[gg * SP + b];
         if (P.factors && (P.tB || P.ch.K)) {
             const int f = P.sframe[j];
@@ -319,14 +337,14 @@ __global__ void __launch_bounds__(256) out_il_kernel(const SampIL P) {
     for (int gg = threadIdx.x; gg < R; gg += blockDim.x) s_j[gg] = g0 + gg < P.mtot ? P.iperm[g0 + gg] : 0;
     __syncthreads();
     for (int e = threadIdx.x; e < R * nch; e += blockDim.x) {
-        const int gg = e / nch, c = e - gg * nch;
+        const int gg = fdiv(e, P.m_nch), c = e - gg * nch;
         const int64_t g = g0 + gg;
         sm[gg * SP + c] = g < P.mtot ? P.src[(int64_t)s_j[gg] * nch + c] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     const int B = P.ch.B, L = P.ch.L, Kc = P.ch.K ? P.ch.K : 1;
     for (int e = threadIdx.x; e < R * B; e += blockDim.x) {
-        const int b = e / R, gg = e - b * R;
+        const int b = e >> P.lrows, gg = e & (R - 1);
         const int64_t g = g0 + gg;
         if (g >= P.mtot) continue;
         float2 acc = make_float2(0.f, 0.f);
@@ -1775,7 +1793,7 @@ int fast_stage(pfb_plan *p, const ApplyDesc &d, int stage, const void *src, void
             O.tB = d.b0_time;
             O.ch = c;
             O.accumulate = accumulate ? 1 : 0;
-            O.rows = out_rows(std::max(c.nch, c.B));
+            set_samp_rows(O, std::max(c.nch, c.B));
             const unsigned blocks = (unsigned)((p->mtot + O.rows - 1) / O.rows);
             if (stage == PFB_STAGE_OUT) {
                 O.src = samp;
@@ -1905,7 +1923,7 @@ int fast_traj_grad(pfb_plan *p, const ApplyDesc &d, const float2 *img, const flo
     V.src = vals;
     V.dst = samp;
     V.factors = 0;
-    V.rows = out_rows(std::max(c.nch, c.B));
+    set_samp_rows(V, std::max(c.nch, c.B));
     size_t smem = (size_t)V.rows * (c.B | 1) * sizeof(float2);
     PFB_RAISE_SMEM(vals_il_kernel, (int)smem);
     vals_il_kernel<<<(unsigned)((p->mtot + V.rows - 1) / V.rows), 256, smem, s>>>(V);
