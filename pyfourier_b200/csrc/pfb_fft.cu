@@ -660,7 +660,11 @@ struct TileInfo {
 
 // src_map: the pass's source as 4D (2X floats, rows, mid, source plane); dst_map:
 // the destination of forward passes (2X floats, n rows, mid, plane).
-__global__ void __launch_bounds__(kThreads, 2)
+// NSLOT ring slots: 2 (the next tile loads while this one transforms; 2 CTAs per
+// SM) or 1 (3 CTAs per SM overlap instead: slower, 1.30 against 1.21 ms for the
+// 200^3 z pass, 1.45 against 1.21 ms for the y pass)
+template <int NSLOT>
+__global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
     col_tma_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
                    const ColTma P) {
     extern __shared__ __align__(128) float2 tsm[];
@@ -668,7 +672,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     __shared__ TileInfo info[2];
     const int n = P.fa.n;
     // slot s of the ring at tsm + s * n rows, the transform's scratch buffer after them
-    float2 *scr = tsm + 2 * n * kTmaPitch;
+    float2 *scr = tsm + NSLOT * n * kTmaPitch;
     const int col = (threadIdx.x % (kCols / 2)) * 2, stream = threadIdx.x / (kCols / 2);
     constexpr int NS = kThreads * 2 / kCols;  // row streams: a thread moves two adjacent columns
     const unsigned box_bytes = (unsigned)P.br * kTmaPitch * sizeof(float2);
@@ -701,7 +705,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int s = 0; s < 2; ++s) {
+        for (int s = 0; s < NSLOT; ++s) {
             const int t = blockIdx.x + s * gridDim.x;
             if (t < P.ntiles) issue(t, s);
         }
@@ -709,8 +713,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     int k = 0;
     bool store_pending = false;  // thread 0: a TMA store of the scratch buffer may still be reading it
     for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++k) {
-        const int s = k & 1;
-        bool ok = mbar_wait(&full[s], (k >> 1) & 1);
+        const int s = NSLOT == 1 ? 0 : k & 1;
+        bool ok = mbar_wait(&full[s], (NSLOT == 1 ? k : k >> 1) & 1);
         const TileInfo ti = info[s];
         float2 *A = tsm + s * n * kTmaPitch;
         const int x = ti.xc * kCols + col;
@@ -755,13 +759,13 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (threadIdx.x == 0) {
                 atomicExch(P.err, 1);
                 // the other slot's load, if one is in flight
-                if (t + (int)gridDim.x < P.ntiles) mbar_wait(&full[s ^ 1], ((k + 1) >> 1) & 1);
+                if (NSLOT == 2 && t + (int)gridDim.x < P.ntiles) mbar_wait(&full[s ^ 1], ((k + 1) >> 1) & 1);
                 if (store_pending) bulk_wait_read0();
             }
             return;
         }
         const float2 *R = fft_run<kTmaPitch>(A, scr, P.fa);
-        const int tn = t + 2 * gridDim.x;  // the tile after next, for this slot
+        const int tn = t + NSLOT * gridDim.x;  // the next tile for this slot
         if (fwd_store) {
             // rows 0..n-1 of the result are the output rows: TMA store from shared memory
             fence_async_smem();
@@ -1238,14 +1242,15 @@ int launch_col_tma(const ColPass &P, int64_t ntiles, cudaStream_t s) {
     } else {
         dmap = smap;  // not read
     }
-    const size_t smem = (size_t)3 * n * kTmaPitch * sizeof(float2);
-    PFB_RAISE_SMEM(col_tma_kernel, (int)smem);
+    constexpr int kSlots = 2;
+    const size_t smem = (size_t)(kSlots + 1) * n * kTmaPitch * sizeof(float2);
+    auto kern = col_tma_kernel<kSlots>;
+    PFB_RAISE_SMEM(kern, (int)smem);
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, col_tma_kernel, kThreads, smem) != cudaSuccess ||
-        per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem) != cudaSuccess || per_sm < 1)
         return 0;
     const int64_t grid = std::min<int64_t>(ntiles, (int64_t)P.nsm * per_sm);
-    col_tma_kernel<<<(unsigned)grid, kThreads, smem, s>>>(smap, dmap, T);
+    kern<<<(unsigned)grid, kThreads, smem, s>>>(smap, dmap, T);
     PFB_CHECK_LAUNCH();
     return 1;
 }
