@@ -1166,7 +1166,7 @@ def extra_workload(args):
 # the 128^3 / 32-coil variant (0.947 + 1.001 GB for 32 x 2.048 M samples) scaled by
 # the samples processed (x 3.906) to the 200^3 / 8 M-sample workload; the capture
 # and its command are summarised under profiles/.
-NCU_TRAFFIC = {("cfg2", "spread"): int(1.948e9 * 3.906)}
+NCU_TRAFFIC = {("cfg2", "spread"): int(1.927e9 * 3.906)}
 
 
 def main():
