@@ -476,7 +476,34 @@ __device__ __forceinline__ void build_tap_list(const InterpIL &P, const float *s
     }
 }
 
-template <int D, int WM, bool WIDE>
+// Per-sample x rows of a 4-wide kernel box in the warp's shared memory, one row per
+// (y, z) tap pair: the row's offset (the y and z parts of the tap offset, scaled like
+// build_tap_list's) and its weight w_y * w_z as a (w, w) pair.  Lanes < rows build
+// one row each.  With the four x taps' offsets and weights in registers, the gather
+// reads 12 bytes of shared memory per row of four taps instead of 12 bytes per tap.
+template <int D, bool WIDE>
+__device__ __forceinline__ void build_rows(const InterpIL &P, const float *sw, const int *sp, int nch,
+                                           int *s_roff, float2 *s_rw, int lane) {
+    constexpr int WM = 4, NR = D == 3 ? 16 : 4;
+    if (lane < NR) {
+        const int iy = lane & 3, iz = lane >> 2;
+        const bool ok = iy < P.g.w[1] && (D < 3 || iz < P.g.w[2]);
+        float w = 0.f;
+        int off = 0;
+        if (ok) {
+            w = sw[WM + iy] * (D > 2 ? sw[2 * WM + iz] : 1.f);
+            off = sp[WM + iy] * P.g.nos[0] + (D > 2 ? sp[2 * WM + iz] * (P.g.nos[0] * P.g.nos[1]) : 0);
+            if (!WIDE) off *= nch;
+        }
+        s_roff[lane] = off;
+        s_rw[lane] = make_float2(w, w);
+    }
+}
+
+// XROWS: the launch has one channel per lane (channel chunks of 32) and a box 4
+// taps wide in 2D or 3D; the kernel then takes the x-row form and keeps no
+// per-tap list.
+template <int D, int WM, bool WIDE, bool XROWS>
 __global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const InterpIL P) {
     constexpr int NT = ipow<D>(WM);
     // up to 64 taps the weights are kept as (w, w) pairs for FFMA2 and, with one
@@ -484,11 +511,17 @@ __global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const Int
     constexpr bool PAIRS = NT <= 64;
     constexpr bool VEC = PAIRS && NT % 4 == 0;
     constexpr bool VEC16 = PAIRS && NT % 16 == 0;
+    constexpr bool ROWS = XROWS && PAIRS && WM == 4 && D >= 2;
+    static_assert(ROWS || !XROWS, "the x-row form needs a 2D / 3D box 4 taps wide");
+    constexpr int NR = ROWS ? NT / 4 : 4;    // x rows of the box
+    constexpr int NL = ROWS ? 4 : NT;        // entries of the per-tap list
     using WT = typename std::conditional<PAIRS, float2, float>::type;
-    __shared__ float s_w[kTileWarps][3 * WM];
-    __shared__ int s_p[kTileWarps][3 * WM];
-    __shared__ __align__(16) int s_off[kTileWarps][NT];
-    __shared__ __align__(16) WT s_wt[kTileWarps][NT];
+    __shared__ __align__(16) float s_w[kTileWarps][3 * WM];
+    __shared__ __align__(16) int s_p[kTileWarps][3 * WM];
+    __shared__ __align__(16) int s_off[kTileWarps][NL];
+    __shared__ __align__(16) WT s_wt[kTileWarps][NL];
+    __shared__ __align__(16) int s_roff[kTileWarps][NR];
+    __shared__ __align__(16) float2 s_rw[kTileWarps][NR];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cw = P.cw, lcw = log2i(cw), tg_n = 32 >> lcw;
     const int cl = lane & (cw - 1), tg = lane >> lcw;
@@ -522,12 +555,55 @@ __global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const Int
         fetch(j + kTileWarps);
         __syncwarp();
         const float2 *G = P.grid + (int64_t)grp * P.g.gvol * nch;
-        build_tap_list<D, WM, WIDE>(P, s_w[warp], s_p[warp], nch, s_off[warp], s_wt[warp], lane);
+        if constexpr (ROWS)
+            build_rows<D, WIDE>(P, s_w[warp], s_p[warp], nch, s_roff[warp], s_rw[warp], lane);
+        else
+            build_tap_list<D, WM, WIDE>(P, s_w[warp], s_p[warp], nch, s_off[warp], s_wt[warp], lane);
         __syncwarp();
         for (int c0 = 0; c0 < nch; c0 += cw) {
             const int c = c0 + cl;
             const float2 *Gc = G + (c < nch ? c : nch - 1);  // in-bounds address; result discarded
             float2 acc = make_float2(0.f, 0.f);
+            if constexpr (ROWS) {
+                // x taps in registers; 4 rows (16 gathers) in flight, each row summed
+                // over x first, then scaled by its w_y * w_z
+                const float4 wx4 = *reinterpret_cast<const float4 *>(s_w[warp]);
+                const int4 px4 = *reinterpret_cast<const int4 *>(s_p[warp]);
+                const int w0 = P.g.w[0];
+                const float wx1 = w0 > 1 ? wx4.y : 0.f, wx2 = w0 > 2 ? wx4.z : 0.f, wx3 = w0 > 3 ? wx4.w : 0.f;
+                const float2 wx[4] = {make_float2(wx4.x, wx4.x), make_float2(wx1, wx1), make_float2(wx2, wx2),
+                                      make_float2(wx3, wx3)};
+                const int ox[4] = {WIDE ? px4.x : px4.x * nch, WIDE ? px4.y : px4.y * nch,
+                                   WIDE ? px4.z : px4.z * nch, WIDE ? px4.w : px4.w * nch};
+                const int4 *ro4 = reinterpret_cast<const int4 *>(s_roff[warp]);
+#pragma unroll
+                for (int rb = 0; rb < NR / 4; ++rb) {
+                    const int4 o = ro4[rb];
+                    const int oo[4] = {o.x, o.y, o.z, o.w};
+                    float2 v[16];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+#ifdef PFB_INTERP_ROWPTR
+                        const float2 *Gr = WIDE ? Gc + (int64_t)oo[q] * nch : Gc + oo[q];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            v[4 * q + u] = WIDE ? __ldg(Gr + (int64_t)ox[u] * nch) : __ldg(Gr + ox[u]);
+#else
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            v[4 * q + u] = WIDE ? __ldg(Gc + ((int64_t)oo[q] + ox[u]) * nch) : __ldg(Gc + oo[q] + ox[u]);
+#endif
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float2 sr = __fmul2_rn(wx[0], v[4 * q]);
+                        sr = __ffma2_rn(wx[1], v[4 * q + 1], sr);
+                        sr = __ffma2_rn(wx[2], v[4 * q + 2], sr);
+                        sr = __ffma2_rn(wx[3], v[4 * q + 3], sr);
+                        acc = __ffma2_rn(s_rw[warp][4 * rb + q], sr, acc);
+                    }
+                }
+            } else {
             if (VEC16 && tg_n == 1) {
                 // 16 gathers issued before their sums (more loads in flight per warp);
                 // taps summed in order 0, 1, 2, ...: the same sums as the loops below
@@ -579,6 +655,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const Int
                     else
                         acc = cfma(s_wt[warp][t], v, acc);
                 }
+            }
             }
             // reduce over tap groups (lanes that share the channel)
             for (int off = cw; off < 32; off <<= 1) {
@@ -1517,8 +1594,16 @@ template <int D, int WM>
 int launch_interp_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
     // element offsets point * nch in 32 bits when the grid allows it
     const bool wide = P.g.gvol * (int64_t)P.ch.nch >= (1LL << 31);
-    if (!wide) interp_il_kernel<D, WM, false><<<blocks, kTileWarps * 32, 0, s>>>(P);
-    else interp_il_kernel<D, WM, true><<<blocks, kTileWarps * 32, 0, s>>>(P);
+    if constexpr (WM == 4 && D >= 2) {
+        if (P.cw == 32) {  // one channel per lane: the x-row form
+            if (!wide) interp_il_kernel<D, WM, false, true><<<blocks, kTileWarps * 32, 0, s>>>(P);
+            else interp_il_kernel<D, WM, true, true><<<blocks, kTileWarps * 32, 0, s>>>(P);
+            PFB_CHECK_LAUNCH();
+            return PFB_OK;
+        }
+    }
+    if (!wide) interp_il_kernel<D, WM, false, false><<<blocks, kTileWarps * 32, 0, s>>>(P);
+    else interp_il_kernel<D, WM, true, false><<<blocks, kTileWarps * 32, 0, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
 }
