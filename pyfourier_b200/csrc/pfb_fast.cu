@@ -479,8 +479,9 @@ __device__ __forceinline__ void build_tap_list(const InterpIL &P, const float *s
 // Per-sample x rows of a 4-wide kernel box in the warp's shared memory, one row per
 // (y, z) tap pair: the row's offset (the y and z parts of the tap offset, scaled like
 // build_tap_list's) and its weight w_y * w_z as a (w, w) pair.  Lanes < rows build
-// one row each.  With the four x taps' offsets and weights in registers, the gather
-// reads 12 bytes of shared memory per row of four taps instead of 12 bytes per tap.
+// one row each.  With the four x taps' positions and weights in registers, the
+// gather reads 12 bytes of shared memory per row of four taps instead of 12 bytes
+// per tap.
 template <int D, bool WIDE>
 __device__ __forceinline__ void build_rows(const InterpIL &P, const float *sw, const int *sp, int nch,
                                            int *s_roff, float2 *s_rw, int lane) {
@@ -502,8 +503,9 @@ __device__ __forceinline__ void build_rows(const InterpIL &P, const float *sw, c
 
 // XROWS: the launch has one channel per lane (channel chunks of 32) and a box 4
 // taps wide in 2D or 3D; the kernel then takes the x-row form and keeps no
-// per-tap list.
-template <int D, int WM, bool WIDE, bool XROWS>
+// per-tap list.  CH: the grid's channel count when fixed at compile time (x-row
+// form only), else 0.
+template <int D, int WM, bool WIDE, bool XROWS, int CH = 0>
 __global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const InterpIL P) {
     constexpr int NT = ipow<D>(WM);
     // up to 64 taps the weights are kept as (w, w) pairs for FFMA2 and, with one
@@ -513,6 +515,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const Int
     constexpr bool VEC16 = PAIRS && NT % 16 == 0;
     constexpr bool ROWS = XROWS && PAIRS && WM == 4 && D >= 2;
     static_assert(ROWS || !XROWS, "the x-row form needs a 2D / 3D box 4 taps wide");
+    static_assert(CH == 0 || (ROWS && !WIDE), "a compile-time channel count is for the 32-bit x-row form");
     constexpr int NR = ROWS ? NT / 4 : 4;    // x rows of the box
     constexpr int NL = ROWS ? 4 : NT;        // entries of the per-tap list
     using WT = typename std::conditional<PAIRS, float2, float>::type;
@@ -565,44 +568,52 @@ __global__ void __launch_bounds__(kTileWarps * 32, 3) interp_il_kernel(const Int
             const float2 *Gc = G + (c < nch ? c : nch - 1);  // in-bounds address; result discarded
             float2 acc = make_float2(0.f, 0.f);
             if constexpr (ROWS) {
-                // x taps in registers; 4 rows (16 gathers) in flight, each row summed
-                // over x first, then scaled by its w_y * w_z
-                const float4 wx4 = *reinterpret_cast<const float4 *>(s_w[warp]);
+                // 4 rows (16 gathers) in flight; each x position accumulates its
+                // column over the rows (weights w_y * w_z), the four columns are
+                // combined with the x weights at the end
                 const int4 px4 = *reinterpret_cast<const int4 *>(s_p[warp]);
+                float2 ax[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+                                make_float2(0.f, 0.f)};
+                const int4 *ro4 = reinterpret_cast<const int4 *>(s_roff[warp]);
+                auto run = [&](auto addr) {
+#pragma unroll
+                    for (int rb = 0; rb < NR / 4; ++rb) {
+                        const int4 o = ro4[rb];
+                        const int oo[4] = {o.x, o.y, o.z, o.w};
+                        float2 v[16];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) v[4 * q + u] = __ldg(addr(oo[q], u));
+                        }
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float2 wr = s_rw[warp][4 * rb + q];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) ax[u] = __ffma2_rn(wr, v[4 * q + u], ax[u]);
+                        }
+                    }
+                };
+                // with a compile-time channel count and the four x taps side by side
+                // (not split by the fftshift seam), a row is one pointer and its taps
+                // sit at fixed offsets from it
+                if (CH > 0 && px4.y == px4.x + 1 && px4.z == px4.x + 2 && px4.w == px4.x + 3) {
+                    const float2 *Gx0 = Gc + px4.x * CH;
+                    run([&](int o, int u) { return Gx0 + o + u * CH; });
+                } else {
+                    const float2 *Gx[4] = {WIDE ? Gc + (int64_t)px4.x * nch : Gc + px4.x * nch,
+                                           WIDE ? Gc + (int64_t)px4.y * nch : Gc + px4.y * nch,
+                                           WIDE ? Gc + (int64_t)px4.z * nch : Gc + px4.z * nch,
+                                           WIDE ? Gc + (int64_t)px4.w * nch : Gc + px4.w * nch};
+                    run([&](int o, int u) { return WIDE ? Gx[u] + (int64_t)o * nch : Gx[u] + o; });
+                }
+                const float4 wx4 = *reinterpret_cast<const float4 *>(s_w[warp]);
                 const int w0 = P.g.w[0];
                 const float wx1 = w0 > 1 ? wx4.y : 0.f, wx2 = w0 > 2 ? wx4.z : 0.f, wx3 = w0 > 3 ? wx4.w : 0.f;
-                const float2 wx[4] = {make_float2(wx4.x, wx4.x), make_float2(wx1, wx1), make_float2(wx2, wx2),
-                                      make_float2(wx3, wx3)};
-                const int ox[4] = {WIDE ? px4.x : px4.x * nch, WIDE ? px4.y : px4.y * nch,
-                                   WIDE ? px4.z : px4.z * nch, WIDE ? px4.w : px4.w * nch};
-                const int4 *ro4 = reinterpret_cast<const int4 *>(s_roff[warp]);
-#pragma unroll
-                for (int rb = 0; rb < NR / 4; ++rb) {
-                    const int4 o = ro4[rb];
-                    const int oo[4] = {o.x, o.y, o.z, o.w};
-                    float2 v[16];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-#ifdef PFB_INTERP_ROWPTR
-                        const float2 *Gr = WIDE ? Gc + (int64_t)oo[q] * nch : Gc + oo[q];
-#pragma unroll
-                        for (int u = 0; u < 4; ++u)
-                            v[4 * q + u] = WIDE ? __ldg(Gr + (int64_t)ox[u] * nch) : __ldg(Gr + ox[u]);
-#else
-#pragma unroll
-                        for (int u = 0; u < 4; ++u)
-                            v[4 * q + u] = WIDE ? __ldg(Gc + ((int64_t)oo[q] + ox[u]) * nch) : __ldg(Gc + oo[q] + ox[u]);
-#endif
-                    }
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        float2 sr = __fmul2_rn(wx[0], v[4 * q]);
-                        sr = __ffma2_rn(wx[1], v[4 * q + 1], sr);
-                        sr = __ffma2_rn(wx[2], v[4 * q + 2], sr);
-                        sr = __ffma2_rn(wx[3], v[4 * q + 3], sr);
-                        acc = __ffma2_rn(s_rw[warp][4 * rb + q], sr, acc);
-                    }
-                }
+                acc = __fmul2_rn(make_float2(wx4.x, wx4.x), ax[0]);
+                acc = __ffma2_rn(make_float2(wx1, wx1), ax[1], acc);
+                acc = __ffma2_rn(make_float2(wx2, wx2), ax[2], acc);
+                acc = __ffma2_rn(make_float2(wx3, wx3), ax[3], acc);
             } else {
             if (VEC16 && tg_n == 1) {
                 // 16 gathers issued before their sums (more loads in flight per warp);
@@ -1596,7 +1607,8 @@ int launch_interp_il_t(const InterpIL &P, int blocks, cudaStream_t s) {
     const bool wide = P.g.gvol * (int64_t)P.ch.nch >= (1LL << 31);
     if constexpr (WM == 4 && D >= 2) {
         if (P.cw == 32) {  // one channel per lane: the x-row form
-            if (!wide) interp_il_kernel<D, WM, false, true><<<blocks, kTileWarps * 32, 0, s>>>(P);
+            if (!wide && P.ch.nch == 32) interp_il_kernel<D, WM, false, true, 32><<<blocks, kTileWarps * 32, 0, s>>>(P);
+            else if (!wide) interp_il_kernel<D, WM, false, true><<<blocks, kTileWarps * 32, 0, s>>>(P);
             else interp_il_kernel<D, WM, true, true><<<blocks, kTileWarps * 32, 0, s>>>(P);
             PFB_CHECK_LAUNCH();
             return PFB_OK;
