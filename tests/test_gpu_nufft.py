@@ -144,6 +144,19 @@ def test_2d_register_tiles(N, nch):
     check_pair(coord, (N, N), crandn(rng, nch, N, N), crandn(rng, nch, 24, 64), width=4, oversamp=2.0)
 
 
+@pytest.mark.parametrize("N, width, oversamp", [((40, 40), 4, 2.0), ((36, 44), (3, 2), 2.0), ((20, 20, 20), 3, 2.0),
+                                                ((16, 20, 24), (2, 4, 3), 1.25)])
+def test_interp_x_rows_32_channels(N, width, oversamp):
+    """Exactly 32 channels in 2D / 3D boxes up to 4 taps wide: the interp's x-row form with
+    a compile-time channel count (fixed-offset taps; samples whose x taps straddle the
+    fftshift seam take computed pointers), widths below 4 padding rows and columns."""
+    rng = np.random.default_rng(70 + len(N))
+    d = len(N)
+    coord = ((rng.random((1, 40, 60, d)) - 0.5) * np.array(N[::-1])).astype(np.float32)
+    coord[0, :5] *= 0.05  # crowd the centre, where the x taps straddle the seam
+    check_pair(coord, N, crandn(rng, 32, *N), crandn(rng, 32, 40, 60), width=width, oversamp=oversamp)
+
+
 def test_multiframe_and_weights():
     rng = np.random.default_rng(6)
     N, F = 40, 3
