@@ -292,19 +292,30 @@ __global__ void __launch_bounds__(256) vals_il_kernel(const SampIL P) {
     const int64_t g0 = (int64_t)blockIdx.x * R;
     const int B = P.ch.B, SP = B | 1;  // odd row pitch: a warp's column accesses hit distinct banks
     for (int gg = threadIdx.x; gg < R; gg += blockDim.x) s_j[gg] = g0 + gg < P.mtot ? P.iperm[g0 + gg] : 0;
-    for (int e = threadIdx.x; e < R * B; e += blockDim.x) {
-        const int b = e >> P.lrows, gg = e & (R - 1);
-        const int64_t g = g0 + gg;
-        float2 v = make_float2(0.f, 0.f);
-        if (g < P.mtot) {
-            v = P.src[(int64_t)b * P.mtot + g];
-            if (P.weight) {
-                const float w = P.weight[g];
-                v.x *= w;
-                v.y *= w;
+    // four loads in flight per thread before their shared-memory stores
+    constexpr int U = 4;
+    for (int e0 = threadIdx.x; e0 < R * B; e0 += U * blockDim.x) {
+        float2 v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * blockDim.x;
+            const int b = e >> P.lrows, gg = e & (R - 1);
+            const int64_t g = g0 + gg;
+            v[u] = make_float2(0.f, 0.f);
+            if (e < R * B && g < P.mtot) {
+                v[u] = P.src[(int64_t)b * P.mtot + g];
+                if (P.weight) {
+                    const float w = P.weight[g];
+                    v[u].x *= w;
+                    v[u].y *= w;
+                }
             }
         }
-        sm[gg * SP + b] = v;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < R * B) sm[(e & (R - 1)) * SP + (e >> P.lrows)] = v[u];
+        }
     }
     __syncthreads();
     const int nch = P.ch.nch, Kc = P.ch.K ? P.ch.K : 1;
@@ -336,10 +347,22 @@ __global__ void __launch_bounds__(256) out_il_kernel(const SampIL P) {
     const int nch = P.ch.nch, SP = nch | 1;  // odd row pitch: a warp's column accesses hit distinct banks
     for (int gg = threadIdx.x; gg < R; gg += blockDim.x) s_j[gg] = g0 + gg < P.mtot ? P.iperm[g0 + gg] : 0;
     __syncthreads();
-    for (int e = threadIdx.x; e < R * nch; e += blockDim.x) {
-        const int gg = fdiv(e, P.m_nch), c = e - gg * nch;
-        const int64_t g = g0 + gg;
-        sm[gg * SP + c] = g < P.mtot ? P.src[(int64_t)s_j[gg] * nch + c] : make_float2(0.f, 0.f);
+    // four row loads in flight per thread before their shared-memory stores
+    constexpr int U = 4;
+    for (int e0 = threadIdx.x; e0 < R * nch; e0 += U * blockDim.x) {
+        float2 v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * blockDim.x;
+            const int gg = fdiv(e, P.m_nch), c = e - gg * nch;
+            v[u] = e < R * nch && g0 + gg < P.mtot ? P.src[(int64_t)s_j[gg] * nch + c] : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * blockDim.x;
+            const int gg = fdiv(e, P.m_nch), c = e - gg * nch;
+            if (e < R * nch) sm[gg * SP + c] = v[u];
+        }
     }
     __syncthreads();
     const int B = P.ch.B, L = P.ch.L, Kc = P.ch.K ? P.ch.K : 1;
