@@ -111,49 +111,60 @@ struct EmbedParams {
     int64_t bk;        // image planes per segment
 };
 
-__global__ void embed_kernel(const EmbedParams P) {
-    const int64_t total = P.nplanes * P.gvol;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        int64_t plane = e / P.gvol;
-        int64_t pos = e - plane * P.gvol;
-        int q0 = (int)(pos % P.nos[0]);
-        int64_t rest = pos / P.nos[0];
-        int q1 = (int)(rest % P.nos[1]);
-        int q2 = (int)(rest / P.nos[1]);
-        int r0 = q0 - P.off[0], r1 = q1 - P.off[1], r2 = q2 - P.off[2];
-        float2 v = make_float2(0.f, 0.f);
-        if (r0 >= 0 && r0 < P.n[0] && r1 >= 0 && r1 < P.n[1] && r2 >= 0 && r2 < P.n[2]) {
-            // grid plane (l, image plane); the segment multiplies by C_l
-            const int64_t l = plane / P.bk, ip = plane - l * P.bk;
-            const int64_t rl = ((int64_t)r2 * P.n[1] + r1) * P.n[0] + r0;
-            v = P.src[ip * P.nvol + rl];
-            if (P.Cl) v = cmul(v, P.Cl[l * P.nvol + rl]);
+// One CTA per grid row (plane, z, y) at a time: the row's index split is done once,
+// the threads walk x (no 64-bit division per element).
+__global__ void __launch_bounds__(128) embed_kernel(const EmbedParams P) {
+    const int64_t rows_per_plane = (int64_t)P.nos[1] * P.nos[2];
+    const int64_t nrows = P.nplanes * rows_per_plane;
+    for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x) {
+        const int64_t plane = row / rows_per_plane;
+        const int rr = (int)(row - plane * rows_per_plane);
+        const int q2 = rr / P.nos[1], q1 = rr - q2 * P.nos[1];
+        const int r1 = q1 - P.off[1], r2 = q2 - P.off[2];
+        float2 *d = P.dst + row * P.nos[0];
+        if (r1 < 0 || r1 >= P.n[1] || r2 < 0 || r2 >= P.n[2]) {
+            for (int q0 = threadIdx.x; q0 < P.nos[0]; q0 += blockDim.x) d[q0] = make_float2(0.f, 0.f);
+            continue;
         }
-        P.dst[e] = v;
+        // grid plane (l, image plane); the segment multiplies by C_l
+        const int64_t l = plane / P.bk, ip = plane - l * P.bk;
+        const int64_t rl0 = ((int64_t)r2 * P.n[1] + r1) * P.n[0];
+        const float2 *src = P.src + ip * P.nvol + rl0;
+        const float2 *cl = P.Cl ? P.Cl + l * P.nvol + rl0 : nullptr;
+        for (int q0 = threadIdx.x; q0 < P.nos[0]; q0 += blockDim.x) {
+            const int r0 = q0 - P.off[0];
+            float2 v = make_float2(0.f, 0.f);
+            if (r0 >= 0 && r0 < P.n[0]) {
+                v = src[r0];
+                if (cl) v = cmul(v, cl[r0]);
+            }
+            d[q0] = v;
+        }
     }
 }
 
-__global__ void extract_kernel(const EmbedParams P) {
-    const int64_t total = P.nplanes * P.nvol;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        int64_t plane = e / P.nvol;
-        int64_t rl = e - plane * P.nvol;
-        int r0 = (int)(rl % P.n[0]);
-        int64_t rest = rl / P.n[0];
-        int r1 = (int)(rest % P.n[1]);
-        int r2 = (int)(rest / P.n[1]);
-        int64_t pos = ((int64_t)(r2 + P.off[2]) * P.nos[1] + (r1 + P.off[1])) * P.nos[0] + (r0 + P.off[0]);
-        // sum over segments of conj(C_l) times segment l's plane
-        float2 v = make_float2(0.f, 0.f);
-        for (int l = 0; l < P.L; ++l) {
-            float2 g = P.src[((int64_t)l * P.bk + plane) * P.gvol + pos];
-            if (P.Cl) g = cmulc(g, P.Cl[(int64_t)l * P.nvol + rl]);
-            v.x += g.x;
-            v.y += g.y;
+// One CTA per image row (plane, z, y) at a time, as embed_kernel.
+__global__ void __launch_bounds__(128) extract_kernel(const EmbedParams P) {
+    const int64_t rows_per_plane = (int64_t)P.n[1] * P.n[2];
+    const int64_t nrows = P.nplanes * rows_per_plane;
+    for (int64_t row = blockIdx.x; row < nrows; row += gridDim.x) {
+        const int64_t plane = row / rows_per_plane;
+        const int rr = (int)(row - plane * rows_per_plane);
+        const int r2 = rr / P.n[1], r1 = rr - r2 * P.n[1];
+        const int64_t pos0 = ((int64_t)(r2 + P.off[2]) * P.nos[1] + (r1 + P.off[1])) * P.nos[0] + P.off[0];
+        const int64_t rl0 = (int64_t)rr * P.n[0];
+        float2 *d = P.dst + row * P.n[0];
+        for (int r0 = threadIdx.x; r0 < P.n[0]; r0 += blockDim.x) {
+            // sum over segments of conj(C_l) times segment l's plane
+            float2 v = make_float2(0.f, 0.f);
+            for (int l = 0; l < P.L; ++l) {
+                float2 g = P.src[((int64_t)l * P.bk + plane) * P.gvol + pos0 + r0];
+                if (P.Cl) g = cmulc(g, P.Cl[(int64_t)l * P.nvol + rl0 + r0]);
+                v.x += g.x;
+                v.y += g.y;
+            }
+            d[r0] = make_float2(v.x * P.factor, v.y * P.factor);
         }
-        P.dst[e] = make_float2(v.x * P.factor, v.y * P.factor);
     }
 }
 
@@ -284,9 +295,9 @@ int launch_embed(int ndim, const int *n, const int *nos, const float2 *img, floa
     P.src = img;
     P.dst = grid;
     P.factor = 1.f;
-    int64_t total = nplanes * P.gvol;
-    if (total == 0) return PFB_OK;
-    embed_kernel<<<blocks_for(total, 256), 256, 0, s>>>(P);
+    const int64_t rows = nplanes * P.nos[1] * P.nos[2];
+    if (rows == 0 || P.nos[0] == 0) return PFB_OK;
+    embed_kernel<<<(unsigned)std::min<int64_t>(rows, 1 << 20), 128, 0, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
 }
@@ -302,9 +313,9 @@ int launch_extract(int ndim, const int *n, const int *nos, const float2 *grid, f
     P.src = grid;
     P.dst = img;
     P.factor = factor;
-    int64_t total = nplanes * P.nvol;
-    if (total == 0) return PFB_OK;
-    extract_kernel<<<blocks_for(total, 256), 256, 0, s>>>(P);
+    const int64_t rows = nplanes * P.n[1] * P.n[2];
+    if (rows == 0 || P.n[0] == 0) return PFB_OK;
+    extract_kernel<<<(unsigned)std::min<int64_t>(rows, 1 << 20), 128, 0, s>>>(P);
     PFB_CHECK_LAUNCH();
     return PFB_OK;
 }
