@@ -1311,37 +1311,44 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
 #pragma unroll
                 for (int g = 0; g < G; ++g) hit = hit || ((m & bmx[g]) && (m & bmy[g]) && (m & bmz[g]));
             }
-            unsigned hm = __ballot_sync(0xffffffffu, hit);
-            // ballots are warp-uniform values: the jump below needs no convergence barrier
+            const unsigned hm = __ballot_sync(0xffffffffu, hit);
+            // ballots are warp-uniform values: the loops below need no convergence barrier
             const unsigned z0 = __ballot_sync(0xffffffffu, zl & 1u), z1 = __ballot_sync(0xffffffffu, zl & 2u);
-            while (hm) {
-                const int k = __ffs(hm) - 1, q = q0 + k;
-                hm &= hm - 1;
-                const float2 v = rv[q * CPW + cl];
-                // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..; zero
-                // outside the sample's support, so the rows of an occupied z layer are
-                // all updated without a test (a branch per row costs more than the row)
-                const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 24);
-                const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
-                const float4 y01 = t4[(8 + by0) >> 1], y23 = t4[((8 + by0) >> 1) + 1];
-                const float4 z01 = t4[(16 + bz0) >> 1];
-                const float2 wx2[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
-                                       make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
-                const float2 wy[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w),
-                                      make_float2(y23.x, y23.y), make_float2(y23.z, y23.w)};
-                const float2 wz[2] = {make_float2(z01.x, z01.y), make_float2(z01.z, z01.w)};
-                // the blocks of a warp share one z layer (block id bits 2-3), so a jump on
-                // the layer's occupied z rows (1.6 of 2 on average at W 4) is warp-uniform
-                // whatever the group size.  Finer cases run slower: 9 or 45 cases over the
-                // y range as well (a jump table), or a nested jump on the y halves, cost more
-                // than the rows they skip
-                switch (((z0 >> k) & 1u) | (((z1 >> k) & 1u) << 1)) {
-                    case 1: reg3_rows<0, 3, 0, 0>(acc, wx2, wy, wz, v); break;
-                    case 2: reg3_rows<0, 3, 1, 1>(acc, wx2, wy, wz, v); break;
-                    case 3: reg3_rows<0, 3, 0, 1>(acc, wx2, wy, wz, v); break;
-                    default: break;
+            // the hits of the round in three passes by the occupied z rows of the warp's
+            // z layer (1.6 of 2 on average at W 4; the blocks of a warp share one z layer,
+            // so the pattern is warp-uniform whatever the group size), each pass with its
+            // rows fixed at compile time: no per-hit jump on the pattern (a 3-case jump per
+            // hit cost 12 instructions a hit).  Finer patterns (the y range as well) cost
+            // more than the rows they skip
+            auto pass = [&](unsigned m, auto rows) {
+                while (m) {
+                    const int k = __ffs(m) - 1, q = q0 + k;
+                    m &= m - 1;
+                    const float2 v = rv[q * CPW + cl];
+                    // weight pairs (w, w): x entries bx0..bx0+3, y 8+by0.., z 16+bz0..; zero
+                    // outside the sample's support, so the rows of an occupied z layer are
+                    // all updated without a test (a branch per row costs more than the row)
+                    const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 24);
+                    const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
+                    const float4 y01 = t4[(8 + by0) >> 1], y23 = t4[((8 + by0) >> 1) + 1];
+                    const float4 z01 = t4[(16 + bz0) >> 1];
+                    const float2 wx2[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
+                                           make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
+                    const float2 wy[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w),
+                                          make_float2(y23.x, y23.y), make_float2(y23.z, y23.w)};
+                    const float2 wz[2] = {make_float2(z01.x, z01.y), make_float2(z01.z, z01.w)};
+                    rows(wx2, wy, wz, v);
                 }
-            }
+            };
+            pass(hm & z0 & z1, [&](const float2(&a)[4], const float2(&b)[4], const float2(&c)[2], float2 v) {
+                reg3_rows<0, 3, 0, 1>(acc, a, b, c, v);
+            });
+            pass(hm & z0 & ~z1, [&](const float2(&a)[4], const float2(&b)[4], const float2(&c)[2], float2 v) {
+                reg3_rows<0, 3, 0, 0>(acc, a, b, c, v);
+            });
+            pass(hm & ~z0 & z1, [&](const float2(&a)[4], const float2(&b)[4], const float2(&c)[2], float2 v) {
+                reg3_rows<0, 3, 1, 1>(acc, a, b, c, v);
+            });
         }
     }
     // the tile leaves through shared memory: [16 blocks x 32 points][CPW + 1]
