@@ -1305,21 +1305,26 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
         for (int q0 = 0; q0 < nb; q0 += 32) {
             bool hit = false;
             unsigned zl = 0;  // occupied z rows of the warp's z layer, sample q0 + lane
+            unsigned yq = 0;  // occupied y rows of the blocks of the warp's groups (relative to each)
             if (q0 + lane < nb) {
                 const unsigned m = tm[q0 + lane];
                 zl = (m >> (16 + bz0)) & 3u;
+#pragma unroll
+                for (int g = 0; g < G; ++g) yq |= (m >> (8 + (((warp * G + g) >> 1) & 1) * 4)) & 0xFu;
 #pragma unroll
                 for (int g = 0; g < G; ++g) hit = hit || ((m & bmx[g]) && (m & bmy[g]) && (m & bmz[g]));
             }
             const unsigned hm = __ballot_sync(0xffffffffu, hit);
             // ballots are warp-uniform values: the loops below need no convergence barrier
             const unsigned z0 = __ballot_sync(0xffffffffu, zl & 1u), z1 = __ballot_sync(0xffffffffu, zl & 2u);
-            // the hits of the round in three passes by the occupied z rows of the warp's
-            // z layer (1.6 of 2 on average at W 4; the blocks of a warp share one z layer,
-            // so the pattern is warp-uniform whatever the group size), each pass with its
-            // rows fixed at compile time: no per-hit jump on the pattern (a 3-case jump per
-            // hit cost 12 instructions a hit).  Finer patterns (the y range as well) cost
-            // more than the rows they skip
+            // the hits of the round in nine passes by their occupied rows, each pass with
+            // its rows fixed at compile time: z rows of the warp's z layer (both, the
+            // first, the second; the blocks of a warp share one z layer) times y halves of
+            // the blocks (both, the lower, the upper; with several lane groups the union
+            // over the warp's blocks).  No per-hit jump on the pattern (a 3-case jump per
+            // hit cost 12 instructions a hit); a pattern of one y half skips half the
+            // rows.  Single y rows as patterns too would add passes costing more than the
+            // rows they skip
             auto pass = [&](unsigned m, auto rows) {
                 while (m) {
                     const int k = __ffs(m) - 1, q = q0 + k;
@@ -1340,15 +1345,23 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
                     rows(wx2, wy, wz, v);
                 }
             };
-            pass(hm & z0 & z1, [&](const float2(&a)[4], const float2(&b)[4], const float2(&c)[2], float2 v) {
-                reg3_rows<0, 3, 0, 1>(acc, a, b, c, v);
-            });
-            pass(hm & z0 & ~z1, [&](const float2(&a)[4], const float2(&b)[4], const float2(&c)[2], float2 v) {
-                reg3_rows<0, 3, 0, 0>(acc, a, b, c, v);
-            });
-            pass(hm & ~z0 & z1, [&](const float2(&a)[4], const float2(&b)[4], const float2(&c)[2], float2 v) {
-                reg3_rows<0, 3, 1, 1>(acc, a, b, c, v);
-            });
+            const unsigned ylo = __ballot_sync(0xffffffffu, yq & 3u), yhi = __ballot_sync(0xffffffffu, yq & 0xCu);
+            const unsigned zm[3] = {z0 & z1, z0 & ~z1, ~z0 & z1}, ym[3] = {ylo & yhi, ylo & ~yhi, ~ylo & yhi};
+            // z pattern ZI, y pattern YI: rows y Y0..Y1, z Z0..Z1 of the block
+#define PFB_PASS(ZI, Y0, Y1, Z0, Z1, YI) \
+    pass(hm & zm[ZI] & ym[YI], [&](const float2(&a)[4], const float2(&b)[4], const float2(&c)[2], float2 v) { \
+        reg3_rows<Y0, Y1, Z0, Z1>(acc, a, b, c, v); \
+    });
+            PFB_PASS(0, 0, 3, 0, 1, 0)
+            PFB_PASS(0, 0, 1, 0, 1, 1)
+            PFB_PASS(0, 2, 3, 0, 1, 2)
+            PFB_PASS(1, 0, 3, 0, 0, 0)
+            PFB_PASS(1, 0, 1, 0, 0, 1)
+            PFB_PASS(1, 2, 3, 0, 0, 2)
+            PFB_PASS(2, 0, 3, 1, 1, 0)
+            PFB_PASS(2, 0, 1, 1, 1, 1)
+            PFB_PASS(2, 2, 3, 1, 1, 2)
+#undef PFB_PASS
         }
     }
     // the tile leaves through shared memory: [16 blocks x 32 points][CPW + 1]
