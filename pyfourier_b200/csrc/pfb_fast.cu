@@ -1392,6 +1392,19 @@ __global__ void __launch_bounds__(RegCfg<CPW, tap_rec(3, WM)>::NW * 32, RegCfg<C
     }
 }
 
+// Rows y in [Y0, Y1] of a 4 x 8 register block: acc[x + 4 y] += wx[x] (wy[y] v); t4y
+// holds the block's 8 y weights as (w, w) pairs, two per float4.
+template <int Y0, int Y1>
+__device__ __forceinline__ void reg2_rows(float2 (&acc)[32], const float2 (&wx2)[4], const float4 *t4y, float2 v) {
+#pragma unroll
+    for (int py = Y0; py <= Y1; ++py) {
+        const float4 y = t4y[py >> 1];
+        const float2 vv = __fmul2_rn((py & 1) ? make_float2(y.z, y.w) : make_float2(y.x, y.y), v);
+#pragma unroll
+        for (int px = 0; px < 4; ++px) acc[px + 4 * py] = __ffma2_rn(wx2[px], vv, acc[px + 4 * py]);
+    }
+}
+
 // Register-tile spread for 2D tiles of up to 16 x 16 points: the 2D form of
 // spread_reg3_kernel.  Eight blocks of 4 (x) x 8 (y) points tile the packed
 // 16 x 16 tile; a lane group of CPW channels owns one block, its 32 points x
@@ -1528,34 +1541,55 @@ __global__ void __launch_bounds__(Reg2Cfg<CPW>::NW * 32, Reg2Cfg<CPW>::MinBlocks
         __syncthreads();  // tile weights and masks of batch b ready
         for (int q0 = 0; q0 < nb; q0 += 32) {
             bool hit = false;
+            unsigned yq = 0;  // occupied y rows of the warp's y block (shared by its groups)
             if (q0 + lane < nb) {
                 const unsigned m = tm[q0 + lane];
+                yq = (m >> (16 + by0)) & 0xFFu;
 #pragma unroll
                 for (int g = 0; g < G; ++g) hit = hit || ((m & bmx[g]) && (m & bmy[g]));
             }
-            unsigned hm = __ballot_sync(0xffffffffu, hit);
-            while (hm) {
-                const int q = q0 + __ffs(hm) - 1;
-                hm &= hm - 1;
-                const float2 v = rv[q * CPW + cl];
-                // weight pairs (w, w): x entries bx0..bx0+3, y 16+by0..16+by0+7, zero
-                // outside the support, so every row of the block is updated without a test
-                const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 32);
-                const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
-                const float2 wx2[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
-                                       make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
-#pragma unroll
-                for (int py2 = 0; py2 < 4; ++py2) {
-                    const float4 y = t4[((16 + by0) >> 1) + py2];
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int py = 2 * py2 + h;
-                        const float2 vv = __fmul2_rn(h ? make_float2(y.z, y.w) : make_float2(y.x, y.y), v);
-#pragma unroll
-                        for (int px = 0; px < 4; ++px) acc[px + 4 * py] = __ffma2_rn(wx2[px], vv, acc[px + 4 * py]);
-                    }
+            const unsigned hm = __ballot_sync(0xffffffffu, hit);
+            // the hits of the round in passes by the occupied quarters (pairs of y rows)
+            // of the block, each pass with its rows fixed at compile time: a support of
+            // W <= 4 rows covers 2 or 3 of the 4 quarters, so most hits update 4 or 6 of
+            // the 8 rows.  Ballots are warp-uniform: the loops need no convergence barrier
+            const unsigned q0b = __ballot_sync(0xffffffffu, yq & 0x03u), q1b = __ballot_sync(0xffffffffu, yq & 0x0Cu);
+            const unsigned q2b = __ballot_sync(0xffffffffu, yq & 0x30u), q3b = __ballot_sync(0xffffffffu, yq & 0xC0u);
+            auto pass = [&](unsigned mk, auto rows) {
+                while (mk) {
+                    const int q = q0 + __ffs(mk) - 1;
+                    mk &= mk - 1;
+                    const float2 v = rv[q * CPW + cl];
+                    // weight pairs (w, w): x entries bx0..bx0+3, y 16+by0..16+by0+7, zero
+                    // outside the support, so the rows of a pass are updated without a test
+                    const float4 *t4 = reinterpret_cast<const float4 *>(tw + q * 32);
+                    const float4 x01 = t4[bx0 >> 1], x23 = t4[(bx0 >> 1) + 1];
+                    const float2 wx2[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w),
+                                           make_float2(x23.x, x23.y), make_float2(x23.z, x23.w)};
+                    rows(wx2, t4 + ((16 + by0) >> 1), v);
                 }
-            }
+            };
+            // quarter range [lo, hi]: exactly the quarters lo..hi occupied
+            auto range = [&](int lo, int hi) {
+                const unsigned b[4] = {q0b, q1b, q2b, q3b};
+                unsigned r = hm;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) r &= (i >= lo && i <= hi) ? b[i] : ~b[i];
+                return r;
+            };
+            unsigned done = 0;
+#define PFB_PASS2(LO, HI)                                                                              \
+    {                                                                                                  \
+        const unsigned mk = range(LO, HI);                                                             \
+        done |= mk;                                                                                    \
+        pass(mk, [&](const float2(&a)[4], const float4 *ty, float2 v) { reg2_rows<2 * LO, 2 * HI + 1>(acc, a, ty, v); }); \
+    }
+            PFB_PASS2(0, 0) PFB_PASS2(0, 1) PFB_PASS2(0, 2) PFB_PASS2(1, 1) PFB_PASS2(1, 2)
+            PFB_PASS2(1, 3) PFB_PASS2(2, 2) PFB_PASS2(2, 3) PFB_PASS2(3, 3)
+#undef PFB_PASS2
+            // every other pattern (all four quarters, or a support wrapped around a
+            // one-tile axis): all 8 rows
+            pass(hm & ~done, [&](const float2(&a)[4], const float4 *ty, float2 v) { reg2_rows<0, 7>(acc, a, ty, v); });
         }
     }
     __syncthreads();  // staging no longer read: reuse it for the output tile
