@@ -91,3 +91,18 @@ def test_resolve_device_maps_the_reference_arguments(monkeypatch):
     monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         rd("cuda:0")
+
+
+@pytest.mark.parametrize("B", [1, 2, 3, 5, 8, 16, 31, 32, 33, 64, 100])
+@pytest.mark.parametrize("chunks", [1, 4, 7])
+def test_host_pipeline_chunks_partition_the_batch(B, chunks):
+    """The host pipeline's chunks cover 0..B once, in order, none empty; with enough items
+    the first and the last are the small B / 16 end chunks."""
+    bounds = _nufft._chunk_bounds(B, chunks)
+    assert bounds[0][0] == 0 and bounds[-1][1] == B
+    assert all(b > a for a, b in bounds)
+    assert all(bounds[i][1] == bounds[i + 1][0] for i in range(len(bounds) - 1))
+    if B == 32 and chunks == 4:
+        assert [b - a for a, b in bounds] == [2, 7, 7, 7, 7, 2]
+    if B == 32 and chunks == 7:
+        assert [b - a for a, b in bounds] == [2, 4, 4, 4, 4, 4, 4, 4, 2]
