@@ -1,31 +1,34 @@
 // Channel-interleaved NUFFT pipeline (the path behind pfb_nufft_fwd / pfb_nufft_adj).
 //
 // Two grid layouts share the workspace:
-//   planar       [group][channel][point]  -- what cuFFT transforms (batched planes)
+//   planar       [group][channel][point]  -- what the spread writes, the z / y passes read
 //   interleaved  [group][point][channel]  -- what the interp gathers from
 //   without a basis: group = frame f, channel = l * B + b        (B0 segment l, batch b)
 //   with a basis:    group = 0,       channel = (l * B + b) * K + k
 // point is the FFT-layout position ((centred index - n_os//2) mod n_os, x fastest).
-// In the interleaved layout a tap of a sample is one contiguous run of
-// channels, so a warp whose lanes are channels gathers it with one coalesced
-// access.  cuFFT is far faster on planar batches than on channel-strided
-// data, so the forward path transposes the transformed grid once, and the
-// spread writes its finished tiles straight into planar planes.
+// In the interleaved layout a tap of a sample is one contiguous run of channels,
+// so a warp whose lanes are channels gathers it with one coalesced access.  In
+// 2D / 3D the transforms are the fused pruned FFT passes of pfb_fft.cu (pad and
+// deapodise in the first pass, the last forward pass writes the interleaved
+// grid, the adjoint's first pass reads it, crop in the last pass); the planar
+// kernels below serve 1D and the layouts those passes do not take.
 //
 // Kernels:
 //   pad_pl       image (B, C, *N) -> planar grid, deapodised, zero-padded, times C_l (B0)
 //   transpose    planar grid -> interleaved grid
-//   interp_il    interleaved grid -> res[j][channel] (one warp per sample, lanes = channels)
+//   interp_il    interleaved grid -> res[j][channel] (one warp per sample, lanes =
+//                channels x tap groups; x rows of the kernel box at 32 channels)
 //   out_il       res -> k-space (B, M): sum over segments / coefficients with
 //                B_l(t) basis[f, k], density weight
 //   vals_il      k-space (B, M) -> vals[j][channel] in bin-sorted order, with the
 //                density weight and conj(B_l(t)) conj(basis[f, k]) factors
-//   spread_il    vals -> planar grid, owner-computes: one CTA per output tile (and
-//                sample chunk) accumulates in shared memory the contributions of
-//                the samples whose first tap lies in the tile or in its 2^d - 1
-//                lower neighbours, then stores the tile (plain stores; tiles too
-//                crowded for one CTA are split and combined with float2 atomics
-//                after a zeroing pass)
+//   spread_reg3 / spread_reg2 / spread_il
+//                vals -> planar grid, owner-computes: one CTA per output tile (and
+//                channel group) accumulates the contributions of the samples whose
+//                first tap lies in the tile or in its 2^d - 1 lower neighbours, in
+//                registers (3D, and 2D above 16 channels) or in shared memory, then
+//                stores the tile (plain stores; tiles too crowded for one CTA are
+//                split and combined with float2 atomics after a zeroing pass)
 //   crop_pl      planar grid -> image, cropped, deapodised, sum_l conj(C_l) (B0)
 //   traj_il      d/dk of sum_b Re(conj(A x)_b v_b) (analytic Kaiser-Bessel derivative)
 #include <cmath>
