@@ -10,8 +10,9 @@
 // so a warp whose lanes are channels gathers it with one coalesced access.  In
 // 2D / 3D the transforms are the fused pruned FFT passes of pfb_fft.cu (pad and
 // deapodise in the first pass, the last forward pass writes the interleaved
-// grid, the adjoint's first pass reads it, crop in the last pass); the planar
-// kernels below serve 1D and the layouts those passes do not take.
+// grid; the adjoint's passes start from the spread's planar grid and crop in the
+// last pass); the planar kernels below serve 1D and the layouts those passes do
+// not take.
 //
 // Kernels:
 //   pad_pl       image (B, C, *N) -> planar grid, deapodised, zero-padded, times C_l (B0)
