@@ -594,7 +594,8 @@ struct ColTma {
     int inv, mode;          // as ColPass: 0 buffer -> buffer, 1 image -> buffer, 2 buffer -> image
     int lin, lout, hn;      // rows read / written; hn: rotation of the fftshift (nax / 2)
     int X, nxc, nmid, nplanes;
-    int ntiles;
+    int ntiles;             // output blocks (16 x positions of one (mid, plane))
+    int nseg;               // tiles per output block: the B0 segments summed by an adjoint last pass, else 1
     int nbox;               // load boxes per tile: smem row, source row (before the +hn rotation fold)
     int box_smem[kTmaMaxBoxes], box_src[kTmaMaxBoxes];
     int br;                 // rows per load box
@@ -605,6 +606,8 @@ struct ColTma {
     int C;
     int64_t nvol;
     const float *apod_ax, *apod_mid, *apod_x;
+    const float2 *Cl;       // B0 segment factors on the image side (nseg x nvol), or null
+    int64_t img_mid, img_ax;  // image strides of Cl (the image side's mid and axis strides)
     float factor;
     int accumulate;
     int *err;               // set to 1 when a wait gives up (the results are then invalid)
@@ -655,7 +658,7 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
 struct TileInfo {
-    int xc, mid, plane;
+    int xc, mid, plane, l;  // l: segment of an adjoint last pass (0 otherwise)
 };
 
 // src_map: the pass's source as 4D (2X floats, rows, mid, source plane); dst_map:
@@ -663,7 +666,9 @@ struct TileInfo {
 // NSLOT ring slots: 2 (the next tile loads while this one transforms; 2 CTAs per
 // SM) or 1 (3 CTAs per SM overlap instead: slower, 1.30 against 1.21 ms for the
 // 200^3 z pass, 1.45 against 1.21 ms for the y pass)
-template <int NSLOT>
+// SEG: B0 factors and segment sums (forward first passes with C_l, adjoint last
+// passes over several segments); the plain instantiation keeps its simpler loops.
+template <int NSLOT, bool SEG>
 __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
     col_tma_kernel(const __grid_constant__ CUtensorMap src_map, const __grid_constant__ CUtensorMap dst_map,
                    const ColTma P) {
@@ -677,8 +682,9 @@ __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
     constexpr int NS = kThreads * 2 / kCols;  // row streams: a thread moves two adjacent columns
     const unsigned box_bytes = (unsigned)P.br * kTmaPitch * sizeof(float2);
     const bool fwd_store = P.mode != 2 && !P.inv;
-    // thread 0: load tile t into slot s (tile coordinates go with it through shared memory)
-    auto issue = [&](int t, int s) {
+    // thread 0: load segment l of output block t into slot s (tile coordinates go with
+    // it through shared memory)
+    auto issue = [&](int t, int l, int s) {
         const int r = t / P.nxc, xc = t - r * P.nxc;
         const int plane = r / P.nmid, mid = r - plane * P.nmid;
         int sp = plane;  // source plane
@@ -687,16 +693,23 @@ __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
             const int grp = plane / P.ch.nch, chn = plane - grp * P.ch.nch;
             const int k = chn % Kc, b = (chn / Kc) % P.ch.B;
             sp = b * P.C + (P.ch.K ? k : grp);
-        } else if (P.mode == 2) {  // image plane (b, c) <- grid plane (grp, chn) of the only segment
+        } else if (P.mode == 2) {  // image plane (b, c) <- grid plane (grp, chn) of segment l
             const int b = plane / P.C, c = plane - b * P.C;
             const int Kc = P.ch.K ? P.ch.K : 1;
-            sp = (P.ch.K ? 0 : c) * P.ch.nch + (P.ch.K ? b * Kc + c : b);
+            sp = (P.ch.K ? 0 : c) * P.ch.nch + (P.ch.K ? (l * P.ch.B + b) * Kc + c : l * P.ch.B + b);
         }
-        info[s] = TileInfo{xc, mid, plane};
+        info[s] = TileInfo{xc, mid, plane, l};
         mbar_expect_tx(&full[s], box_bytes * P.nbox);
         for (int b = 0; b < P.nbox; ++b)
             tma_load4(tsm + (s * n + P.box_smem[b]) * kTmaPitch, &src_map, xc * 2 * kCols, P.box_src[b], mid, sp,
                       &full[s]);
+    };
+    // the CTA's k-th tile: segment k mod nseg of its output block k / nseg (the
+    // segments of one block are consecutive, so one CTA sums them)
+    auto block_of = [&](int kk, int &l) {
+        const int q = SEG ? kk / P.nseg : kk;
+        l = kk - q * P.nseg;
+        return (int)blockIdx.x + q * (int)gridDim.x;
     };
     if (threadIdx.x == 0) {
         mbar_init(&full[0], 1);
@@ -706,13 +719,16 @@ __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int s = 0; s < NSLOT; ++s) {
-            const int t = blockIdx.x + s * gridDim.x;
-            if (t < P.ntiles) issue(t, s);
+            int l;
+            const int t = block_of(s, l);
+            if (t < P.ntiles) issue(t, l, s);
         }
     }
-    int k = 0;
     bool store_pending = false;  // thread 0: a TMA store of the scratch buffer may still be reading it
-    for (int t = blockIdx.x; t < P.ntiles; t += gridDim.x, ++k) {
+    for (int k = 0;; ++k) {
+        int lk;
+        const int t = block_of(k, lk);
+        if (t >= P.ntiles) break;
         const int s = NSLOT == 1 ? 0 : k & 1;
         bool ok = mbar_wait(&full[s], (NSLOT == 1 ? k : k >> 1) & 1);
         const TileInfo ti = info[s];
@@ -731,7 +747,53 @@ __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
                 amid1 *= P.apod_x[xs + 1];
             }
         }
-        if (ok && P.mode == 1) {
+        if (SEG && ok && P.mode == 1) {
+            // B0 factors of the plane's segment, then deapodise, on the rows that hold
+            // image data (the others were filled with zeros)
+            const float2 *clp = nullptr;
+            if (P.Cl) {
+                const int Kc = P.ch.K ? P.ch.K : 1;
+                const int chn = ti.plane % P.ch.nch;
+                const int ll = chn / Kc / P.ch.B;
+                clp = P.Cl + (int64_t)ll * P.nvol + (int64_t)ti.mid * P.img_mid + xs;
+            }
+            // kU rows per thread at a time: their factor loads are all in flight
+            // before the first product
+            constexpr int kU = 4;
+            for (int p0 = stream; p0 < n; p0 += kU * NS) {
+                int ii[kU];
+                float aa[kU];
+                float4 cc[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int p = p0 + u * NS;
+                    int i = p + P.hn;
+                    if (i >= n) i -= n;
+                    ii[u] = p < n && i < P.lin ? i : -1;
+                    const int ic = ii[u] < 0 ? 0 : ii[u];
+                    aa[u] = P.apod_ax ? P.apod_ax[ic] : 1.f;
+                    cc[u] = clp ? __ldg(reinterpret_cast<const float4 *>(clp + (int64_t)ic * P.img_ax))
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    if (ii[u] < 0) continue;
+                    float4 *q = reinterpret_cast<float4 *>(A + (p0 + u * NS) * kTmaPitch + col);
+                    float4 v = *q;
+                    if (clp) {
+                        const float2 v0 = cmul(make_float2(v.x, v.y), make_float2(cc[u].x, cc[u].y));
+                        const float2 v1 = cmul(make_float2(v.z, v.w), make_float2(cc[u].z, cc[u].w));
+                        v = make_float4(v0.x, v0.y, v1.x, v1.y);
+                    }
+                    const float a0 = aa[u] * amid0, a1 = aa[u] * amid1;
+                    v.x *= a0;
+                    v.y *= a0;
+                    v.z *= a1;
+                    v.w *= a1;
+                    *q = v;
+                }
+            }
+        } else if (ok && P.mode == 1) {
             // deapodise the rows that hold image data (the others were filled with zeros)
             for (int p = stream; p < n; p += NS) {
                 int i = p + P.hn;
@@ -759,13 +821,15 @@ __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
             if (threadIdx.x == 0) {
                 atomicExch(P.err, 1);
                 // the other slot's load, if one is in flight
-                if (NSLOT == 2 && t + (int)gridDim.x < P.ntiles) mbar_wait(&full[s ^ 1], ((k + 1) >> 1) & 1);
+                int l1;
+                if (NSLOT == 2 && block_of(k + 1, l1) < P.ntiles) mbar_wait(&full[s ^ 1], ((k + 1) >> 1) & 1);
                 if (store_pending) bulk_wait_read0();
             }
             return;
         }
         const float2 *R = fft_run<kTmaPitch>(A, scr, P.fa);
-        const int tn = t + NSLOT * gridDim.x;  // the next tile for this slot
+        int ln;
+        const int tn = block_of(k + NSLOT, ln);  // the next tile for this slot
         if (fwd_store) {
             // rows 0..n-1 of the result are the output rows: TMA store from shared memory
             fence_async_smem();
@@ -780,7 +844,7 @@ __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
                 // buffer is waited for before the next transform
                 if (R == A) bulk_wait_read0();
                 else store_pending = true;
-                if (tn < P.ntiles) issue(tn, s);
+                if (tn < P.ntiles) issue(tn, ln, s);
             }
             continue;
         } else {
@@ -788,29 +852,85 @@ __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
             // forward transform's position (n - pp) mod n
             const int64_t obase = P.mode == 2 ? (int64_t)ti.plane * P.nvol + (int64_t)ti.mid * P.out_mid
                                               : (int64_t)ti.plane * P.out_plane + (int64_t)ti.mid * P.out_mid;
-            for (int o = stream; o < P.lout; o += NS) {
-                int pp = o - P.hn;
-                if (pp < 0) pp += n;
-                const int q = pp == 0 ? 0 : n - pp;
-                float4 v = *reinterpret_cast<const float4 *>(R + q * kTmaPitch + col);
-                if (!xin) continue;
-                float4 *d = reinterpret_cast<float4 *>(P.dst + obase + (int64_t)o * P.out_ax + x);
-                if (P.mode == 2) {
-                    const float a = P.apod_ax ? P.apod_ax[o] : 1.f;
-                    const float a0 = a * amid0, a1 = a * amid1;
-                    v.x *= a0;
-                    v.y *= a0;
-                    v.z *= a1;
-                    v.w *= a1;
-                    if (P.accumulate) {
-                        const float4 old = *d;
-                        v.x += old.x;
-                        v.y += old.y;
-                        v.z += old.z;
-                        v.w += old.w;
+            if (SEG) {
+                // kU rows per thread at a time: the factor and partial-sum loads of an
+                // adjoint last pass are all in flight before the first product
+                constexpr int kU = 3;
+                const bool seg_sum = P.mode == 2 && (P.accumulate || ti.l > 0);
+                const float2 *clp =
+                    P.mode == 2 && P.Cl ? P.Cl + (int64_t)ti.l * P.nvol + (int64_t)ti.mid * P.out_mid : nullptr;
+                for (int o0 = stream; o0 < P.lout; o0 += kU * NS) {
+                    float4 cc[kU], old[kU];
+                    float aa[kU];
+#pragma unroll
+                    for (int u = 0; u < kU; ++u) {
+                        const int o = o0 + u * NS;
+                        const int oc = o < P.lout ? o : 0;
+                        if (P.mode == 2 && xin) {
+                            const int64_t off = (int64_t)oc * P.out_ax + x;
+                            cc[u] = clp ? __ldg(reinterpret_cast<const float4 *>(clp + off))
+                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+                            // segments after the first add to the sum this thread stored for
+                            // the ones before (same addresses, same thread: a plain load)
+                            old[u] = seg_sum ? *reinterpret_cast<const float4 *>(P.dst + obase + off)
+                                             : make_float4(0.f, 0.f, 0.f, 0.f);
+                            aa[u] = P.apod_ax ? P.apod_ax[oc] : 1.f;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kU; ++u) {
+                        const int o = o0 + u * NS;
+                        if (o >= P.lout || !xin) continue;
+                        int pp = o - P.hn;
+                        if (pp < 0) pp += n;
+                        const int q = pp == 0 ? 0 : n - pp;
+                        float4 w = *reinterpret_cast<const float4 *>(R + q * kTmaPitch + col);
+                        if (P.mode == 2) {
+                            if (clp) {  // times conj(C_l) of the tile's segment
+                                const float2 v0 = cmulc(make_float2(w.x, w.y), make_float2(cc[u].x, cc[u].y));
+                                const float2 v1 = cmulc(make_float2(w.z, w.w), make_float2(cc[u].z, cc[u].w));
+                                w = make_float4(v0.x, v0.y, v1.x, v1.y);
+                            }
+                            const float a0 = aa[u] * amid0, a1 = aa[u] * amid1;
+                            w.x *= a0;
+                            w.y *= a0;
+                            w.z *= a1;
+                            w.w *= a1;
+                            if (seg_sum) {
+                                w.x += old[u].x;
+                                w.y += old[u].y;
+                                w.z += old[u].z;
+                                w.w += old[u].w;
+                            }
+                        }
+                        *reinterpret_cast<float4 *>(P.dst + obase + (int64_t)o * P.out_ax + x) = w;
                     }
                 }
-                *d = v;
+            } else {
+                for (int o = stream; o < P.lout; o += NS) {
+                    int pp = o - P.hn;
+                    if (pp < 0) pp += n;
+                    const int q = pp == 0 ? 0 : n - pp;
+                    float4 v = *reinterpret_cast<const float4 *>(R + q * kTmaPitch + col);
+                    if (!xin) continue;
+                    float4 *d = reinterpret_cast<float4 *>(P.dst + obase + (int64_t)o * P.out_ax + x);
+                    if (P.mode == 2) {
+                        const float a = P.apod_ax ? P.apod_ax[o] : 1.f;
+                        const float a0 = a * amid0, a1 = a * amid1;
+                        v.x *= a0;
+                        v.y *= a0;
+                        v.z *= a1;
+                        v.w *= a1;
+                        if (P.accumulate) {
+                            const float4 old = *d;
+                            v.x += old.x;
+                            v.y += old.y;
+                            v.z += old.z;
+                            v.w += old.w;
+                        }
+                    }
+                    *d = v;
+                }
             }
             // the slot and the scratch buffer are read; the generic accesses are ordered
             // before the slot's next TMA load
@@ -818,7 +938,7 @@ __global__ void __launch_bounds__(kThreads, NSLOT == 1 ? 3 : 2)
             __syncthreads();
         }
         // refill this slot with the tile after next
-        if (threadIdx.x == 0 && tn < P.ntiles) issue(tn, s);
+        if (threadIdx.x == 0 && tn < P.ntiles) issue(tn, ln, s);
     }
     if (threadIdx.x == 0 && store_pending) bulk_wait_read0();
 }
@@ -1172,13 +1292,17 @@ int box_rows(int a, int b) {
 }
 
 // The column pass on TMA when its layout allows it (every stride and base
-// 16-byte aligned, even X, no B0 factors, one segment); returns 1 if launched,
-// 0 to take the copy-based kernel, or an error.
+// 16-byte aligned, even X); returns 1 if launched, 0 to take the copy-based
+// kernel, or an error.  An adjoint last pass over B0 segments walks the segments
+// of each output block as consecutive tiles of one CTA.
 int launch_col_tma(const ColPass &P, int64_t ntiles, cudaStream_t s) {
     const int n = P.fa.n;
-    if (!P.err || P.nsm <= 0 || P.Cl || (P.mode == 2 && P.ch.L != 1) || P.X % 2 != 0 || n > kMaxN) return 0;
+    if (!P.err || P.nsm <= 0 || P.X % 2 != 0 || n > kMaxN) return 0;
     auto a16 = [](const void *q) { return ((uintptr_t)q & 15u) == 0; };
     if (!a16(P.src) || !a16(P.dst)) return 0;
+    if (P.Cl && (P.mode == 0 || !a16(P.Cl))) return 0;
+    const int nseg = P.mode == 2 ? P.ch.L : 1;
+    if (nseg < 1) return 0;
     const int64_t src_plane = P.mode == 1 ? P.nvol : P.in_plane;
     const int64_t dst_plane = P.mode == 2 ? P.nvol : P.out_plane;
     for (int64_t v : {P.in_ax, P.in_mid, src_plane, P.out_ax, P.out_mid, dst_plane})
@@ -1196,6 +1320,7 @@ int launch_col_tma(const ColPass &P, int64_t ntiles, cudaStream_t s) {
     T.nplanes = P.nplanes;
     if (ntiles >= (1LL << 31) - 2LL * P.nsm * 4) return 0;
     T.ntiles = (int)ntiles;
+    T.nseg = nseg;
     // load boxes: forward passes rotate (smem row p <- source row (p + hn) mod n),
     // inverse passes read the rows in order
     const int seg0 = P.inv ? n : n - T.hn, seg1 = P.inv ? 0 : T.hn;
@@ -1229,6 +1354,9 @@ int launch_col_tma(const ColPass &P, int64_t ntiles, cudaStream_t s) {
     T.apod_ax = P.apod_ax;
     T.apod_mid = P.apod_mid;
     T.apod_x = P.apod_x;
+    T.Cl = P.Cl;
+    T.img_mid = P.in_mid;  // read for forward first passes (image -> buffer)
+    T.img_ax = P.in_ax;
     T.factor = P.factor;
     T.accumulate = P.accumulate;
     T.err = P.err;
@@ -1244,7 +1372,7 @@ int launch_col_tma(const ColPass &P, int64_t ntiles, cudaStream_t s) {
     }
     constexpr int kSlots = 2;
     const size_t smem = (size_t)(kSlots + 1) * n * kTmaPitch * sizeof(float2);
-    auto kern = col_tma_kernel<kSlots>;
+    auto kern = P.Cl || nseg > 1 ? col_tma_kernel<kSlots, true> : col_tma_kernel<kSlots, false>;
     PFB_RAISE_SMEM(kern, (int)smem);
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem) != cudaSuccess || per_sm < 1)
