@@ -170,6 +170,86 @@ __device__ __forceinline__ void dft<10>(float2 *a) {
     }
 }
 
+// N = N1 N2 point DFT by one mixed-radix split: with n = n1 + N1 n2 and
+// k = N2 k1 + k2, b_k = sum_n1 W_N1^(n1 k1) W_N^(n1 k2) sum_n2 W_N2^(n2 k2) a_n:
+// N1 inner N2-point DFTs, the twiddles W_N^(n1 k2), N2 outer N1-point DFTs.
+// C / S hold cos / sin of 2 pi m / N, m = 0..N-1 (constant-folded once unrolled).
+template <int N1, int N2>
+__device__ __forceinline__ void dft_split(float2 *a, const float *C, const float *S) {
+    constexpr int N = N1 * N2;
+    float2 y[N1][N2];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) y[n1][n2] = a[n1 + N1 * n2];
+        dft<N2>(y[n1]);
+    }
+#pragma unroll
+    for (int n1 = 1; n1 < N1; ++n1)
+#pragma unroll
+        for (int k2 = 1; k2 < N2; ++k2) {
+            const int m = (n1 * k2) % N;
+            y[n1][k2] = cmul(y[n1][k2], make_float2(C[m], -S[m]));
+        }
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+        float2 z[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) z[n1] = y[n1][k2];
+        dft<N1>(z);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) a[N2 * k1 + k2] = z[k1];
+    }
+}
+
+template <>
+__device__ __forceinline__ void dft<16>(float2 *a) {
+    // cos and sin of 2 pi m / 16, m = 0..7 (the split uses m = k2 < 8)
+    const float C[8] = {1.f, 0.92387953251128674f, 0.70710678118654757f, 0.38268343236508984f,
+                        0.f, -0.38268343236508973f, -0.70710678118654746f, -0.92387953251128674f};
+    const float S[8] = {0.f, 0.38268343236508978f, 0.70710678118654746f, 0.92387953251128674f,
+                        1.f, 0.92387953251128674f, 0.70710678118654757f, 0.38268343236508989f};
+    dft_split<2, 8>(a, C, S);
+}
+
+template <>
+__device__ __forceinline__ void dft<15>(float2 *a) {
+    // cos and sin of 2 pi m / 15
+    const float C[15] = {1.f, 0.91354545764260087f, 0.66913060635885824f, 0.30901699437494745f,
+                         -0.10452846326765333f, -0.49999999999999978f, -0.80901699437494734f,
+                         -0.97814760073380569f, -0.97814760073380569f, -0.80901699437494756f,
+                         -0.50000000000000044f, -0.10452846326765423f, 0.30901699437494723f,
+                         0.66913060635885846f, 0.91354545764260098f};
+    const float S[15] = {0.f, 0.40673664307580015f, 0.74314482547739413f, 0.95105651629515353f,
+                         0.9945218953682734f, 0.86602540378443871f, 0.58778525229247325f,
+                         0.20791169081775931f, -0.20791169081775907f, -0.58778525229247303f,
+                         -0.86602540378443837f, -0.99452189536827329f, -0.95105651629515364f,
+                         -0.74314482547739402f, -0.40673664307580015f};
+    dft_split<3, 5>(a, C, S);
+}
+
+template <>
+__device__ __forceinline__ void dft<25>(float2 *a) {
+    // cos and sin of 2 pi m / 25
+    const float C[25] = {1.f, 0.96858316112863108f, 0.87630668004386358f, 0.72896862742141155f,
+                         0.53582679497899655f, 0.30901699437494745f, 0.062790519529313527f,
+                         -0.1873813145857246f, -0.42577929156507272f, -0.63742398974868975f,
+                         -0.80901699437494734f, -0.92977648588825135f, -0.99211470131447776f,
+                         -0.99211470131447788f, -0.92977648588825146f, -0.80901699437494778f,
+                         -0.63742398974868952f, -0.42577929156507216f, -0.18738131458572463f,
+                         0.062790519529312833f, 0.30901699437494723f, 0.53582679497899677f,
+                         0.72896862742141122f, 0.87630668004386314f, 0.96858316112863097f};
+    const float S[25] = {0.f, 0.24868988716485479f, 0.48175367410171532f, 0.68454710592868862f,
+                         0.84432792550201508f, 0.95105651629515353f, 0.99802672842827156f,
+                         0.98228725072868872f, 0.90482705246601947f, 0.77051324277578925f,
+                         0.58778525229247325f, 0.36812455268467814f, 0.12533323356430454f,
+                         -0.12533323356430429f, -0.36812455268467792f, -0.58778525229247269f,
+                         -0.77051324277578936f, -0.9048270524660198f, -0.98228725072868872f,
+                         -0.99802672842827156f, -0.95105651629515364f, -0.84432792550201496f,
+                         -0.68454710592868895f, -0.4817536741017161f, -0.24868988716485535f};
+    dft_split<5, 5>(a, C, S);
+}
+
 // One Stockham stage over the CTA's 16 columns (rows PITCH float2 apart); a
 // thread takes two adjacent columns (one float4) of each of its butterflies.
 template <int R, int PITCH>
@@ -201,31 +281,50 @@ __device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2
     }
 }
 
-// The stage plan of a transform length known at compile time: the same radix
-// order as make_axis (8, 10, 5, 4, 3, 7, 2, each as often as it divides), so
-// the twiddle table built on the host serves both forms.
+// The stage plan of a transform length: the radix order 8, 10, 5, 4, 3, 7, 2, each
+// as often as it divides, except for the lengths of the benchmark grids, which run
+// two stages (one CTA barrier and one shared-memory round trip fewer than the three
+// the radix order gives): 240 = 16 x 15 and 250 = 25 x 10.  make_axis builds the
+// twiddle table from the same plan, so the compile-time and table-driven forms
+// agree; radices 15, 16 and 25 only occur in the compile-time form.
 constexpr int kRadixOrder[7] = {8, 10, 5, 4, 3, 7, 2};
 struct StagePlan {
     int nst = 0;
     int radix[kFftMaxStages] = {};
     int ns[kFftMaxStages] = {};
-    int twoff[kFftMaxStages] = {};
+    int twoff[kFftMaxStages] = {};  // relative to the axis's first twiddle
 };
 constexpr StagePlan stage_plan(int n) {
     StagePlan p{};
-    int m = n, ns = 1, off = 0;
-    for (int k = 0; k < 7; ++k) {
-        const int r = kRadixOrder[k];
-        while (m % r == 0 && p.nst < kFftMaxStages) {
-            p.radix[p.nst] = r;
-            p.ns[p.nst] = ns;
-            p.twoff[p.nst] = off;
-            off += ns * (r - 1);
-            ++p.nst;
-            ns *= r;
-            m /= r;
+    int rad[kFftMaxStages] = {};
+    int nr = 0;
+    if (n == 240) {
+        rad[0] = 16;
+        rad[1] = 15;
+        nr = 2;
+    } else if (n == 250) {
+        rad[0] = 25;
+        rad[1] = 10;
+        nr = 2;
+    } else {
+        int m = n;
+        for (int k = 0; k < 7; ++k) {
+            const int r = kRadixOrder[k];
+            while (m % r == 0 && nr < kFftMaxStages) {
+                rad[nr++] = r;
+                m /= r;
+            }
         }
     }
+    int ns = 1, off = 0;
+    for (int s = 0; s < nr; ++s) {
+        p.radix[s] = rad[s];
+        p.ns[s] = ns;
+        p.twoff[s] = off;
+        off += ns * (rad[s] - 1);
+        ns *= rad[s];
+    }
+    p.nst = nr;
     return p;
 }
 
@@ -240,6 +339,8 @@ struct PitchLoad {
     __device__ __forceinline__ float4 operator()(int pos, int cp) const {
         return *reinterpret_cast<const float4 *>(src + pos * PITCH + 2 * cp);
     }
+    // position pos of column c alone
+    __device__ __forceinline__ float2 one(int pos, int c) const { return src[pos * PITCH + c]; }
 };
 
 // Source of the first stage of an x pass: 16 rows (one per vector) of `pitch`
@@ -255,7 +356,44 @@ struct RowMajorLoad {
         const float2 a = src[(2 * cp) * pitch + x], b = src[(2 * cp + 1) * pitch + x];
         return make_float4(a.x, a.y, b.x, b.y);
     }
+    __device__ __forceinline__ float2 one(int pos, int c) const {
+        int x = pos + rot;
+        if (x >= n) x -= n;
+        if (x >= len) return make_float2(0.f, 0.f);
+        return src[c * pitch + x];
+    }
 };
+
+// Radices whose stages run with one column per thread (16 columns x 16 butterfly
+// streams): a butterfly of two columns would hold 30 to 50 complex values
+constexpr bool one_col_radix(int r) { return r >= 15; }
+constexpr int kColStreams = kThreads / kCols;
+
+// A Stockham stage with one column per thread: thread t takes column t mod 16 of
+// butterflies t / 16, t / 16 + 16, ...  Same positions, twiddles and results as
+// the two-column form.
+template <int R, int NS, int M, int PITCH, class L>
+__device__ __forceinline__ void fft_stage1_cl(const L &ld, float2 *__restrict__ dst, const float2 *__restrict__ tw) {
+    constexpr int IT = (M + kColStreams - 1) / kColStreams;
+    const int c = threadIdx.x & (kCols - 1), stream = threadIdx.x / kCols;
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int i = stream + it * kColStreams;
+        if (M % kColStreams != 0 && i >= M) break;
+        const int j = NS == 1 ? 0 : i % NS;
+        float2 a[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) a[q] = ld.one(i + q * M, c);
+        if (NS > 1 && j != 0) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) a[q] = cmul(a[q], __ldg(tw + j * (R - 1) + (q - 1)));
+        }
+        dft<R>(a);
+        const int base = (i - j) * R + j;
+#pragma unroll
+        for (int k = 0; k < R; ++k) dst[(base + k * NS) * PITCH + c] = a[k];
+    }
+}
 
 template <int R, int NS, int M, int PITCH, class L>
 __device__ __forceinline__ void fft_stage_cl(const L &ld, float2 *__restrict__ dst, const float2 *__restrict__ tw,
@@ -302,7 +440,10 @@ __device__ __forceinline__ void fft_stages_c(float2 *&src, float2 *&dst, const f
     constexpr StagePlan P = stage_plan(N);
     if constexpr (S < P.nst) {
         constexpr int R = P.radix[S], NS = P.ns[S];
-        fft_stage_c<R, NS, N / R, PITCH>(src, dst, tw + P.twoff[S], stream, cp);
+        if constexpr (one_col_radix(R))
+            fft_stage1_cl<R, NS, N / R, PITCH>(PitchLoad<PITCH>{src}, dst, tw + P.twoff[S]);
+        else
+            fft_stage_c<R, NS, N / R, PITCH>(src, dst, tw + P.twoff[S], stream, cp);
         __syncthreads();
         float2 *t = src;
         src = dst;
@@ -360,7 +501,10 @@ template <int N, int PITCH, class L>
 __device__ __forceinline__ float2 *fft_run_first_n(const L &ld, float2 *A, float2 *B, const float2 *tw) {
     constexpr StagePlan SP = stage_plan(N);
     const int cp = threadIdx.x & (kCols / 2 - 1), stream = threadIdx.x / (kCols / 2);
-    fft_stage_cl<SP.radix[0], SP.ns[0], N / SP.radix[0], PITCH>(ld, B, tw + SP.twoff[0], stream, cp);
+    if constexpr (one_col_radix(SP.radix[0]))
+        fft_stage1_cl<SP.radix[0], SP.ns[0], N / SP.radix[0], PITCH>(ld, B, tw + SP.twoff[0]);
+    else
+        fft_stage_cl<SP.radix[0], SP.ns[0], N / SP.radix[0], PITCH>(ld, B, tw + SP.twoff[0], stream, cp);
     __syncthreads();
     float2 *src = B, *dst = A;
     fft_stages_c<N, 1, PITCH>(src, dst, tw, stream, cp);
@@ -1211,31 +1355,32 @@ __global__ void __launch_bounds__(kThreads) row_inv_kernel(const RowPass P) {
 
 constexpr double kPi = 3.14159265358979323846;
 
-// radices in the order the stages use them
-bool make_axis(int n, FftAxis *fa, std::vector<float2> &tw) {
+// Appends the axis's twiddles to tw: its stages' offsets are relative to *base,
+// the axis's first twiddle in tw (the kernels get the table from there).
+bool make_axis(int n, FftAxis *fa, std::vector<float2> &tw, size_t *base) {
     if (n < 1 || n > kMaxN) return false;
     *fa = FftAxis{};
     fa->n = n;
-    int m = n, ns = 1;
-    const int order[7] = {8, 10, 5, 4, 3, 7, 2};
-    for (int r : order) {
-        while (m % r == 0) {
-            if (fa->nst >= kFftMaxStages) return false;
-            const int s = fa->nst++;
-            fa->radix[s] = r;
-            fa->ns[s] = ns;
-            fa->twoff[s] = (int)tw.size();
-            fa->magic[s] = ns > 1 ? (unsigned)(0xFFFFFFFFull / (unsigned long long)ns + 1ull) : 0u;
-            for (int j = 0; j < ns; ++j)
-                for (int q = 1; q < r; ++q) {
-                    const double ang = -2.0 * kPi * (double)j * (double)q / ((double)ns * (double)r);
-                    tw.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
-                }
-            ns *= r;
-            m /= r;
-        }
+    const StagePlan sp = stage_plan(n);
+    int prod = 1;
+    for (int s = 0; s < sp.nst; ++s) prod *= sp.radix[s];
+    if (prod != n) return false;
+    *base = tw.size();
+    fa->nst = sp.nst;
+    for (int s = 0; s < sp.nst; ++s) {
+        const int r = sp.radix[s], ns = sp.ns[s];
+        fa->radix[s] = r;
+        fa->ns[s] = ns;
+        fa->twoff[s] = (int)(tw.size() - *base);
+        if (fa->twoff[s] != sp.twoff[s]) return false;
+        fa->magic[s] = ns > 1 ? (unsigned)(0xFFFFFFFFull / (unsigned long long)ns + 1ull) : 0u;
+        for (int j = 0; j < ns; ++j)
+            for (int q = 1; q < r; ++q) {
+                const double ang = -2.0 * kPi * (double)j * (double)q / ((double)ns * (double)r);
+                tw.push_back(make_float2((float)std::cos(ang), (float)std::sin(ang)));
+            }
     }
-    return m == 1;
+    return true;
 }
 
 // the accumulator over segments only when there are several
@@ -1522,8 +1667,9 @@ int fft_fused_ready(pfb_plan *p) {
     const int D = p->g.ndim;
     if (D < 2) return 0;
     std::vector<float2> tw;
+    size_t tw_base[3] = {0, 0, 0};
     for (int a = 0; a < D; ++a)
-        if (!make_axis(p->g.nos[a], &p->fft_ax[a], tw)) return 0;
+        if (!make_axis(p->g.nos[a], &p->fft_ax[a], tw, &tw_base[a])) return 0;
     if (tw.empty()) tw.push_back(make_float2(1.f, 0.f));
     if (pool_alloc(reinterpret_cast<void **>(&p->d_fft_tw), tw.size() * sizeof(float2)) != PFB_OK) return 0;
     if (cudaMemcpy(p->d_fft_tw, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -1531,7 +1677,7 @@ int fft_fused_ready(pfb_plan *p) {
         p->d_fft_tw = nullptr;
         return 0;
     }
-    for (int a = 0; a < D; ++a) p->fft_ax[a].tw = p->d_fft_tw;
+    for (int a = 0; a < D; ++a) p->fft_ax[a].tw = p->d_fft_tw + tw_base[a];
     // the TMA column pass's flag and persistent grid (optional: without them the
     // copy-based column pass runs)
     int dev = 0;

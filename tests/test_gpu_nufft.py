@@ -86,6 +86,17 @@ def test_odd_sizes_and_anisotropic():
     check_pair(coord, N, crandn(rng, 2, *N), crandn(rng, 2, 30, 50), width=(5, 3), oversamp=(1.5, 2.0))
 
 
+@pytest.mark.parametrize("N", [(128, 200), (200, 192), (96, 128, 200)])
+def test_anisotropic_grids_with_fused_transform_lengths(N):
+    """Grids whose axes have different lengths of the fused transform's compile-time
+    plans (osf 1.25: 160 x 250, 250 x 240, 120 x 160 x 250): each axis reads its own
+    twiddles, the two-stage 240 / 250 plans included."""
+    rng = np.random.default_rng(11)
+    d = len(N)
+    coord = ((rng.random((20, 600, d)) - 0.5) * np.array(N[::-1])).astype(np.float32)
+    check_pair(coord, N, crandn(rng, 2, *N), crandn(rng, 2, 20, 600), width=4, oversamp=1.25)
+
+
 def test_edges_and_out_of_range_wrap():
     """Samples at exactly -N/2 and +N/2 - eps, and beyond +-N/2 (reference wraps mod n_os)."""
     rng = np.random.default_rng(4)
