@@ -19,13 +19,16 @@
 // of an unpruned transform, and the pad, crop and channel transpose cost nothing
 // extra.
 //
-// Each 1D transform is a mixed-radix Stockham autosort FFT (radices 8, 5, 4, 3, 7, 2;
-// Govindaraju et al., "High performance discrete Fourier transforms on graphics
-// processors", SC 2008): stage s with radix r and ns = product of the earlier radices
-// reads x_q = src[i + q n / r], multiplies by exp(-2 pi i j q / (ns r)) (j = i mod
-// ns), takes the r-point DFT and writes dst[(i - j) r + j + k ns].  A CTA holds 16
-// vectors (columns of shared memory, one lane each in a half-warp); 16 streams of
-// butterflies run over them.  The inverse transform conjugates on load and store.
+// Each 1D transform is a mixed-radix Stockham autosort FFT (radices 8, 10, 5, 4, 3, 7,
+// 2, and 16 x 15 / 25 x 10 for the 240- and 250-point transforms; Govindaraju et al.,
+// "High performance discrete Fourier transforms on graphics processors", SC 2008):
+// stage s with radix r and ns = product of the earlier radices reads
+// x_q = src[i + q n / r], multiplies by exp(-2 pi i j q / (ns r)) (j = i mod ns),
+// takes the r-point DFT and writes dst[(i - j) r + j + k ns].  A CTA holds 16 vectors
+// (columns of shared memory); a thread takes two adjacent columns of a butterfly, or
+// one column for radices 15, 16 and 25.  Inverse passes run the forward transform
+// and read its output reversed, IDFT(x)[k] = DFT(x)[(n - k) mod n], or (the
+// copy-based x pass) conjugate on load and store.
 // Twiddles are computed in double precision on the host.
 
 #include <cuda.h>
