@@ -309,6 +309,14 @@ constexpr StagePlan stage_plan(int n) {
         rad[0] = 25;
         rad[1] = 10;
         nr = 2;
+    } else if (n == 160) {
+        rad[0] = 16;
+        rad[1] = 10;
+        nr = 2;
+    } else if (n == 256) {
+        rad[0] = 16;
+        rad[1] = 16;
+        nr = 2;
     } else {
         int m = n;
         for (int k = 0; k < 7; ++k) {
