@@ -20,8 +20,9 @@
 // extra.
 //
 // Each 1D transform is a mixed-radix Stockham autosort FFT (radices 8, 10, 5, 4, 3, 7,
-// 2, and 16 x 15 / 25 x 10 for the 240- and 250-point transforms; Govindaraju et al.,
-// "High performance discrete Fourier transforms on graphics processors", SC 2008):
+// 2, and two stages of radix 15, 16, 25 or 10 for the 240-, 250-, 160- and 256-point
+// transforms; Govindaraju et al., "High performance discrete Fourier transforms on
+// graphics processors", SC 2008):
 // stage s with radix r and ns = product of the earlier radices reads
 // x_q = src[i + q n / r], multiplies by exp(-2 pi i j q / (ns r)) (j = i mod ns),
 // takes the r-point DFT and writes dst[(i - j) r + j + k ns].  A CTA holds 16 vectors
@@ -287,9 +288,10 @@ __device__ __forceinline__ void fft_stage(const float2 *__restrict__ src, float2
 // The stage plan of a transform length: the radix order 8, 10, 5, 4, 3, 7, 2, each
 // as often as it divides, except for the lengths of the benchmark grids, which run
 // two stages (one CTA barrier and one shared-memory round trip fewer than the three
-// the radix order gives): 240 = 16 x 15 and 250 = 25 x 10.  make_axis builds the
-// twiddle table from the same plan, so the compile-time and table-driven forms
-// agree; radices 15, 16 and 25 only occur in the compile-time form.
+// the radix order gives): 240 = 16 x 15, 250 = 25 x 10, 160 = 16 x 10 and
+// 256 = 16 x 16.  make_axis builds the twiddle table from the same plan, so the
+// compile-time and table-driven forms agree; radices 15, 16 and 25 only occur in
+// the compile-time form.
 constexpr int kRadixOrder[7] = {8, 10, 5, 4, 3, 7, 2};
 struct StagePlan {
     int nst = 0;
